@@ -1,0 +1,219 @@
+// cpm_internal.cuh — shared device helpers and launcher declarations of libcpm_cuda.so.
+//
+// Arithmetic that must round exactly like the reference's Rust f32 code (CIC stencil and
+// gather, density contrast, Green's function, kick/drift, the tree's accept/prune tests) is
+// written with __fmul_rn/__fadd_rn/__fdiv_rn, which the compiler never contracts into FMAs.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/cpm.h"
+
+namespace cpm {
+
+// ---------------------------------------------------------------------------------------------
+// Status word written by kernels (no __trap, no device assert): the first error wins.
+// ---------------------------------------------------------------------------------------------
+enum DevError : int {
+  DEV_OK = 0,
+  DEV_NONFINITE = 1,        // NaN / Inf position
+  DEV_NODE_CAPACITY = 2,    // octree needs more nodes than allocated
+  DEV_STACK_OVERFLOW = 3,   // walk stack deeper than its bound
+  DEV_DEPTH_LIMIT = 4,      // more than LEAF_SIZE particles share all key digits (informational)
+};
+
+struct DevStatus {
+  int code;
+  int detail;
+};
+
+__device__ __forceinline__ void dev_fail(DevStatus* st, int code, int detail) {
+  if (atomicCAS(&st->code, 0, code) == 0) st->detail = detail;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Reference constants (tree.rs:12-17)
+// ---------------------------------------------------------------------------------------------
+constexpr int LEAF_SIZE = 8;
+constexpr int MAX_DEPTH = 40;
+constexpr int KEY_LEVELS = 21;  // 63-bit octant keys
+constexpr float SQRT_3 = 1.7320508f;
+constexpr float TWO_OVER_SQRT_PI = 1.1283792f;
+
+// ---------------------------------------------------------------------------------------------
+// mesh.rs:29-59 — CIC stencil, bit-identical to the reference's f32 arithmetic.
+// ---------------------------------------------------------------------------------------------
+struct CicBase {
+  int b[3];    // floor(x/h - 1/2)
+  float f[3];  // fractional part
+};
+
+__device__ __forceinline__ void cic_base(const float x[3], float h, CicBase& c) {
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float s = __fsub_rn(__fdiv_rn(x[k], h), 0.5f);
+    const float i0 = floorf(s);
+    c.b[k] = (int)i0;
+    c.f[k] = __fsub_rn(s, i0);
+  }
+}
+
+__device__ __forceinline__ int wrap_index(int i, int n) {
+  int r = i % n;
+  return r < 0 ? r + n : r;
+}
+
+// mesh.rs:81-83
+__device__ __forceinline__ float axis_weight(float f, int d) { return d == 0 ? __fsub_rn(1.0f, f) : f; }
+
+// Weight of corner c (c = dx*4 + dy*2 + dz, the reference's loop order).
+__device__ __forceinline__ float cic_weight(const CicBase& c, int corner) {
+  const int dx = (corner >> 2) & 1, dy = (corner >> 1) & 1, dz = corner & 1;
+  return __fmul_rn(__fmul_rn(axis_weight(c.f[0], dx), axis_weight(c.f[1], dy)), axis_weight(c.f[2], dz));
+}
+
+__device__ __forceinline__ size_t cic_index(const CicBase& c, int corner, int n) {
+  const int dx = (corner >> 2) & 1, dy = (corner >> 1) & 1, dz = corner & 1;
+  const size_t ix = (size_t)wrap_index(c.b[0] + dx, n);
+  const size_t iy = (size_t)wrap_index(c.b[1] + dy, n);
+  const size_t iz = (size_t)wrap_index(c.b[2] + dz, n);
+  return (ix * (size_t)n + iy) * (size_t)n + iz;
+}
+
+// fft.rs:86-95 with two_pi_over_l = (2 * (f32)pi) / L precomputed on the host.
+__device__ __forceinline__ float wavenumber(int i, int n, float two_pi_over_l) {
+  if ((n & 1) == 0 && i == n / 2) return 0.0f;
+  if (i <= n / 2) return __fmul_rn((float)i, two_pi_over_l);
+  return __fmul_rn(__fsub_rn((float)i, (float)n), two_pi_over_l);
+}
+
+// f32::rem_euclid (Rust std) for the drift (integrator.rs:313).
+__device__ __forceinline__ float rem_euclid_f32(float v, float rhs) {
+  const float r = fmodf(v, rhs);
+  return r < 0.0f ? __fadd_rn(r, fabsf(rhs)) : r;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Device buffers
+// ---------------------------------------------------------------------------------------------
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+cudaError_t ensure(DevBuf& b, size_t bytes);
+void release(DevBuf& b);
+
+template <typename T>
+T* as(DevBuf& b) {
+  return static_cast<T*>(b.p);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Radix sort of (u64 key, u32 value) pairs — keys.cu / sort.cu
+// ---------------------------------------------------------------------------------------------
+struct SortScratch {
+  DevBuf keys_alt, vals_alt, block_hist, scan_tmp;
+};
+
+// Octant keys (tree.rs descent) of positions (AoS f32 or float4), values = 0..n-1.
+void launch_octant_keys(const float* x3, size_t n, float box, int levels, uint64_t* keys, uint32_t* vals,
+                        DevStatus* st, cudaStream_t s);
+// Stable LSD sort of the low `bits` bits of keys; result in keys/vals (ping-pong handled inside).
+cudaError_t radix_sort_pairs(uint64_t* keys, uint32_t* vals, size_t n, int bits, SortScratch& sc,
+                             cudaStream_t s);
+// Exclusive scan of u32 (in place allowed); `tmp` is grown as needed.
+cudaError_t exclusive_scan_u32(const uint32_t* in, uint32_t* out, size_t n, DevBuf& tmp, cudaStream_t s);
+
+// ---------------------------------------------------------------------------------------------
+// Deposit — deposit.cu
+// ---------------------------------------------------------------------------------------------
+// Fixed-point scale exponent for masses summing to at most `total_mass`.
+int fixed_point_shift(double total_mass);
+// CIC deposit of `mass` per particle into the u64 fixed-point mesh (zeroed inside).
+void launch_deposit_fixed(const float* x3, size_t n, float mass, int mesh_n, float h, int shift,
+                          unsigned long long* mesh_fx, cudaStream_t s);
+// cells = (float)fx * 2^-shift, or delta = cells / mean - 1 when to_delta.
+void launch_fixed_to_f32(const unsigned long long* fx, size_t m, int shift, int to_delta, float mean, float* out,
+                         cudaStream_t s);
+
+// ---------------------------------------------------------------------------------------------
+// FFT / Poisson — fft.cu
+// ---------------------------------------------------------------------------------------------
+bool fft_supported(int n);
+struct FftPlan {
+  int n = 0;
+  DevBuf twiddle;  // exp(-2 pi i m / n), m < n, float2 built from double
+};
+cudaError_t fft_plan_init(FftPlan& p, int n);
+void fft_plan_free(FftPlan& p);
+// In-place unnormalised c2c n^3 transform (z, then y, then x lines).
+void launch_fft3_c2c(const FftPlan& p, float2* data, int inverse, cudaStream_t s);
+
+struct PoissonParams {
+  int n;
+  float two_pi_over_l;
+  float prefactor;  // 1.5 Omega_m / a (f32)
+  float r_split;
+  float scale;      // 1 / n^3 (f32)
+  int deconvolve;
+};
+// Input: either f32 delta (delta != nullptr) or the u64 fixed-point mass mesh (fx != nullptr,
+// converted to delta = c/mean - 1 on load). Output: three f32 meshes. spec: 3 half spectra
+// of n*n*(n/2+1) float2 each; slot 0 also holds the forward spectrum.
+void launch_poisson(const FftPlan& p, const PoissonParams& pp, const float* delta, const unsigned long long* fx,
+                    int fx_shift, float mean, float2* spec, float* gx, float* gy, float* gz, cudaStream_t s);
+
+// ---------------------------------------------------------------------------------------------
+// Gather — gather.cu
+// ---------------------------------------------------------------------------------------------
+void launch_interpolate(const float* cells, const float* x3, size_t n, int mesh_n, float h, float* out,
+                        cudaStream_t s);
+// out3[i] = (interp gx, gy, gz)[i]; when `add` != 0, out3 += that instead (f32 add in reference order).
+void launch_interpolate3(const float* gx, const float* gy, const float* gz, const float* x3, size_t n, int mesh_n,
+                         float h, float* out3, cudaStream_t s);
+
+// ---------------------------------------------------------------------------------------------
+// Tree — tree.cu
+// ---------------------------------------------------------------------------------------------
+struct TreeNodes {
+  DevBuf geo;    // float4 centre.xyz, half
+  DevBuf mass;   // float4 com.xyz, count
+  DevBuf link;   // uint4 start, end, first_child, child_mask | depth << 8
+  DevBuf counters;  // u32[64]: per-level allocation counts, totals
+  DevBuf prefix;    // double prefix sums of sorted positions (3 per particle + 3)
+  DevBuf scan_tmp;
+  size_t capacity = 0;
+};
+struct TreeCounters {
+  unsigned long long leaf_pairs;
+  unsigned long long node_accepts;
+};
+// Builds the octree over sorted keys/positions (sorted x as AoS f32). Returns the node count
+// through the counters buffer (read by tree_node_count).
+cudaError_t tree_build(TreeNodes& t, const uint64_t* sorted_keys, const float* sorted_x3, size_t n, float box,
+                       DevStatus* st, cudaStream_t s);
+// Walks the tree for every sorted particle; acc3 (sorted order) receives g_sr, or g + g_sr
+// when `accumulate` (the reference's g[c] += s[c], integrator.rs:154-158).
+void launch_tree_walk(const TreeNodes& t, const float* sorted_x3, size_t n, float box, const cpm_force_split& split,
+                      float k, float* acc3, int accumulate, TreeCounters* counters, DevStatus* st, cudaStream_t s);
+
+// ---------------------------------------------------------------------------------------------
+// Particle updates — kdk.cu
+// ---------------------------------------------------------------------------------------------
+// p += g * k (integrator.rs:301-307)
+void launch_kick(float* p3, const float* g3, size_t n, float k, cudaStream_t s);
+// Optional kick with k_prev, then kick with k1, then drift (integrator.rs:301-316).
+void launch_kick_kick_drift(float* x3, float* p3, const float* g3, size_t n, float k_prev, int has_prev, float k1,
+                            float d, float box, cudaStream_t s);
+// Gather permutation: out[i] = in[perm[i]] for AoS triples and for u32 ids.
+void launch_permute3(const float* in3, const uint32_t* perm, size_t n, float* out3, cudaStream_t s);
+void launch_permute_u32(const uint32_t* in, const uint32_t* perm, size_t n, uint32_t* out, cudaStream_t s);
+// Scatter back to caller order: out[id[i]] = in[i].
+void launch_scatter3(const float* in3, const uint32_t* id, size_t n, float* out3, cudaStream_t s);
+// Flags a non-finite coordinate in the status word.
+void launch_check_finite(const float* x3, size_t n, DevStatus* st, cudaStream_t s);
+
+}  // namespace cpm

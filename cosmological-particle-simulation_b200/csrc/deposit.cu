@@ -1,0 +1,152 @@
+// deposit.cu — CIC mass deposit (mesh.rs:62-69) into a 64-bit fixed-point mesh.
+//
+// Particles arrive sorted by octant key, so a chunk of consecutive particles covers a compact
+// box of cells. Each CTA accumulates its chunk into that box in shared memory with 64-bit
+// integer atomics, then flushes every non-zero cell to the global mesh with one 64-bit integer
+// atomic. Integer addition is associative, so the mesh does not depend on particle order or
+// scheduling (bit-reproducible), and it holds the exactly rounded sum of the reference's f32
+// weights `mass * w`. Chunks whose box does not fit in shared memory fall back to direct global
+// atomics (same integers, same result).
+#include <algorithm>
+#include <cmath>
+
+#include "cpm_internal.cuh"
+
+namespace cpm {
+
+constexpr int DEP_THREADS = 256;
+constexpr int DEP_PPT = 4;                          // particles per thread
+constexpr int DEP_CHUNK = DEP_THREADS * DEP_PPT;    // 1024 particles per CTA
+constexpr int DEP_SMEM_CELLS = 12288;               // 96 KB of u64 per CTA
+
+int fixed_point_shift(double total_mass) {
+  // Largest k with total_mass * 2^k < 2^62, clamped so a unit weight keeps >= 24 fractional bits.
+  const double m = total_mass > 1e-30 ? total_mass : 1e-30;
+  int k = 62 - (int)std::ceil(std::log2(m));
+  if (k > 60) k = 60;
+  if (k < 24) k = 24;
+  return k;
+}
+
+__device__ __forceinline__ unsigned long long to_fixed(float mass, float w, float scale) {
+  // mass * w is the reference's f32 product; scaling by 2^k is exact.
+  return __float2ull_rn(__fmul_rn(__fmul_rn(mass, w), scale));
+}
+
+__global__ void __launch_bounds__(DEP_THREADS) k_deposit_fixed(const float* __restrict__ x3, size_t n, float mass,
+                                                               int mesh_n, float h, float scale,
+                                                               unsigned long long* __restrict__ mesh) {
+  extern __shared__ unsigned long long sm_cells[];
+  __shared__ int bb[6];  // min x,y,z then max x,y,z of the stencil base
+  if (threadIdx.x < 3) bb[threadIdx.x] = 0x7fffffff;
+  else if (threadIdx.x < 6) bb[threadIdx.x] = -0x7fffffff;
+  __syncthreads();
+
+  const size_t base = (size_t)blockIdx.x * DEP_CHUNK;
+  CicBase cb[DEP_PPT];
+  bool valid[DEP_PPT];
+  int lo[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff}, hi[3] = {-0x7fffffff, -0x7fffffff, -0x7fffffff};
+#pragma unroll
+  for (int q = 0; q < DEP_PPT; ++q) {
+    const size_t i = base + (size_t)q * DEP_THREADS + threadIdx.x;
+    valid[q] = i < n;
+    if (valid[q]) {
+      const float x[3] = {x3[3 * i], x3[3 * i + 1], x3[3 * i + 2]};
+      cic_base(x, h, cb[q]);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        lo[k] = min(lo[k], cb[q].b[k]);
+        hi[k] = max(hi[k], cb[q].b[k]);
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      lo[k] = min(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
+      hi[k] = max(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
+    }
+  }
+  if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      atomicMin(&bb[k], lo[k]);
+      atomicMax(&bb[3 + k], hi[k]);
+    }
+  }
+  __syncthreads();
+  const int e0 = bb[3] - bb[0] + 2, e1 = bb[4] - bb[1] + 2, e2 = bb[5] - bb[2] + 2;
+  const long long cells = (long long)e0 * e1 * e2;
+  if (bb[0] > bb[3]) return;  // empty chunk
+
+  if (cells <= DEP_SMEM_CELLS && e0 > 0 && e1 > 0 && e2 > 0) {
+    for (int t = threadIdx.x; t < (int)cells; t += DEP_THREADS) sm_cells[t] = 0ull;
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < DEP_PPT; ++q) {
+      if (!valid[q]) continue;
+      const int lx = cb[q].b[0] - bb[0], ly = cb[q].b[1] - bb[1], lz = cb[q].b[2] - bb[2];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        const int dx = (c >> 2) & 1, dy = (c >> 1) & 1, dz = c & 1;
+        const int li = ((lx + dx) * e1 + (ly + dy)) * e2 + (lz + dz);
+        atomicAdd(&sm_cells[li], to_fixed(mass, cic_weight(cb[q], c), scale));
+      }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < (int)cells; t += DEP_THREADS) {
+      const unsigned long long v = sm_cells[t];
+      if (v == 0ull) continue;
+      const int lz = t % e2, ly = (t / e2) % e1, lx = t / (e1 * e2);
+      const size_t gx = (size_t)wrap_index(bb[0] + lx, mesh_n);
+      const size_t gy = (size_t)wrap_index(bb[1] + ly, mesh_n);
+      const size_t gz = (size_t)wrap_index(bb[2] + lz, mesh_n);
+      atomicAdd(&mesh[(gx * mesh_n + gy) * mesh_n + gz], v);
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < DEP_PPT; ++q) {
+      if (!valid[q]) continue;
+#pragma unroll
+      for (int c = 0; c < 8; ++c)
+        atomicAdd(&mesh[cic_index(cb[q], c, mesh_n)], to_fixed(mass, cic_weight(cb[q], c), scale));
+    }
+  }
+}
+
+void launch_deposit_fixed(const float* x3, size_t n, float mass, int mesh_n, float h, int shift,
+                          unsigned long long* mesh_fx, cudaStream_t s) {
+  const size_t m = (size_t)mesh_n * mesh_n * mesh_n;
+  cudaMemsetAsync(mesh_fx, 0, m * sizeof(unsigned long long), s);
+  if (n == 0) return;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(k_deposit_fixed, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         DEP_SMEM_CELLS * (int)sizeof(unsigned long long));
+    attr_set = true;
+  }
+  const float scale = std::ldexp(1.0f, shift);
+  const unsigned blocks = (unsigned)((n + DEP_CHUNK - 1) / DEP_CHUNK);
+  k_deposit_fixed<<<blocks, DEP_THREADS, DEP_SMEM_CELLS * sizeof(unsigned long long), s>>>(x3, n, mass, mesh_n, h,
+                                                                                         scale, mesh_fx);
+}
+
+// integrator.rs:117-126: cell mass c = fixed * 2^-k rounded once to f32; delta = c / mean - 1.
+__global__ void k_fixed_to_f32(const unsigned long long* __restrict__ fx, size_t m, float inv_scale, int to_delta,
+                               float mean, float* __restrict__ out) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (size_t)gridDim.x * blockDim.x) {
+    const float c = __fmul_rn(__ull2float_rn(fx[i]), inv_scale);
+    out[i] = to_delta ? __fsub_rn(__fdiv_rn(c, mean), 1.0f) : c;
+  }
+}
+
+void launch_fixed_to_f32(const unsigned long long* fx, size_t m, int shift, int to_delta, float mean, float* out,
+                         cudaStream_t s) {
+  if (m == 0) return;
+  const float inv_scale = std::ldexp(1.0f, -shift);
+  const size_t blocks = std::min<size_t>((m + 255) / 256, 148 * 32);
+  k_fixed_to_f32<<<(unsigned)blocks, 256, 0, s>>>(fx, m, inv_scale, to_delta, mean, out);
+}
+
+}  // namespace cpm

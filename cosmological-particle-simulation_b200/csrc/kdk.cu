@@ -1,0 +1,95 @@
+// kdk.cu — kick and drift (integrator.rs:301-316), permutations of the particle arrays.
+//
+// The reference's `p += g * k` and `x = (x + p * d).rem_euclid(L)` are written with separately
+// rounded f32 operations (no FMA), so the update is bit-identical to the reference.
+#include "cpm_internal.cuh"
+
+namespace cpm {
+
+__global__ void k_kick(float* __restrict__ p3, const float* __restrict__ g3, size_t n3, float k) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += (size_t)gridDim.x * blockDim.x)
+    p3[i] = __fadd_rn(p3[i], __fmul_rn(g3[i], k));
+}
+
+// Second half-kick of the previous step (when has_prev), first half-kick of this step, drift.
+__global__ void k_kick_kick_drift(float* __restrict__ x3, float* __restrict__ p3, const float* __restrict__ g3,
+                                  size_t n3, float k_prev, int has_prev, float k1, float d, float box) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += (size_t)gridDim.x * blockDim.x) {
+    const float g = g3[i];
+    float p = p3[i];
+    if (has_prev) p = __fadd_rn(p, __fmul_rn(g, k_prev));
+    p = __fadd_rn(p, __fmul_rn(g, k1));
+    p3[i] = p;
+    x3[i] = rem_euclid_f32(__fadd_rn(x3[i], __fmul_rn(p, d)), box);
+  }
+}
+
+__global__ void k_permute3(const float* __restrict__ in3, const uint32_t* __restrict__ perm, size_t n,
+                           float* __restrict__ out3) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const size_t j = perm[i];
+  out3[3 * i] = in3[3 * j];
+  out3[3 * i + 1] = in3[3 * j + 1];
+  out3[3 * i + 2] = in3[3 * j + 2];
+}
+
+__global__ void k_permute_u32(const uint32_t* __restrict__ in, const uint32_t* __restrict__ perm, size_t n,
+                              uint32_t* __restrict__ out) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = in[perm[i]];
+}
+
+__global__ void k_scatter3(const float* __restrict__ in3, const uint32_t* __restrict__ id, size_t n,
+                           float* __restrict__ out3) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const size_t j = id[i];
+  out3[3 * j] = in3[3 * i];
+  out3[3 * j + 1] = in3[3 * i + 1];
+  out3[3 * j + 2] = in3[3 * i + 2];
+}
+
+__global__ void k_check_finite(const float* __restrict__ x3, size_t n3, DevStatus* st) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += (size_t)gridDim.x * blockDim.x)
+    if (!isfinite(x3[i])) dev_fail(st, DEV_NONFINITE, (int)(i / 3));
+}
+
+static unsigned grid_for(size_t work) {
+  size_t b = (work + 255) / 256;
+  if (b > 148 * 16) b = 148 * 16;
+  return (unsigned)(b ? b : 1);
+}
+
+void launch_kick(float* p3, const float* g3, size_t n, float k, cudaStream_t s) {
+  if (n == 0) return;
+  k_kick<<<grid_for(3 * n), 256, 0, s>>>(p3, g3, 3 * n, k);
+}
+
+void launch_kick_kick_drift(float* x3, float* p3, const float* g3, size_t n, float k_prev, int has_prev, float k1,
+                            float d, float box, cudaStream_t s) {
+  if (n == 0) return;
+  k_kick_kick_drift<<<grid_for(3 * n), 256, 0, s>>>(x3, p3, g3, 3 * n, k_prev, has_prev, k1, d, box);
+}
+
+void launch_permute3(const float* in3, const uint32_t* perm, size_t n, float* out3, cudaStream_t s) {
+  if (n == 0) return;
+  k_permute3<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(in3, perm, n, out3);
+}
+
+void launch_permute_u32(const uint32_t* in, const uint32_t* perm, size_t n, uint32_t* out, cudaStream_t s) {
+  if (n == 0) return;
+  k_permute_u32<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(in, perm, n, out);
+}
+
+void launch_scatter3(const float* in3, const uint32_t* id, size_t n, float* out3, cudaStream_t s) {
+  if (n == 0) return;
+  k_scatter3<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(in3, id, n, out3);
+}
+
+void launch_check_finite(const float* x3, size_t n, DevStatus* st, cudaStream_t s) {
+  if (n == 0) return;
+  k_check_finite<<<grid_for(3 * n), 256, 0, s>>>(x3, 3 * n, st);
+}
+
+}  // namespace cpm

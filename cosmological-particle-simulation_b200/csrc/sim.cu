@@ -1,0 +1,284 @@
+// sim.cu — device-resident simulation (integrator.rs:34-186 `Simulation`).
+//
+// State lives in HBM in octant-key order: x, p, acc (AoS f32) and id (the caller's index of each
+// particle). One KDK step is
+//   kick(k1) + drift(d)            (integrator.rs:178-181; k1, d from the reference's f32 factors)
+//   keys -> radix sort -> permute x, p, id into key order
+//   CIC deposit (u64 fixed point)  -> FFT-Poisson (poisson.rs) -> gather (integrator.rs:144-148)
+//   tree build + walk, added to the PM force (integrator.rs:149-159)
+//   kick(k2)                       (integrator.rs:183-184)
+// Particles are reordered every step; each particle's update is independent of its position in
+// the arrays, so the order only changes f32 summation order inside tree leaves.
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "cpm_host.h"
+#include "cpm_internal.cuh"
+
+using namespace cpm;
+
+namespace {
+constexpr int N_PHASES = 8;
+}
+
+struct cpm_sim {
+  cpm_sim_params P{};
+  cudaStream_t stream = nullptr;
+  std::string err;
+  size_t n = 0;
+  float box = 0.0f, h = 0.0f, mean = 0.0f, a = 0.0f;
+  int shift = 0;
+  FftPlan plan;
+  SortScratch sort;
+  TreeNodes tree;
+  DevBuf x, p, acc, id, x2, p2, id2, keys, vals, fx, gx, gy, gz, spec, status, counters;
+  cudaEvent_t ev[N_PHASES + 1] = {};
+  double phase_ms[N_PHASES] = {};
+  uint64_t timed_steps = 0;
+  uint32_t launches = 0;
+};
+
+#define SIM_CU(s, call)                                                                                      \
+  do {                                                                                                       \
+    cudaError_t e_ = (call);                                                                                 \
+    if (e_ != cudaSuccess)                                                                                   \
+      return set_error(&(s)->err, e_ == cudaErrorMemoryAllocation ? CPM_E_NOMEM : CPM_E_CUDA,                \
+                       std::string(#call) + ": " + cudaGetErrorString(e_));                                  \
+  } while (0)
+
+static int sim_check(cpm_sim* s) {
+  cudaError_t e = cudaStreamSynchronize(s->stream);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) return set_error(&s->err, CPM_E_CUDA, std::string("kernel: ") + cudaGetErrorString(e));
+  DevStatus st{0, 0};
+  e = cudaMemcpy(&st, s->status.p, sizeof(st), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return set_error(&s->err, CPM_E_CUDA, cudaGetErrorString(e));
+  if (st.code != DEV_OK) {
+    cudaMemset(s->status.p, 0, sizeof(DevStatus));
+    if (st.code == DEV_NONFINITE)
+      return set_error(&s->err, CPM_E_NONFINITE, "non-finite position at particle " + std::to_string(st.detail));
+    return set_error(&s->err, CPM_E_DEVICE,
+                     "device status " + std::to_string(st.code) + " detail " + std::to_string(st.detail));
+  }
+  return CPM_OK;
+}
+
+static void mark(cpm_sim* s, int phase) {
+  if (s->P.flags & CPM_SIM_TIMING) cudaEventRecord(s->ev[phase], s->stream);
+}
+
+// Sort into key order, then the force: deposit, FFT-Poisson, gather, tree. Phases 1..6.
+static int sim_accelerations(cpm_sim* s, float a) {
+  const size_t n = s->n;
+  const int mn = s->P.mesh_n;
+  mark(s, 1);
+  launch_octant_keys(as<float>(s->x), n, s->box, KEY_LEVELS, as<uint64_t>(s->keys), as<uint32_t>(s->vals),
+                     as<DevStatus>(s->status), s->stream);
+  SIM_CU(s, radix_sort_pairs(as<uint64_t>(s->keys), as<uint32_t>(s->vals), n, 3 * KEY_LEVELS, s->sort, s->stream));
+  launch_permute3(as<float>(s->x), as<uint32_t>(s->vals), n, as<float>(s->x2), s->stream);
+  launch_permute3(as<float>(s->p), as<uint32_t>(s->vals), n, as<float>(s->p2), s->stream);
+  launch_permute_u32(as<uint32_t>(s->id), as<uint32_t>(s->vals), n, as<uint32_t>(s->id2), s->stream);
+  std::swap(s->x, s->x2);
+  std::swap(s->p, s->p2);
+  std::swap(s->id, s->id2);
+  mark(s, 2);
+  launch_deposit_fixed(as<float>(s->x), n, 1.0f, mn, s->h, s->shift, as<unsigned long long>(s->fx), s->stream);
+  mark(s, 3);
+  const float r_split = s->P.use_tree ? s->P.split.r_split : 0.0f;
+  const PoissonParams pp =
+      make_poisson_params(mn, s->box, s->P.cosmo.omega_m, a, r_split, (s->P.flags & CPM_SIM_DECONVOLVE) ? 1 : 0);
+  launch_poisson(s->plan, pp, nullptr, as<unsigned long long>(s->fx), s->shift, s->mean, as<float2>(s->spec),
+                 as<float>(s->gx), as<float>(s->gy), as<float>(s->gz), s->stream);
+  mark(s, 4);
+  launch_interpolate3(as<float>(s->gx), as<float>(s->gy), as<float>(s->gz), as<float>(s->x), n, mn, s->h,
+                      as<float>(s->acc), s->stream);
+  mark(s, 5);
+  if (s->P.use_tree) {
+    SIM_CU(s, tree_build(s->tree, as<uint64_t>(s->keys), as<float>(s->x), n, s->box, as<DevStatus>(s->status),
+                         s->stream));
+    mark(s, 6);
+    SIM_CU(s, cudaMemsetAsync(s->counters.p, 0, 2 * sizeof(unsigned long long), s->stream));
+    const float k = tree_coupling(s->P.cosmo.omega_m, s->box, a, n);
+    launch_tree_walk(s->tree, as<float>(s->x), n, s->box, s->P.split, k, as<float>(s->acc), 1,
+                     as<TreeCounters>(s->counters), as<DevStatus>(s->status), s->stream);
+  } else {
+    mark(s, 6);
+  }
+  return CPM_OK;
+}
+
+extern "C" {
+
+int cpm_sim_create(const cpm_sim_params* params, const float* x3, const float* p3, float a0, cpm_sim** out) {
+  if (!out) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_create: out is NULL");
+  *out = nullptr;
+  if (!params || !x3 || !p3) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_create: null pointer");
+  const cpm_sim_params& P = *params;
+  if (P.n_particles == 0 || P.n_particles > 0x7FFFFFFFull)
+    return set_error(nullptr, CPM_E_INVALID, "cpm_sim_create: n_particles must be in [1, 2^31)");
+  if (!(P.box_size > 0.0f) || !(a0 > 0.0f)) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_create: box and a0 must be > 0");
+  if (!fft_supported(P.mesh_n))
+    return set_error(nullptr, CPM_E_UNSUPPORTED,
+                     "cpm_sim_create: mesh_n = " + std::to_string(P.mesh_n) + " is not a power of two in [4, 1024]");
+  int rc = check_device_once(nullptr);
+  if (rc) return rc;
+  cpm_sim* s = new cpm_sim();
+  s->P = P;
+  s->n = P.n_particles;
+  s->box = P.box_size;
+  s->h = P.box_size / (float)P.mesh_n;
+  const size_t m = (size_t)P.mesh_n * P.mesh_n * P.mesh_n;
+  s->mean = (float)s->n / (float)m;  // integrator.rs:120-121
+  s->shift = fixed_point_shift((double)s->n + 1.0);
+  s->a = a0;
+  auto fail = [&](int code) {
+    g_last_error = s->err;
+    cpm_sim_destroy(s);
+    return code;
+  };
+  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(CPM_E_CUDA);
+  for (auto& e : s->ev)
+    if (cudaEventCreate(&e) != cudaSuccess) return fail(CPM_E_CUDA);
+  const size_t n = s->n;
+  const size_t half = (size_t)P.mesh_n * P.mesh_n * (P.mesh_n / 2 + 1);
+  bool ok = true;
+  for (DevBuf* b : {&s->x, &s->p, &s->acc, &s->x2, &s->p2}) ok = ok && ensure(*b, 3 * n * sizeof(float)) == cudaSuccess;
+  for (DevBuf* b : {&s->id, &s->id2, &s->vals}) ok = ok && ensure(*b, n * sizeof(uint32_t)) == cudaSuccess;
+  ok = ok && ensure(s->keys, n * sizeof(uint64_t)) == cudaSuccess;
+  ok = ok && ensure(s->fx, m * sizeof(unsigned long long)) == cudaSuccess;
+  for (DevBuf* b : {&s->gx, &s->gy, &s->gz}) ok = ok && ensure(*b, m * sizeof(float)) == cudaSuccess;
+  ok = ok && ensure(s->spec, 3 * half * sizeof(float2)) == cudaSuccess;
+  ok = ok && ensure(s->status, sizeof(DevStatus)) == cudaSuccess;
+  ok = ok && ensure(s->counters, 2 * sizeof(unsigned long long)) == cudaSuccess;
+  ok = ok && fft_plan_init(s->plan, P.mesh_n) == cudaSuccess;
+  if (!ok) {
+    s->err = "cpm_sim_create: device allocation failed";
+    return fail(CPM_E_NOMEM);
+  }
+  cudaMemsetAsync(s->status.p, 0, sizeof(DevStatus), s->stream);
+  cudaMemsetAsync(s->counters.p, 0, 2 * sizeof(unsigned long long), s->stream);
+  if ((rc = cpm_sim_set_state(s, x3, p3)) != CPM_OK) {
+    g_last_error = s->err;
+    cpm_sim_destroy(s);
+    return rc;
+  }
+  *out = s;
+  return CPM_OK;
+}
+
+int cpm_sim_set_state(cpm_sim* s, const float* x3, const float* p3) {
+  if (!s || !x3 || !p3) return set_error(s ? &s->err : nullptr, CPM_E_INVALID, "cpm_sim_set_state: null pointer");
+  const size_t n = s->n;
+  SIM_CU(s, cudaMemcpyAsync(s->x.p, x3, 3 * n * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+  SIM_CU(s, cudaMemcpyAsync(s->p.p, p3, 3 * n * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+  std::vector<uint32_t> iota(n);
+  for (size_t i = 0; i < n; ++i) iota[i] = (uint32_t)i;
+  SIM_CU(s, cudaMemcpyAsync(s->id.p, iota.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+  launch_check_finite(as<float>(s->x), n, as<DevStatus>(s->status), s->stream);
+  int rc = sim_accelerations(s, s->a);
+  if (rc) return rc;
+  return sim_check(s);
+}
+
+int cpm_sim_step_to(cpm_sim* s, float a1) {
+  if (!s) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_step_to: sim is NULL");
+  if (!(a1 > 0.0f) || !std::isfinite(a1)) return set_error(&s->err, CPM_E_INVALID, "cpm_sim_step_to: a1 must be > 0");
+  const cpm_cosmology& c = s->P.cosmo;
+  const float a0 = s->a;
+  const float am = midpoint(c, a0, a1);
+  const float k1 = kick_factor(c, a0, am);
+  const float d = drift_factor(c, a0, a1);
+  const float k2 = kick_factor(c, am, a1);
+  mark(s, 0);
+  launch_kick_kick_drift(as<float>(s->x), as<float>(s->p), as<float>(s->acc), s->n, 0.0f, 0, k1, d, s->box, s->stream);
+  int rc = sim_accelerations(s, a1);
+  if (rc) return rc;
+  launch_kick(as<float>(s->p), as<float>(s->acc), s->n, k2, s->stream);
+  mark(s, 7);
+  s->a = a1;
+  if (s->P.flags & CPM_SIM_TIMING) {
+    SIM_CU(s, cudaEventSynchronize(s->ev[7]));
+    float ms;
+    // phases: 0 kick/drift [ev0, ev1], 1 sort [ev1, ev2], 2 deposit [ev2, ev3], 3 poisson [ev3, ev4],
+    // 4 gather [ev4, ev5], 5 tree build [ev5, ev6], 6 walk + kick2 [ev6, ev7], 7 whole [ev0, ev7]
+    for (int ph = 0; ph < 7; ++ph) {
+      cudaEventElapsedTime(&ms, s->ev[ph], s->ev[ph + 1]);
+      s->phase_ms[ph] += ms;
+    }
+    cudaEventElapsedTime(&ms, s->ev[0], s->ev[7]);
+    s->phase_ms[7] += ms;
+    s->timed_steps += 1;
+  }
+  return CPM_OK;
+}
+
+int cpm_sim_get_state(cpm_sim* s, float* x3, float* p3, float* acc3, float* delta, float* a) {
+  if (!s) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_get_state: sim is NULL");
+  const size_t n = s->n;
+  const float* srcs[3] = {as<float>(s->x), as<float>(s->p), as<float>(s->acc)};
+  float* dsts[3] = {x3, p3, acc3};
+  for (int q = 0; q < 3; ++q) {
+    if (!dsts[q]) continue;
+    launch_scatter3(srcs[q], as<uint32_t>(s->id), n, as<float>(s->x2), s->stream);
+    SIM_CU(s, cudaMemcpyAsync(dsts[q], s->x2.p, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+  }
+  if (delta) {
+    const size_t m = (size_t)s->P.mesh_n * s->P.mesh_n * s->P.mesh_n;
+    launch_fixed_to_f32(as<unsigned long long>(s->fx), m, s->shift, 1, s->mean, as<float>(s->gx), s->stream);
+    SIM_CU(s, cudaMemcpyAsync(delta, s->gx.p, m * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+  }
+  if (a) *a = s->a;
+  return sim_check(s);
+}
+
+int cpm_sim_phase_times(cpm_sim* s, double* ms8, uint64_t* steps, int reset) {
+  if (!s) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_phase_times: sim is NULL");
+  if (ms8)
+    for (int i = 0; i < N_PHASES; ++i) ms8[i] = s->timed_steps ? s->phase_ms[i] / (double)s->timed_steps : 0.0;
+  if (steps) *steps = s->timed_steps;
+  if (reset) {
+    for (double& v : s->phase_ms) v = 0.0;
+    s->timed_steps = 0;
+  }
+  return CPM_OK;
+}
+
+int cpm_sim_counters(cpm_sim* s, uint64_t* nodes, uint64_t* leaf_pairs, uint64_t* node_accepts,
+                     uint32_t* launches_per_step) {
+  if (!s) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_counters: sim is NULL");
+  SIM_CU(s, cudaStreamSynchronize(s->stream));
+  unsigned long long tc[2] = {0, 0};
+  SIM_CU(s, cudaMemcpy(tc, s->counters.p, sizeof(tc), cudaMemcpyDeviceToHost));
+  uint64_t nn = 0;
+  if (s->tree.counters.p) {
+    uint32_t cnt[64];
+    SIM_CU(s, cudaMemcpy(cnt, s->tree.counters.p, sizeof(cnt), cudaMemcpyDeviceToHost));
+    for (int d = 0; d <= KEY_LEVELS; ++d) nn += cnt[d];
+  }
+  if (nodes) *nodes = nn;
+  if (leaf_pairs) *leaf_pairs = tc[0];
+  if (node_accepts) *node_accepts = tc[1];
+  if (launches_per_step) *launches_per_step = s->launches;
+  return CPM_OK;
+}
+
+void* cpm_sim_stream(cpm_sim* s) { return s ? (void*)s->stream : nullptr; }
+
+int cpm_sim_destroy(cpm_sim* s) {
+  if (!s) return CPM_OK;
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  fft_plan_free(s->plan);
+  for (DevBuf* b : {&s->sort.keys_alt, &s->sort.vals_alt, &s->sort.block_hist, &s->sort.scan_tmp, &s->tree.geo,
+                    &s->tree.mass, &s->tree.link, &s->tree.counters, &s->tree.prefix, &s->tree.scan_tmp, &s->x, &s->p,
+                    &s->acc, &s->id, &s->x2, &s->p2, &s->id2, &s->keys, &s->vals, &s->fx, &s->gx, &s->gy, &s->gz,
+                    &s->spec, &s->status, &s->counters})
+    release(*b);
+  for (auto& e : s->ev)
+    if (e) cudaEventDestroy(e);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+  return CPM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,275 @@
+// sort.cu — octant keys of the tree descent, stable LSD radix sort of (u64 key, u32 value)
+// pairs, and exclusive scans. HBM-bound integer work: coalesced tiles, per-warp ranking with
+// __match_any_sync, no tensor cores.
+#include <algorithm>
+
+#include "cpm_internal.cuh"
+
+namespace cpm {
+
+cudaError_t ensure(DevBuf& b, size_t bytes) {
+  if (b.p != nullptr && b.bytes >= bytes) return cudaSuccess;
+  release(b);
+  const size_t want = bytes ? bytes : 16;
+  cudaError_t e = cudaMalloc(&b.p, want);
+  if (e != cudaSuccess) {
+    b.p = nullptr;
+    b.bytes = 0;
+    return e;
+  }
+  b.bytes = want;
+  return cudaSuccess;
+}
+
+void release(DevBuf& b) {
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.bytes = 0;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Octant keys: tree.rs:186-250 descent. At depth d the octant is (x>=cx)|(y>=cy)<<1|(z>=cz)<<2
+// against the node centre; the child centre is centre +- half/2, in f32. The first digit is the
+// most significant. Comparisons and additions only, so the digits are bit-exact.
+// ---------------------------------------------------------------------------------------------
+__global__ void k_octant_keys(const float* __restrict__ x3, size_t n, float half0, int levels,
+                              uint64_t* __restrict__ keys, uint32_t* __restrict__ vals, DevStatus* st) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float p0 = x3[3 * i], p1 = x3[3 * i + 1], p2 = x3[3 * i + 2];
+  if (!(isfinite(p0) && isfinite(p1) && isfinite(p2))) dev_fail(st, DEV_NONFINITE, (int)i);
+  float half = half0, c0 = half0, c1 = half0, c2 = half0;
+  uint64_t key = 0;
+  for (int d = 0; d < levels; ++d) {
+    const uint32_t o = (uint32_t)(p0 >= c0) | ((uint32_t)(p1 >= c1) << 1) | ((uint32_t)(p2 >= c2) << 2);
+    key = (key << 3) | o;
+    const float q = half * 0.5f;  // == half / 2.0 exactly
+    c0 = __fadd_rn(c0, (o & 1u) ? q : -q);
+    c1 = __fadd_rn(c1, (o & 2u) ? q : -q);
+    c2 = __fadd_rn(c2, (o & 4u) ? q : -q);
+    half = q;
+  }
+  keys[i] = key;
+  if (vals) vals[i] = (uint32_t)i;
+}
+
+void launch_octant_keys(const float* x3, size_t n, float box, int levels, uint64_t* keys, uint32_t* vals,
+                        DevStatus* st, cudaStream_t s) {
+  if (n == 0) return;
+  const int T = 256;
+  k_octant_keys<<<(unsigned)((n + T - 1) / T), T, 0, s>>>(x3, n, box / 2.0f, levels, keys, vals, st);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Exclusive scan of u32: tiles of 2048 (256 threads x 8 items), multi-level for large n.
+// ---------------------------------------------------------------------------------------------
+constexpr int SC_THREADS = 256;
+constexpr int SC_ITEMS = 8;
+constexpr int SC_TILE = SC_THREADS * SC_ITEMS;
+
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* total, uint32_t* warp_sums) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_sums[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = lane < (SC_THREADS / 32) ? warp_sums[lane] : 0u;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    if (lane < (SC_THREADS / 32)) warp_sums[lane] = w;
+  }
+  __syncthreads();
+  const uint32_t warp_prefix = warp ? warp_sums[warp - 1] : 0u;
+  *total = warp_sums[SC_THREADS / 32 - 1];
+  return warp_prefix + x - v;
+}
+
+__global__ void __launch_bounds__(SC_THREADS) k_scan_reduce(const uint32_t* __restrict__ in, size_t n,
+                                                            uint32_t* __restrict__ partial) {
+  __shared__ uint32_t ws[SC_THREADS / 32];
+  const size_t base = (size_t)blockIdx.x * SC_TILE;
+  uint32_t sum = 0;
+#pragma unroll
+  for (int j = 0; j < SC_ITEMS; ++j) {
+    const size_t i = base + (size_t)j * SC_THREADS + threadIdx.x;
+    if (i < n) sum += in[i];
+  }
+  uint32_t total;
+  block_exclusive_scan(sum, &total, ws);
+  if (threadIdx.x == 0) partial[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(SC_THREADS) k_scan_tile(const uint32_t* __restrict__ in, uint32_t* out, size_t n,
+                                                          const uint32_t* __restrict__ block_offsets) {
+  __shared__ uint32_t ws[SC_THREADS / 32];
+  const size_t base = (size_t)blockIdx.x * SC_TILE + (size_t)threadIdx.x * SC_ITEMS;
+  uint32_t v[SC_ITEMS];
+  uint32_t sum = 0;
+#pragma unroll
+  for (int j = 0; j < SC_ITEMS; ++j) {
+    const size_t i = base + j;
+    v[j] = i < n ? in[i] : 0u;
+    sum += v[j];
+  }
+  uint32_t total;
+  uint32_t run = block_exclusive_scan(sum, &total, ws);
+  if (block_offsets) run += block_offsets[blockIdx.x];
+#pragma unroll
+  for (int j = 0; j < SC_ITEMS; ++j) {
+    const size_t i = base + j;
+    if (i < n) out[i] = run;
+    run += v[j];
+  }
+}
+
+static size_t scan_tmp_words(size_t n) {
+  size_t total = 0;
+  while (n > (size_t)SC_TILE) {
+    n = (n + SC_TILE - 1) / SC_TILE;
+    total += n + 64;
+  }
+  return total + 64;
+}
+
+static void scan_rec(const uint32_t* in, uint32_t* out, size_t n, uint32_t* tmp, cudaStream_t s) {
+  if (n == 0) return;
+  if (n <= (size_t)SC_TILE) {
+    k_scan_tile<<<1, SC_THREADS, 0, s>>>(in, out, n, nullptr);
+    return;
+  }
+  const size_t nb = (n + SC_TILE - 1) / SC_TILE;
+  uint32_t* partial = tmp;
+  k_scan_reduce<<<(unsigned)nb, SC_THREADS, 0, s>>>(in, n, partial);
+  scan_rec(partial, partial, nb, tmp + nb + 64, s);
+  k_scan_tile<<<(unsigned)nb, SC_THREADS, 0, s>>>(in, out, n, partial);
+}
+
+cudaError_t exclusive_scan_u32(const uint32_t* in, uint32_t* out, size_t n, DevBuf& tmp, cudaStream_t s) {
+  cudaError_t e = ensure(tmp, scan_tmp_words(n) * sizeof(uint32_t));
+  if (e != cudaSuccess) return e;
+  scan_rec(in, out, n, as<uint32_t>(tmp), s);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------------------
+// LSD radix sort, 8-bit digits. Per pass: block histograms (digit-major), exclusive scan of the
+// histograms, then a stable scatter. Within a block each warp ranks a contiguous sub-tile in
+// warp-striped rounds with __match_any_sync, so equal digits keep their input order.
+// ---------------------------------------------------------------------------------------------
+constexpr int RS_THREADS = 256;
+constexpr int RS_ITEMS = 16;
+constexpr int RS_TILE = RS_THREADS * RS_ITEMS;
+constexpr int RS_WARPS = RS_THREADS / 32;
+constexpr int RS_BINS = 256;
+
+__global__ void __launch_bounds__(RS_THREADS) k_radix_hist(const uint64_t* __restrict__ keys, size_t n, int shift,
+                                                           uint32_t* __restrict__ block_hist, int nblocks) {
+  __shared__ uint32_t h[RS_BINS];
+  for (int t = threadIdx.x; t < RS_BINS; t += RS_THREADS) h[t] = 0;
+  __syncthreads();
+  const size_t base = (size_t)blockIdx.x * RS_TILE;
+  const int lane = threadIdx.x & 31;
+#pragma unroll 4
+  for (int j = 0; j < RS_ITEMS; ++j) {
+    const size_t i = base + (size_t)j * RS_THREADS + threadIdx.x;
+    const bool valid = i < n;
+    const uint32_t d = valid ? (uint32_t)((keys[i] >> shift) & (RS_BINS - 1)) : (0x100u | (uint32_t)lane);
+    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    if (valid && (__ffs(peers) - 1) == lane) atomicAdd(&h[d], (uint32_t)__popc(peers));
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < RS_BINS; t += RS_THREADS) block_hist[(size_t)t * nblocks + blockIdx.x] = h[t];
+}
+
+__global__ void __launch_bounds__(RS_THREADS) k_radix_scatter(const uint64_t* __restrict__ kin,
+                                                              const uint32_t* __restrict__ vin,
+                                                              uint64_t* __restrict__ kout,
+                                                              uint32_t* __restrict__ vout, size_t n, int shift,
+                                                              const uint32_t* __restrict__ offsets, int nblocks) {
+  __shared__ uint32_t wc[RS_WARPS][RS_BINS];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int t = threadIdx.x; t < RS_WARPS * RS_BINS; t += RS_THREADS) (&wc[0][0])[t] = 0;
+  __syncthreads();
+  const unsigned lt_mask = (1u << lane) - 1u;
+  const size_t wbase = (size_t)blockIdx.x * RS_TILE + (size_t)warp * 32 * RS_ITEMS;
+  uint64_t k[RS_ITEMS];
+  uint32_t v[RS_ITEMS];
+  uint32_t rank[RS_ITEMS];
+#pragma unroll
+  for (int j = 0; j < RS_ITEMS; ++j) {
+    const size_t i = wbase + (size_t)j * 32 + lane;
+    const bool valid = i < n;
+    k[j] = valid ? kin[i] : 0ull;
+    v[j] = valid ? vin[i] : 0u;
+    const uint32_t d = valid ? (uint32_t)((k[j] >> shift) & (RS_BINS - 1)) : (0x100u | (uint32_t)lane);
+    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    uint32_t prev = 0;
+    if (valid) prev = wc[warp][d];
+    __syncwarp();
+    if (valid) {
+      rank[j] = prev + (uint32_t)__popc(peers & lt_mask);
+      if ((__ffs(peers) - 1) == lane) wc[warp][d] = prev + (uint32_t)__popc(peers);
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < RS_BINS; t += RS_THREADS) {
+    uint32_t run = offsets[(size_t)t * nblocks + blockIdx.x];
+#pragma unroll
+    for (int w = 0; w < RS_WARPS; ++w) {
+      const uint32_t c = wc[w][t];
+      wc[w][t] = run;
+      run += c;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < RS_ITEMS; ++j) {
+    const size_t i = wbase + (size_t)j * 32 + lane;
+    if (i < n) {
+      const uint32_t d = (uint32_t)((k[j] >> shift) & (RS_BINS - 1));
+      const uint32_t pos = wc[warp][d] + rank[j];
+      kout[pos] = k[j];
+      vout[pos] = v[j];
+    }
+  }
+}
+
+cudaError_t radix_sort_pairs(uint64_t* keys, uint32_t* vals, size_t n, int bits, SortScratch& sc, cudaStream_t s) {
+  if (n <= 1 || bits <= 0) return cudaSuccess;
+  if (n > 0xFFFFFFFFull) return cudaErrorInvalidValue;
+  const int nblocks = (int)((n + RS_TILE - 1) / RS_TILE);
+  cudaError_t e;
+  if ((e = ensure(sc.keys_alt, n * sizeof(uint64_t))) != cudaSuccess) return e;
+  if ((e = ensure(sc.vals_alt, n * sizeof(uint32_t))) != cudaSuccess) return e;
+  if ((e = ensure(sc.block_hist, (size_t)RS_BINS * nblocks * sizeof(uint32_t))) != cudaSuccess) return e;
+  uint64_t* ka = keys;
+  uint32_t* va = vals;
+  uint64_t* kb = as<uint64_t>(sc.keys_alt);
+  uint32_t* vb = as<uint32_t>(sc.vals_alt);
+  uint32_t* hist = as<uint32_t>(sc.block_hist);
+  const int passes = (bits + 7) / 8;
+  for (int p = 0; p < passes; ++p) {
+    const int shift = 8 * p;
+    k_radix_hist<<<nblocks, RS_THREADS, 0, s>>>(ka, n, shift, hist, nblocks);
+    if ((e = exclusive_scan_u32(hist, hist, (size_t)RS_BINS * nblocks, sc.scan_tmp, s)) != cudaSuccess) return e;
+    k_radix_scatter<<<nblocks, RS_THREADS, 0, s>>>(ka, va, kb, vb, n, shift, hist, nblocks);
+    std::swap(ka, kb);
+    std::swap(va, vb);
+  }
+  if (ka != keys) {
+    if ((e = cudaMemcpyAsync(keys, ka, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(vals, va, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s)) != cudaSuccess) return e;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace cpm

@@ -1,0 +1,453 @@
+// tree.cu — octree build from sorted octant keys and the short-range walk (tree.rs:171-323).
+//
+// Build. Particles are sorted by their 63-bit octant key (21 digits of the reference's descent,
+// tree.rs:186-250), so every node of the reference's tree is a contiguous range of the sorted
+// array: the particles whose first d digits equal the node's prefix. One kernel per level splits
+// each node of that level that holds more than LEAF_SIZE particles: the 8 octant sub-ranges are
+// found by binary search on digit d+1 (sorted within the node), and the non-empty ones become
+// children, allocated contiguously in octant order. Node centres are built with the reference's
+// f32 arithmetic (centre +- half/2), so they are bit-identical. A node deeper than the 21 key
+// digits that still holds more than LEAF_SIZE particles stays a leaf (the reference would keep
+// splitting to depth 40); such nodes are counted.
+//
+// Centres of mass come from an FP64 exclusive prefix sum of the sorted positions: the sum over a
+// node is P[end] - P[start], divided by the count and rounded once to f32. (The reference sums
+// in f32 sequentially in input order; the difference is f32 round-off of that sum.)
+//
+// Walk. One warp walks for 32 consecutive sorted particles with one shared LIFO stack of
+// (node, lane mask) entries. A lane is in a node's mask exactly when its own reference walk
+// (tree.rs:264-310) would pop that node; each lane applies the reference's tests for itself:
+// prune when |min_image(centre - x)| > r_cut + sqrt(3) half; direct sum over the node's particles
+// when its octant-0 child is missing (`children[0] == NO_CHILD`, which includes leaves); else
+// accept the centre of mass when 2 half < theta |min_image(com - x)|, or push the children 0..7
+// for the lanes that opened it. Popping order is the reference's (7 first), so each lane adds its
+// contributions in the reference's node order. The tests use separately rounded f32 operations
+// and an exact minimum image, so accept/prune/cutoff decisions match the reference for equal
+// inputs.
+#include <algorithm>
+#include <vector>
+
+#include "cpm_internal.cuh"
+
+namespace cpm {
+
+constexpr int BUILD_THREADS = 256;
+constexpr int BUILD_BLOCKS = 148 * 4;
+
+// counters layout (u32): [0..KEY_LEVELS+1] per-level node counts (level 0 = root),
+// [32] nodes that hit the key-depth limit with > LEAF_SIZE particles, [33] max depth.
+constexpr int CNT_DEPTH_LIMIT = 32;
+constexpr int CNT_MAX_DEPTH = 33;
+constexpr int CNT_WORDS = 64;
+
+__device__ __forceinline__ uint32_t digit_at(uint64_t key, int shift) { return (uint32_t)(key >> shift) & 7u; }
+
+// first index in [lo, hi) whose digit is >= o (digits non-decreasing in the range)
+__device__ __forceinline__ uint32_t lower_bound_digit(const uint64_t* __restrict__ keys, uint32_t lo, uint32_t hi,
+                                                      uint32_t o, int shift) {
+  while (lo < hi) {
+    const uint32_t mid = lo + ((hi - lo) >> 1);
+    if (digit_at(__ldg(keys + mid), shift) < o)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+__global__ void k_tree_root(uint4* link, float4* geo, uint32_t* counters, uint32_t n, float half0) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    link[0] = make_uint4(0u, n, 0u, 0u);
+    geo[0] = make_float4(half0, half0, half0, half0);
+  }
+  if (blockIdx.x == 0 && threadIdx.x < CNT_WORDS) counters[threadIdx.x] = threadIdx.x == 0 ? 1u : 0u;
+}
+
+__global__ void __launch_bounds__(BUILD_THREADS) k_tree_level(int d, const uint64_t* __restrict__ keys, uint4* link,
+                                                              float4* geo, uint32_t* counters, uint32_t capacity,
+                                                              DevStatus* st) {
+  uint32_t lb = 0;
+  for (int j = 0; j < d; ++j) lb += counters[j];
+  const uint32_t cnt = counters[d];
+  const uint32_t next_base = lb + cnt;
+  // After a capacity failure the counters overshoot; never touch nodes past the arrays.
+  const uint32_t level_end = min(next_base, capacity);
+  const int shift = 3 * (KEY_LEVELS - 1 - d);
+  for (uint32_t node = lb + blockIdx.x * BUILD_THREADS + threadIdx.x; node < level_end;
+       node += gridDim.x * BUILD_THREADS) {
+    const uint4 L = link[node];
+    const uint32_t s = L.x, e = L.y, c = e - s;
+    if (c <= (uint32_t)LEAF_SIZE || d >= MAX_DEPTH) {
+      link[node] = make_uint4(s, e, 0u, (uint32_t)d << 8);
+      continue;
+    }
+    if (d >= KEY_LEVELS) {
+      atomicAdd(&counters[CNT_DEPTH_LIMIT], 1u);
+      link[node] = make_uint4(s, e, 0u, (uint32_t)d << 8);
+      continue;
+    }
+    uint32_t b[9];
+    b[0] = s;
+    b[8] = e;
+    uint32_t lo = s;
+#pragma unroll
+    for (uint32_t o = 1; o < 8; ++o) {
+      lo = lower_bound_digit(keys, lo, e, o, shift);
+      b[o] = lo;
+    }
+    uint32_t mask = 0;
+#pragma unroll
+    for (int o = 0; o < 8; ++o)
+      if (b[o + 1] > b[o]) mask |= 1u << o;
+    const uint32_t nch = (uint32_t)__popc(mask);
+    const uint32_t first = next_base + atomicAdd(&counters[d + 1], nch);
+    if (first + nch > capacity) {
+      dev_fail(st, DEV_NODE_CAPACITY, (int)(first + nch));
+      link[node] = make_uint4(s, e, 0u, (uint32_t)d << 8);
+      continue;
+    }
+    const float4 G = geo[node];
+    const float q = G.w * 0.5f;  // half / 2.0
+    uint32_t r = 0;
+#pragma unroll
+    for (int o = 0; o < 8; ++o) {
+      if (!(mask & (1u << o))) continue;
+      const uint32_t child = first + r++;
+      link[child] = make_uint4(b[o], b[o + 1], 0u, 0u);
+      geo[child] = make_float4(__fadd_rn(G.x, (o & 1) ? q : -q), __fadd_rn(G.y, (o & 2) ? q : -q),
+                               __fadd_rn(G.z, (o & 4) ? q : -q), q);
+    }
+    link[node] = make_uint4(s, e, first, mask | ((uint32_t)d << 8));
+    atomicMax(&counters[CNT_MAX_DEPTH], (uint32_t)(d + 1));
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// FP64 exclusive prefix sums of sorted positions: P[i] = sum_{j<i} x_j, P[n] = total.
+// ---------------------------------------------------------------------------------------------
+constexpr int PS_THREADS = 256;
+constexpr int PS_ITEMS = 8;
+constexpr int PS_TILE = PS_THREADS * PS_ITEMS;
+
+struct D3 {
+  double x, y, z;
+};
+__device__ __forceinline__ D3 d3add(D3 a, D3 b) { return D3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+
+__device__ __forceinline__ D3 shfl_up_d3(D3 v, int o) {
+  return D3{__shfl_up_sync(0xffffffffu, v.x, o), __shfl_up_sync(0xffffffffu, v.y, o),
+            __shfl_up_sync(0xffffffffu, v.z, o)};
+}
+
+// Block-wide exclusive scan of D3 (per-thread partial), returns the thread's prefix and the total.
+__device__ __forceinline__ D3 block_scan_d3(D3 v, D3* total, D3* ws) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  D3 x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const D3 y = shfl_up_d3(x, o);
+    if (lane >= o) x = d3add(x, y);
+  }
+  if (lane == 31) ws[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    D3 w = lane < PS_THREADS / 32 ? ws[lane] : D3{0.0, 0.0, 0.0};
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const D3 y = shfl_up_d3(w, o);
+      if (lane >= o) w = d3add(w, y);
+    }
+    if (lane < PS_THREADS / 32) ws[lane] = w;
+  }
+  __syncthreads();
+  const D3 wp = warp ? ws[warp - 1] : D3{0.0, 0.0, 0.0};
+  *total = ws[PS_THREADS / 32 - 1];
+  return D3{wp.x + x.x - v.x, wp.y + x.y - v.y, wp.z + x.z - v.z};
+}
+
+__global__ void __launch_bounds__(PS_THREADS) k_pos_reduce(const float* __restrict__ x3, size_t n, D3* partial) {
+  __shared__ D3 ws[PS_THREADS / 32];
+  const size_t base = (size_t)blockIdx.x * PS_TILE + (size_t)threadIdx.x * PS_ITEMS;
+  D3 s{0.0, 0.0, 0.0};
+#pragma unroll
+  for (int j = 0; j < PS_ITEMS; ++j) {
+    const size_t i = base + j;
+    if (i < n) s = d3add(s, D3{(double)x3[3 * i], (double)x3[3 * i + 1], (double)x3[3 * i + 2]});
+  }
+  D3 total;
+  block_scan_d3(s, &total, ws);
+  if (threadIdx.x == 0) partial[blockIdx.x] = total;
+}
+
+// Exclusive scan of the block partials in one block (sequential chunks of PS_THREADS).
+__global__ void __launch_bounds__(PS_THREADS) k_partial_scan(D3* partial, size_t nb) {
+  __shared__ D3 ws[PS_THREADS / 32];
+  D3 carry{0.0, 0.0, 0.0};
+  for (size_t c0 = 0; c0 < nb; c0 += PS_THREADS) {
+    const size_t i = c0 + threadIdx.x;
+    const D3 v = i < nb ? partial[i] : D3{0.0, 0.0, 0.0};
+    D3 total;
+    const D3 ex = block_scan_d3(v, &total, ws);
+    if (i < nb) partial[i] = d3add(carry, ex);
+    carry = d3add(carry, total);
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(PS_THREADS) k_pos_prefix(const float* __restrict__ x3, size_t n,
+                                                           const D3* __restrict__ partial, double* P) {
+  __shared__ D3 ws[PS_THREADS / 32];
+  const size_t base = (size_t)blockIdx.x * PS_TILE + (size_t)threadIdx.x * PS_ITEMS;
+  D3 v[PS_ITEMS];
+  D3 s{0.0, 0.0, 0.0};
+#pragma unroll
+  for (int j = 0; j < PS_ITEMS; ++j) {
+    const size_t i = base + j;
+    v[j] = i < n ? D3{(double)x3[3 * i], (double)x3[3 * i + 1], (double)x3[3 * i + 2]} : D3{0.0, 0.0, 0.0};
+    s = d3add(s, v[j]);
+  }
+  D3 total;
+  D3 run = d3add(block_scan_d3(s, &total, ws), partial[blockIdx.x]);
+#pragma unroll
+  for (int j = 0; j < PS_ITEMS; ++j) {
+    const size_t i = base + j;
+    if (i <= n) {
+      P[3 * i] = run.x;
+      P[3 * i + 1] = run.y;
+      P[3 * i + 2] = run.z;
+    }
+    run = d3add(run, v[j]);
+  }
+}
+
+__global__ void k_tree_com(const uint4* __restrict__ link, const double* __restrict__ P, float4* mass,
+                           const uint32_t* __restrict__ counters, uint32_t capacity) {
+  uint32_t total = 0;
+  for (int j = 0; j <= KEY_LEVELS; ++j) total += counters[j];
+  total = min(total, capacity);
+  for (uint32_t node = blockIdx.x * blockDim.x + threadIdx.x; node < total; node += gridDim.x * blockDim.x) {
+    const uint4 L = link[node];
+    const double c = (double)(L.y - L.x);
+    const double sx = P[3 * (size_t)L.y] - P[3 * (size_t)L.x];
+    const double sy = P[3 * (size_t)L.y + 1] - P[3 * (size_t)L.x + 1];
+    const double sz = P[3 * (size_t)L.y + 2] - P[3 * (size_t)L.x + 2];
+    mass[node] = make_float4((float)(sx / c), (float)(sy / c), (float)(sz / c), (float)(L.y - L.x));
+  }
+}
+
+cudaError_t tree_build(TreeNodes& t, const uint64_t* sorted_keys, const float* sorted_x3, size_t n, float box,
+                       DevStatus* st, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  const size_t cap = 2 * n + 64;
+  cudaError_t e;
+  if (t.capacity < cap || !t.link.p) {
+    if ((e = ensure(t.geo, cap * sizeof(float4))) != cudaSuccess) return e;
+    if ((e = ensure(t.mass, cap * sizeof(float4))) != cudaSuccess) return e;
+    if ((e = ensure(t.link, cap * sizeof(uint4))) != cudaSuccess) return e;
+    t.capacity = cap;
+  }
+  if ((e = ensure(t.counters, CNT_WORDS * sizeof(uint32_t))) != cudaSuccess) return e;
+  if ((e = ensure(t.prefix, 3 * (n + 1) * sizeof(double))) != cudaSuccess) return e;
+  const size_t nb = (n + 1 + PS_TILE - 1) / PS_TILE;
+  if ((e = ensure(t.scan_tmp, (nb + 1) * sizeof(D3))) != cudaSuccess) return e;
+
+  uint4* link = as<uint4>(t.link);
+  float4* geo = as<float4>(t.geo);
+  uint32_t* counters = as<uint32_t>(t.counters);
+  k_tree_root<<<1, CNT_WORDS, 0, s>>>(link, geo, counters, (uint32_t)n, box / 2.0f);
+  for (int d = 0; d <= KEY_LEVELS; ++d)
+    k_tree_level<<<BUILD_BLOCKS, BUILD_THREADS, 0, s>>>(d, sorted_keys, link, geo, counters, (uint32_t)t.capacity, st);
+
+  D3* partial = as<D3>(t.scan_tmp);
+  double* P = as<double>(t.prefix);
+  k_pos_reduce<<<(unsigned)nb, PS_THREADS, 0, s>>>(sorted_x3, n, partial);
+  k_partial_scan<<<1, PS_THREADS, 0, s>>>(partial, nb);
+  k_pos_prefix<<<(unsigned)nb, PS_THREADS, 0, s>>>(sorted_x3, n, partial, P);
+  k_tree_com<<<BUILD_BLOCKS, BUILD_THREADS, 0, s>>>(link, P, as<float4>(t.mass), counters, (uint32_t)t.capacity);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------------------
+// Walk
+// ---------------------------------------------------------------------------------------------
+constexpr int WALK_WARPS = 4;
+constexpr int WALK_THREADS = WALK_WARPS * 32;
+constexpr int STACK_CAP = 8 * (KEY_LEVELS + 2);
+
+struct WalkParams {
+  float box;
+  float half_box_guard;  // |x| below this: round(x / L) == 0 exactly
+  float r_cut;
+  float cut2;            // r_cut * r_cut
+  float theta;
+  float r_split;
+  float two_rs;          // 2 * r_split
+  float eps2;            // softening^2
+  float k;               // Newtonian coupling
+};
+
+// tree.rs:253-261: d = x - L round(x / L), with x = a - b. For |x| < 0.49 L the quotient rounds
+// to 0 whatever its last bit, so only the remaining cases need the IEEE division.
+__device__ __forceinline__ float min_image1(float a, float b, const WalkParams& w) {
+  const float x = __fsub_rn(a, b);
+  if (fabsf(x) < w.half_box_guard) return x;
+  const float q = roundf(__fdiv_rn(x, w.box));
+  return __fsub_rn(x, __fmul_rn(w.box, q));
+}
+
+__device__ __forceinline__ float norm2(float a, float b, float c) {
+  return __fadd_rn(__fadd_rn(__fmul_rn(a, a), __fmul_rn(b, b)), __fmul_rn(c, c));
+}
+
+// tree.rs:54-66: f = -K m S(r) / (r^2 + eps^2)^{3/2}, S(r) = erfc(u) + (2/sqrt(pi)) u e^{-u^2}, u = r/(2 r_s)
+__device__ __forceinline__ void add_pair(float d0, float d1, float d2, float r2, float mass, const WalkParams& w,
+                                         float& a0, float& a1, float& a2) {
+  const float s = __fadd_rn(r2, w.eps2);
+  const float r = sqrtf(r2);
+  const float u = __fdiv_rn(r, w.two_rs);
+  const float S = __fadd_rn(erfcf(u), __fmul_rn(__fmul_rn(TWO_OVER_SQRT_PI, u), expf(__fmul_rn(-u, u))));
+  const float f = __fdiv_rn(__fmul_rn(__fmul_rn(-w.k, mass), S), __fmul_rn(s, sqrtf(s)));
+  a0 = __fadd_rn(a0, __fmul_rn(d0, f));
+  a1 = __fadd_rn(a1, __fmul_rn(d1, f));
+  a2 = __fadd_rn(a2, __fmul_rn(d2, f));
+}
+
+__global__ void __launch_bounds__(WALK_THREADS) k_tree_walk(const uint4* __restrict__ link,
+                                                            const float4* __restrict__ geo,
+                                                            const float4* __restrict__ mass,
+                                                            const float* __restrict__ x3, size_t n, WalkParams w,
+                                                            float* __restrict__ acc3, int accumulate,
+                                                            unsigned long long* counters, DevStatus* st) {
+  __shared__ uint2 stack[WALK_WARPS][STACK_CAP];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const size_t i = ((size_t)blockIdx.x * WALK_WARPS + warp) * 32 + lane;
+  const bool valid = i < n;
+  const unsigned group = __ballot_sync(0xffffffffu, valid);
+  if (group == 0) return;
+  float x0 = 0.0f, x1 = 0.0f, x2 = 0.0f;
+  if (valid) {
+    x0 = x3[3 * i];
+    x1 = x3[3 * i + 1];
+    x2 = x3[3 * i + 2];
+  }
+  float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
+  unsigned long long n_pairs = 0, n_accepts = 0;
+  uint2* stk = stack[warp];
+  int sp = 0;
+  if (lane == 0) stk[0] = make_uint2(0u, group);
+  sp = 1;
+  __syncwarp();
+  while (sp > 0) {
+    --sp;
+    const uint2 top = stk[sp];
+    __syncwarp();
+    const uint32_t node = top.x;
+    const bool act = (top.y >> lane) & 1u;
+    const float4 G = __ldg(geo + node);
+    bool live = false;
+    if (act) {
+      const float t0 = min_image1(G.x, x0, w), t1 = min_image1(G.y, x1, w), t2 = min_image1(G.z, x2, w);
+      const float max_r = __fadd_rn(w.r_cut, __fmul_rn(SQRT_3, G.w));
+      live = !(norm2(t0, t1, t2) > __fmul_rn(max_r, max_r));
+    }
+    const unsigned live_mask = __ballot_sync(0xffffffffu, live);
+    if (live_mask == 0) continue;
+    const uint4 L = __ldg(link + node);
+    if ((L.w & 1u) == 0u) {
+      // children[0] == NO_CHILD: direct sum over the node's particles (tree.rs:286-298)
+      for (uint32_t b0 = L.x; b0 < L.y; b0 += 32) {
+        const uint32_t j = b0 + lane;
+        float s0 = 0.0f, s1 = 0.0f, s2 = 0.0f;
+        if (j < L.y) {
+          s0 = __ldg(x3 + 3 * (size_t)j);
+          s1 = __ldg(x3 + 3 * (size_t)j + 1);
+          s2 = __ldg(x3 + 3 * (size_t)j + 2);
+        }
+        const int cnt = (int)min(32u, L.y - b0);
+        for (int t = 0; t < cnt; ++t) {
+          const float y0 = __shfl_sync(0xffffffffu, s0, t);
+          const float y1 = __shfl_sync(0xffffffffu, s1, t);
+          const float y2 = __shfl_sync(0xffffffffu, s2, t);
+          if (live && (size_t)(b0 + t) != i) {
+            const float d0 = min_image1(x0, y0, w), d1 = min_image1(x1, y1, w), d2 = min_image1(x2, y2, w);
+            const float r2 = norm2(d0, d1, d2);
+            if (!(r2 > w.cut2)) {
+              add_pair(d0, d1, d2, r2, 1.0f, w, a0, a1, a2);
+              ++n_pairs;
+            }
+          }
+        }
+      }
+    } else {
+      bool open = false;
+      if (live) {
+        const float4 M = __ldg(mass + node);
+        const float t0 = min_image1(M.x, x0, w), t1 = min_image1(M.y, x1, w), t2 = min_image1(M.z, x2, w);
+        const float r2 = norm2(t0, t1, t2);
+        const float r = sqrtf(r2);
+        if (__fmul_rn(2.0f, G.w) < __fmul_rn(w.theta, r)) {
+          add_pair(-t0, -t1, -t2, r2, M.w, w, a0, a1, a2);
+          ++n_accepts;
+        } else {
+          open = true;
+        }
+      }
+      const unsigned open_mask = __ballot_sync(0xffffffffu, open);
+      if (open_mask) {
+        const uint32_t cmask = L.w & 0xFFu;
+        const int nch = __popc(cmask);
+        if (sp + nch > STACK_CAP) {
+          if (lane == 0) dev_fail(st, DEV_STACK_OVERFLOW, (int)node);
+          break;
+        }
+        if (lane < nch) stk[sp + lane] = make_uint2(L.z + (uint32_t)lane, open_mask);
+        sp += nch;
+        __syncwarp();
+      }
+    }
+  }
+  if (valid) {
+    if (accumulate) {
+      acc3[3 * i] = __fadd_rn(acc3[3 * i], a0);
+      acc3[3 * i + 1] = __fadd_rn(acc3[3 * i + 1], a1);
+      acc3[3 * i + 2] = __fadd_rn(acc3[3 * i + 2], a2);
+    } else {
+      acc3[3 * i] = a0;
+      acc3[3 * i + 1] = a1;
+      acc3[3 * i + 2] = a2;
+    }
+  }
+  if (counters) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      n_pairs += __shfl_xor_sync(0xffffffffu, n_pairs, o);
+      n_accepts += __shfl_xor_sync(0xffffffffu, n_accepts, o);
+    }
+    if (lane == 0) {
+      atomicAdd(&counters[0], n_pairs);
+      atomicAdd(&counters[1], n_accepts);
+    }
+  }
+}
+
+void launch_tree_walk(const TreeNodes& t, const float* sorted_x3, size_t n, float box, const cpm_force_split& split,
+                      float k, float* acc3, int accumulate, TreeCounters* counters, DevStatus* st, cudaStream_t s) {
+  if (n == 0) return;
+  WalkParams w;
+  w.box = box;
+  w.half_box_guard = 0.49f * box;
+  w.r_cut = split.r_cut;
+  w.cut2 = split.r_cut * split.r_cut;
+  w.theta = split.theta;
+  w.r_split = split.r_split;
+  w.two_rs = 2.0f * split.r_split;
+  w.eps2 = split.softening * split.softening;
+  w.k = k;
+  const size_t groups = (n + 31) / 32;
+  const unsigned blocks = (unsigned)((groups + WALK_WARPS - 1) / WALK_WARPS);
+  k_tree_walk<<<blocks, WALK_THREADS, 0, s>>>(static_cast<const uint4*>(t.link.p), static_cast<const float4*>(t.geo.p),
+                                              static_cast<const float4*>(t.mass.p), sorted_x3, n, w, acc3, accumulate,
+                                              reinterpret_cast<unsigned long long*>(counters), st);
+}
+
+}  // namespace cpm

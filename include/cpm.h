@@ -1,0 +1,180 @@
+/*
+ * cpm.h — C ABI of libcpm_cuda.so, the B200 (sm_100a) TreePM gravity solve.
+ *
+ * Each entry point replaces one function of the reference crate's CPU path
+ * (BenSmith1202/Cosmological-Particle-Simulation, src/mesh.rs, src/fft.rs,
+ * src/poisson.rs, src/tree.rs, src/integrator.rs); the comment on each
+ * declaration names the reference item (file:line) it stands in for.
+ *
+ * Conventions
+ *  - Positions, momenta and accelerations are AoS f32 triples, exactly the
+ *    memory of a Rust `&[[f32; 3]]` (12-byte stride): pass `as_ptr() as *const f32`.
+ *  - Meshes are n^3 f32 cells indexed (ix*n + iy)*n + iz, z fastest (mesh.rs:11).
+ *  - Complex data is interleaved {re, im} f32, the layout of num_complex's
+ *    `#[repr(C)] Complex<f32>`.
+ *  - Every call that takes host pointers copies to the device, computes, copies
+ *    back and synchronises its context's stream before returning: it behaves like
+ *    the synchronous Rust function it replaces.
+ *  - Every function returns CPM_OK (0) or a negative CPM_E_* code; the text of the
+ *    last error of a context is available from cpm_last_error(). The reference
+ *    panics where these return an error (e.g. poisson.rs:35 asserts the mesh size);
+ *    a Rust shim maps a non-zero code back to panic!.
+ *  - A context is not thread-safe: use one per host thread (the reference calls
+ *    the path from one worker thread, runner.rs:130).
+ */
+#ifndef CPM_H
+#define CPM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status codes */
+#define CPM_OK 0
+#define CPM_E_INVALID (-1)       /* null pointer, zero or negative size, bad enum value */
+#define CPM_E_MESH_MISMATCH (-2) /* mesh size differs from the context's (poisson.rs:35) */
+#define CPM_E_CAPACITY (-3)      /* more particles than the context or simulation holds */
+#define CPM_E_UNSUPPORTED (-4)   /* mesh size whose FFT length this build does not support */
+#define CPM_E_CUDA (-5)          /* a CUDA runtime call failed */
+#define CPM_E_NONFINITE (-6)     /* NaN or infinite input position */
+#define CPM_E_NOMEM (-7)         /* device allocation failed */
+#define CPM_E_DEVICE (-8)        /* a kernel reported an error through its status word */
+#define CPM_E_NO_DEVICE (-9)     /* no CUDA device, or not an sm_100 device */
+
+/* ------------------------------------------------------------------ plain data */
+typedef struct {
+  float re, im;
+} cpm_cf32; /* num_complex::Complex<f32> */
+
+typedef struct {
+  float omega_r, omega_m, omega_l, h0;
+} cpm_cosmology; /* cosmology.rs:9-16 `Cosmology` (pub fields) */
+
+typedef struct {
+  float r_split, r_cut, softening, theta;
+} cpm_force_split; /* tree.rs:21-30 `ForceSplit` */
+
+typedef struct cpm_ctx cpm_ctx;
+typedef struct cpm_sim cpm_sim;
+
+/* ------------------------------------------------------------------ library */
+/* Version string of the library build ("cpm <semver> sm_100a"). */
+const char* cpm_version(void);
+/* Text of the last error recorded on `ctx` (or of the last context-free failure when ctx is NULL). */
+const char* cpm_last_error(const cpm_ctx* ctx);
+
+/* ------------------------------------------------------------------ context (fine-grained API) */
+/* Creates a context for meshes of n_mesh^3 cells in a periodic box of side `box_size`, with device
+ * buffers for up to `max_particles` particles (they grow on demand). Owns one CUDA stream.
+ * Replaces the state that `PoissonSolver::new(n, L)` (poisson.rs:23) and `Mesh::new(n, L)`
+ * (mesh.rs:16) set up. flags: 0. */
+int cpm_ctx_create(int n_mesh, float box_size, size_t max_particles, uint32_t flags, cpm_ctx** out);
+int cpm_ctx_destroy(cpm_ctx* ctx);
+
+/* mesh.rs:62-69 `Mesh::deposit(&mut self, positions, mass)`: clears `cells_out` (n^3) and deposits
+ * `mass` per particle with CIC weights. Accumulates in 64-bit fixed point, so the result does not
+ * depend on particle order and is the exactly-rounded sum of the reference's f32 weights. */
+int cpm_mesh_deposit(cpm_ctx* ctx, const float* x3, size_t n, float mass, float* cells_out);
+
+/* integrator.rs:117-126 `Simulation::density_contrast`: deposit of unit masses, then
+ * delta = c / (N / n^3) - 1 in f32. */
+int cpm_density_contrast(cpm_ctx* ctx, const float* x3, size_t n, float* delta_out);
+
+/* mesh.rs:72-77 `Mesh::interpolate`, batched over n positions: out[i] = sum of the 8 CIC
+ * products in the reference's stencil order (bit-identical to the reference's f32 arithmetic). */
+int cpm_mesh_interpolate(cpm_ctx* ctx, const float* cells, const float* x3, size_t n, float* out);
+
+/* integrator.rs:144-148: the three components of the PM force at n positions from the meshes
+ * returned by cpm_poisson_accel, one stencil per particle; out3 is AoS [n][3]. */
+int cpm_mesh_interpolate3(cpm_ctx* ctx, const float* gx, const float* gy, const float* gz, const float* x3,
+                          size_t n, float* out3);
+
+/* fft.rs:28-33 `Fft3::forward` / `Fft3::inverse`: unnormalised in-place c2c transform of n^3
+ * complex values (forward e^{-ikx}, inverse e^{+ikx}). n must equal the context's mesh size. */
+int cpm_fft3(cpm_ctx* ctx, cpm_cf32* data, int n, int inverse);
+
+/* fft.rs:86-95 `wavenumber(i, n, L)` (host function; Nyquist index of an even grid -> 0). */
+float cpm_wavenumber(size_t i, size_t n, float box_size);
+
+/* poisson.rs:33-88 `PoissonSolver::acceleration(&delta, &cosmo, a, r_split) -> [Mesh; 3]`:
+ * g = -grad phi with phi_k = -(3/2) Omega_m delta_k / (a k^2) exp(-k^2 r_split^2); k = 0 dropped.
+ * delta, gx, gy, gz are n^3 meshes. Returns CPM_E_MESH_MISMATCH when n differs from the context. */
+int cpm_poisson_accel(cpm_ctx* ctx, const float* delta, int n, const cpm_cosmology* cosmo, float a, float r_split,
+                      float* gx, float* gy, float* gz);
+
+/* tree.rs:40-50 `ForceSplit::with(L, mesh_n, particles_per_side, softening_scale, theta)` (host). */
+cpm_force_split cpm_force_split_with(float box_size, size_t mesh_n, size_t particles_per_side,
+                                     float softening_scale, float theta);
+
+/* tree.rs:54-57 `short_range_factor(r, r_split)` (host, f32). */
+float cpm_short_range_factor(float r, float r_split);
+
+/* tree.rs:314-323 `tree::accelerations(positions, L, &split, k) -> Vec<[f32; 3]>`: builds the
+ * octree of tree.rs:171-250 from octant keys and walks it on the GPU with the reference's rules
+ * (prune by r_cut + sqrt(3) half, direct sum when octant 0 is empty, 2 half < theta r opening). */
+int cpm_tree_accel(cpm_ctx* ctx, const float* x3, size_t n, float box_size, const cpm_force_split* split, float k,
+                   float* acc3);
+
+/* The octant keys of the tree descent (tree.rs:186-250: digit d is (x>=cx)|(y>=cy)<<1|(z>=cz)<<2 at
+ * depth d-1, with the same f32 centre arithmetic; `levels` <= 21 digits, first digit most
+ * significant) and the stable ascending sort permutation of those keys. Either output may be NULL.
+ * The reference has no such entry point: it is the sort the tree build runs on. */
+int cpm_octant_keys(cpm_ctx* ctx, const float* x3, size_t n, float box_size, int levels, uint64_t* keys_out,
+                    uint32_t* perm_out);
+
+/* Tree statistics of the last cpm_tree_accel on this context: node count, leaf-pair and
+ * accepted-node interaction counts, maximum depth. Any pointer may be NULL. */
+int cpm_tree_stats(cpm_ctx* ctx, uint64_t* nodes, uint64_t* leaf_pairs, uint64_t* node_accepts, uint32_t* max_depth);
+
+/* ------------------------------------------------------------------ device-resident simulation */
+/* Replaces `Simulation` (integrator.rs:34-186) under a `cuda` feature: state stays in HBM and
+ * `step_to` runs one KDK step (kick, drift, deposit, FFT-Poisson, gather, tree build and walk,
+ * kick) as one CUDA graph. */
+typedef struct {
+  cpm_cosmology cosmo;
+  float box_size;
+  int mesh_n;
+  size_t n_particles;
+  int use_tree;           /* 0: pure PM (split == None); 1: TreePM with `split` */
+  cpm_force_split split;
+  uint32_t flags;         /* CPM_SIM_* below */
+} cpm_sim_params;
+
+/* Positions as uint32 fixed point (x = q L / 2^32) so the periodic wrap of the drift is exact.
+ * Precision mode; the default f32 mode is the reference's arithmetic. */
+#define CPM_SIM_FIXED_POINT 0x1u
+/* Divide the PM Green's function by the CIC window squared (the reference does not). */
+#define CPM_SIM_DECONVOLVE 0x2u
+/* Record per-phase CUDA-event timings for cpm_sim_phase_times(). */
+#define CPM_SIM_TIMING 0x4u
+/* Run the step without CUDA-graph capture (each kernel launched directly). */
+#define CPM_SIM_NO_GRAPH 0x8u
+
+/* integrator.rs:54-79 `Simulation::new`: uploads x3, p3 (AoS [n][3]) and computes the initial
+ * acceleration at a0. */
+int cpm_sim_create(const cpm_sim_params* params, const float* x3, const float* p3, float a0, cpm_sim** out);
+/* integrator.rs:174-186 `Simulation::step_to(a1)`. Kick and drift factors are the reference's f32
+ * Simpson/bisection values (integrator.rs:263-297), computed on the host. */
+int cpm_sim_step_to(cpm_sim* sim, float a1);
+/* Reads the state in the caller's particle order. Any pointer may be NULL. delta is n^3. */
+int cpm_sim_get_state(cpm_sim* sim, float* x3, float* p3, float* acc3, float* delta, float* a);
+/* Overwrites positions and momenta (caller's order) and recomputes the acceleration at the current a. */
+int cpm_sim_set_state(cpm_sim* sim, const float* x3, const float* p3);
+/* Average device milliseconds per step of each phase since the last reset (needs CPM_SIM_TIMING):
+ * [0] kick+drift, [1] keys+sort+reorder, [2] deposit, [3] FFT-Poisson, [4] gather, [5] tree build,
+ * [6] tree walk, [7] whole step. Also the number of steps averaged. */
+int cpm_sim_phase_times(cpm_sim* sim, double* ms8, uint64_t* steps, int reset);
+/* Device-side counters of the last step: nodes, leaf pairs, accepted nodes, kernels launched per step. */
+int cpm_sim_counters(cpm_sim* sim, uint64_t* nodes, uint64_t* leaf_pairs, uint64_t* node_accepts,
+                     uint32_t* launches_per_step);
+/* The CUDA stream the simulation launches on (cudaStream_t), for callers that time with events. */
+void* cpm_sim_stream(cpm_sim* sim);
+int cpm_sim_destroy(cpm_sim* sim);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CPM_H */

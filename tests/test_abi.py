@@ -1,0 +1,63 @@
+"""CPU-only checks of the C ABI: the library builds, loads, exports every symbol include/cpm.h
+declares, and its host-only functions agree bit for bit with the oracle. No GPU compute here."""
+import ctypes as C
+import subprocess
+
+import numpy as np
+import pytest
+
+
+@pytest.fixture(scope="module")
+def native(cpm):
+    from importlib import import_module
+    nat = import_module("cosmological-particle-simulation_b200._native")
+    if not nat.LIB_PATH.exists():
+        import_module("cosmological-particle-simulation_b200.build").build()
+    return nat
+
+
+def test_library_exports_every_declared_symbol(native):
+    names = native.exported_symbols()
+    assert len(names) >= 20
+    raw = C.CDLL(str(native.LIB_PATH))
+    missing = [n for n in names if not hasattr(raw, n)]
+    assert not missing, missing
+    out = subprocess.run(["nm", "-D", "--defined-only", str(native.LIB_PATH)], capture_output=True, text=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if " T " in line}
+    assert set(names) <= exported
+
+
+def test_library_targets_sm100a(native):
+    out = subprocess.run(["cuobjdump", "--list-elf", str(native.LIB_PATH)], capture_output=True, text=True)
+    assert out.returncode == 0 and "sm_100a" in out.stdout
+
+
+def test_version_string(native):
+    assert native.lib().cpm_version().decode().startswith("cpm ")
+
+
+def test_host_wavenumber_bit_exact(native, orc):
+    for n in (4, 7, 16, 64, 512):
+        for i in range(n):
+            assert native.lib().cpm_wavenumber(i, n, 64.0) == orc.wavenumber(i, n, 64.0)
+
+
+def test_host_force_split_bit_exact(native, orc):
+    for args in [(64.0, 64, 32, 1 / 30, 0.5), (256.0, 512, 256, 1 / 30, 0.5), (100.0, 80, 40, 0.05, 0.5)]:
+        a = native.lib().cpm_force_split_with(*args)
+        b = orc.split_with(*args)
+        assert (a.r_split, a.r_cut, a.softening, a.theta) == (b.r_split, b.r_cut, b.softening, b.theta)
+
+
+def test_host_short_range_factor_bit_exact(native, orc):
+    for r in np.linspace(0.0, 6.0, 301, dtype=np.float32):
+        assert native.lib().cpm_short_range_factor(float(r), 0.7) == orc.short_range_factor(float(r), 0.7)
+
+
+def test_invalid_arguments_fail_without_a_device(native):
+    h = C.c_void_p()
+    rc = native.lib().cpm_ctx_create(0, 1.0, 0, 0, C.byref(h))
+    assert rc == -1 and h.value is None
+    assert "n_mesh" in native.last_error()
+    assert native.lib().cpm_ctx_create(8, 1.0, 0, 0, None) == -1
+    assert native.lib().cpm_mesh_deposit(None, None, 0, 1.0, None) == -1

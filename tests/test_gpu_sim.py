@@ -1,0 +1,135 @@
+"""GPU parity of the device-resident simulation (integrator.rs:34-186) against the oracle, and the
+reference's integrator tests (integrator.rs:368-461) run on the GPU path."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_rms(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.sqrt(((a - b) ** 2).sum() / max((b ** 2).sum(), 1e-300)))
+
+
+def periodic_max_diff(a, b, box):
+    d = np.abs(a.astype(np.float64) - b)
+    return float(np.minimum(d, box - d).max())
+
+
+def _plane_wave(orc, n, box, amp, cosmo, a_init):
+    f32 = np.float32
+    k = f32(f32(2.0) * f32(np.pi)) / f32(box)
+    h = f32(box) / f32(n)
+    d = f32(orc.growth(cosmo, a_init))
+    f = f32(orc.growth_rate(cosmo, a_init))
+    e = f32(orc.cosmo_e(cosmo, a_init))
+    a = f32(a_init)
+    i = np.arange(n, dtype=np.float32) * h
+    qx, qy, qz = (v.ravel() for v in np.meshgrid(i, i, i, indexing="ij"))
+    psi_x = (-(f32(amp) / k) * np.sin(k * qx).astype(np.float32)).astype(np.float32)
+    x = np.mod(qx + d * psi_x, f32(box)).astype(np.float32)
+    pos = np.stack([x, qy, qz], 1).astype(np.float32)
+    mom = np.zeros_like(pos)
+    mom[:, 0] = (a * a * f * e * d) * psi_x
+    return pos, mom
+
+
+def _ics(orc, n, box, a_init, seed):
+    """Zel'dovich ICs of the config cosmology (Omega_m 0.3, h 0.7, sigma8 0.8, n_s 0.96)."""
+    c = orc.cosmology(0.0, 0.3, 0.7, 70.0)
+    ps = orc.power_normalized(c, 0.96, 0.8, 8.0)
+    x, p = orc.zeldovich(n, box, c, ps, a_init, seed)
+    return c, x, p
+
+
+def test_pm_step_matches_oracle_bit_for_bit_kick_drift(cpm, orc):
+    """PM only: the initial force within 1e-5 RMS, and after 3 steps positions within 1e-5 L."""
+    c, x, p = _ics(orc, 16, 64.0, 0.02, 42)
+    cc = cpm.Cosmology(c.omega_r, c.omega_m, c.omega_l, c.h0)
+    gpu = cpm.Simulation(cc, 64.0, 32, x, p, 0.02, None)
+    ref = orc.Simulation(c, 64.0, 32, x, p, 0.02, None)
+    assert rel_rms(gpu.state()["acc"], ref.state()["acc"]) < 1e-5
+    for a1 in cpm.ln_a_schedule(0.02, 0.05, 3):
+        gpu.step_to(a1)
+        ref.step_to(a1)
+    g, r = gpu.state(), ref.state()
+    assert g["a"] == r["a"]
+    assert periodic_max_diff(g["x"], r["x"], 64.0) < 1e-5 * 64.0
+    assert rel_rms(g["acc"], r["acc"]) < 1e-5
+
+
+def test_treepm_accelerations_match_oracle(cpm, orc):
+    """TreePM force at the ICs and after 2 steps: within 1e-5 relative RMS (config-1 cosmology)."""
+    n, box, mesh = 16, 32.0, 32
+    c, x, p = _ics(orc, n, box, 0.02, 42)
+    split = orc.split_with(box, mesh, n, 1.0 / 30.0, 0.5)
+    cc = cpm.Cosmology(c.omega_r, c.omega_m, c.omega_l, c.h0)
+    cs = cpm.ForceSplit(split.r_split, split.r_cut, split.softening, split.theta)
+    gpu = cpm.Simulation(cc, box, mesh, x, p, 0.02, cs)
+    ref = orc.Simulation(c, box, mesh, x, p, 0.02, split)
+    assert rel_rms(gpu.state()["acc"], ref.state()["acc"]) < 1e-5
+    for a1 in cpm.ln_a_schedule(0.02, 0.2, 8)[:2]:
+        gpu.step_to(a1)
+        ref.step_to(a1)
+    g, r = gpu.state(want_delta=True), ref.state(want_delta=True)
+    assert periodic_max_diff(g["x"], r["x"], box) < 1e-5 * box
+    assert rel_rms(g["acc"], r["acc"]) < 1e-5
+    assert rel_rms(g["delta"] + 1.0, r["delta"] + 1.0) < 1e-6
+
+
+def test_linear_growth_matches_growth_factor(cpm, orc):
+    """integrator.rs:368-388 on the GPU."""
+    box, cosmo = 1.0, orc.lcdm_default()
+    a_init, a_final = 0.02, 0.1
+    x, p = _plane_wave(orc, 32, box, 0.5, cosmo, a_init)
+    sim = cpm.Simulation(cpm.Cosmology.lcdm_default(), box, 32, x, p, a_init, None)
+
+    def mode(xs):
+        d = orc.density_contrast(32, box, xs).reshape(32, 32, 32).astype(np.float64)
+        cx = np.cos((np.arange(32) + 0.5) * (box / 32) * 2 * np.pi / box)
+        return 2.0 * float((d * cx[:, None, None]).sum()) / 32 ** 3
+
+    before = mode(x)
+    for a1 in cpm.ln_a_schedule(a_init, a_final, 40):
+        sim.step_to(a1)
+    after = mode(sim.positions)
+    expected = orc.growth(cosmo, a_final) / orc.growth(cosmo, a_init)
+    assert abs(after / before - expected) / expected < 0.01
+
+
+def test_total_momentum_stays_near_zero(cpm, orc):
+    """integrator.rs:417-435 on the GPU."""
+    x, p = _plane_wave(orc, 16, 1.0, 0.5, orc.lcdm_default(), 0.02)
+    sim = cpm.Simulation(cpm.Cosmology.lcdm_default(), 1.0, 32, x, p, 0.02, None)
+    for a1 in cpm.ln_a_schedule(0.02, 0.1, 20):
+        sim.step_to(a1)
+    mom = sim.momenta.astype(np.float64)
+    assert np.all(np.abs(mom.sum(0)) < 1e-3 * np.abs(mom[:, 0]).sum())
+
+
+def test_treepm_pair_force_matches_newton(cpm, orc):
+    """integrator.rs:437-461 on the GPU."""
+    box, mesh_n = 100.0, 64
+    std = cpm.ForceSplit.with_(box, mesh_n, 2, 0.05, 0.5)
+    split = cpm.ForceSplit(std.r_split, std.r_cut, 0.01, std.theta)
+    pos = np.array([[50.0, 50.0, 50.0], [53.0, 50.0, 50.0]], np.float32)
+    cosmo = cpm.Cosmology.lcdm_default()
+    sim = cpm.Simulation(cosmo, box, mesh_n, pos, np.zeros_like(pos), 1.0, split)
+    acc = sim.state()["acc"]
+    f32 = np.float32
+    k = f32(1.5) * f32(cosmo.omega_m) * f32(box) ** 3 / (f32(4.0) * f32(np.pi) * f32(1.0) * f32(2.0))
+    newton = float(k / f32(9.0))
+    assert acc[0, 0] > 0.0 and acc[1, 0] < 0.0
+    assert abs(acc[0, 0] - newton) / newton < 0.05 and abs(acc[1, 0] + newton) / newton < 0.05
+
+
+def test_sim_rejects_bad_arguments(cpm):
+    x = np.zeros((8, 3), np.float32)
+    with pytest.raises(cpm.CpmError) as e:
+        cpm.Simulation(cpm.Cosmology.lcdm_default(), 1.0, 12, x, x, 0.1, None)
+    assert e.value.code == -4
+    x[3, 0] = np.inf
+    with pytest.raises(cpm.CpmError) as e:
+        cpm.Simulation(cpm.Cosmology.lcdm_default(), 1.0, 8, x, np.zeros_like(x), 0.1, None)
+    assert e.value.code == -6
