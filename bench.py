@@ -1,0 +1,382 @@
+#!/usr/bin/env python
+"""Throughput of the TreePM step in particle-steps/s on B200s (one JSON line on rank 0).
+
+Workload (default): 256^3 = 16,777,216 particles in a periodic 256 Mpc/h box with a 512^3 PM
+mesh; Zel'dovich ICs at z = 49 (a = 0.02) from a seed-7 Gaussian field with a BBKS spectrum
+(Omega_m 0.3, Omega_L 0.7, h 0.7, sigma8 0.8, n_s 0.96); r_s = 1.25 cells, r_cut = 4.5 r_s,
+theta = 0.5, Plummer softening 1/30 of the mean spacing; KDK steps on the 128-step schedule
+uniform in ln a to z = 0. A "step" is one KDK step of that schedule: the first W are warm-up, the
+next K are timed. Inputs are generated on the GPU (synthetic, no dataset).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`value` is device time (CUDA events on the simulation's stream, max over ranks) with the state
+resident in HBM; `e2e` is the same metric through the host-buffer C-ABI step (cpm_sim_step_host:
+positions and momenta copied host->device and back every step). `--impl reference` times the
+CPU restatement of the reference path (oracle/) on this host's cores.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+PKG = "cosmological-particle-simulation_b200"
+
+WORKLOADS = {
+    # BASELINE configuration at scale: 256^3 particles, 512^3 mesh, 256 Mpc/h, seed 7, 128 steps.
+    "treepm-256": dict(n_side=256, mesh=512, box=256.0, seed=7, steps_total=128),
+    # the reference's CPU-runnable case: 32^3 particles, 64^3 mesh, 64 Mpc/h, seed 42, 64 steps.
+    "treepm-32": dict(n_side=32, mesh=64, box=64.0, seed=42, steps_total=64),
+}
+COSMO = dict(omega_r=0.0, omega_m=0.3, omega_l=0.7, h0=70.0)
+N_S, SIGMA8, A_INIT, A_END, THETA, SOFT = 0.96, 0.8, 0.02, 1.0, 0.5, 1.0 / 30.0
+
+
+def pm_bytes_per_step(n: int, mesh: int) -> int:
+    """Algorithmic HBM bytes of the PM kernels per step: deposit 12N + 4M, R2C 4M + 4M, k-space
+    4M + 12M, 3 C2R 12M + 12M, gather 12M + 24N  =>  36N + 64M."""
+    m = mesh ** 3
+    return 36 * n + 64 * m
+
+
+def schedule(steps_total: int, count: int) -> list[float]:
+    """runner.rs:240: a_i = a0 (a_end / a0)^(i / steps), i = 1..count (continues past a_end if asked)."""
+    a0, ratio = np.float32(A_INIT), np.float32(np.float32(A_END) / np.float32(A_INIT))
+    return [float(np.float32(a0 * np.float32(np.power(ratio, np.float32(np.float32(i) / np.float32(steps_total)),
+                                                      dtype=np.float32))))
+            for i in range(1, count + 1)]
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+        self.t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.t:
+            self.t.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except (KeyError, ValueError):
+            pass
+    return 6650.0, "fallback"
+
+
+def ncu_traffic() -> dict | None:
+    """Per-launch DRAM bytes of the PM kernels from the committed ncu summary, when present."""
+    p = ROOT / "profiles" / "traffic.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text())
+        except ValueError:
+            return None
+    return None
+
+
+# ------------------------------------------------------------------------------------------ ours
+
+def run_ours(args, rank: int, world: int, dist) -> dict | None:
+    import torch
+
+    cpm = importlib.import_module(PKG)
+    wl = WORKLOADS[args.workload]
+    n_side, mesh, box = wl["n_side"], wl["mesh"], wl["box"]
+    n = n_side ** 3
+    cosmo = cpm.Cosmology(**COSMO)
+    split = cpm.ForceSplit.with_(box, mesh, n_side, SOFT, THETA)
+    sched = schedule(wl["steps_total"], args.warmup + args.steps)
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+
+    sim = cpm.Simulation.from_zeldovich(cosmo, box, mesh, n_side, N_S, SIGMA8, A_INIT, wl["seed"] + rank, split,
+                                        flags=cpm._native.SIM_TIMING)
+    stream = torch.cuda.ExternalStream(sim.stream())
+    for a1 in sched[:args.warmup]:
+        sim.step_to(a1)
+    snapshots = {}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        st = sim.state()
+        snapshots["start"] = (st["x"], st["p"], st["acc"], sched[args.warmup - 1] if args.warmup else A_INIT)
+    sim.phase_times(reset=True)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(dev.index)
+    clocks.start()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for a1 in sched[args.warmup:]:
+        sim.step_to(a1)
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms_local = t_start.elapsed_time(t_end)
+    if dist:
+        dist.barrier()
+        t = torch.tensor([ms_local], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    else:
+        ms = ms_local
+    phases, nsteps = sim.phase_times()
+    counters = sim.counters()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        st = sim.state()
+        snapshots["end"] = (st["x"], st["p"], st["acc"], sched[-1])
+
+    # End to end through the host-buffer C-ABI step, same schedule window, on a fresh simulation.
+    e2e = None
+    if not args.no_e2e:
+        sim.close()
+        sim2 = cpm.Simulation.from_zeldovich(cosmo, box, mesh, n_side, N_S, SIGMA8, A_INIT, wl["seed"] + rank, split)
+        for a1 in sched[:args.warmup]:
+            sim2.step_to(a1)
+        xs = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
+        ps = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
+        st = sim2.state()
+        xs.numpy()[:] = st["x"]
+        ps.numpy()[:] = st["p"]
+        xh, ph = xs.numpy(), ps.numpy()
+        e2e_steps = sched[args.warmup:args.warmup + args.e2e_steps] if args.e2e_steps else sched[args.warmup:]
+        s2 = torch.cuda.ExternalStream(sim2.stream())
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(s2)
+        for a1 in e2e_steps:
+            sim2.step_host(a1, xh, ph)
+        e1.record(s2)
+        torch.cuda.synchronize()
+        ems = e0.elapsed_time(e1)
+        if dist:
+            t = torch.tensor([ems], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        sim2.close()
+        e2e = {"value": n * world * len(e2e_steps) / (ems / 1e3), "unit": "particle-steps/s",
+               "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": 24 * n, "steps": len(e2e_steps),
+               "api": "cpm_sim_step_host (pinned host x, p in/out each step)"}
+    else:
+        sim.close()
+
+    if rank != 0:
+        return None
+    peak, peak_kind = measured_peaks()
+    pm_ms = phases[2] + phases[3] + phases[4]  # deposit, FFT-Poisson, gather
+    pm_b = pm_bytes_per_step(n, mesh)
+    achieved = pm_b / (pm_ms / 1e3) / 1e9 if pm_ms > 0 else 0.0
+    traffic = ncu_traffic()
+    phase_names = ["kick_drift", "keys_sort_reorder", "deposit", "fft_poisson", "gather", "tree_build",
+                   "tree_walk_kick2", "step"]
+    line = {
+        "metric": "particle-steps/s", "value": n * world * args.steps / (ms / 1e3), "unit": "particle-steps/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (Zel'dovich ICs generated on the GPU, Philox white noise)",
+        "config": {"workload": f"TreePM {n_side}^3 particles, {mesh}^3 mesh, L={box:g} Mpc/h, seed {wl['seed']}"
+                               f"{'+rank' if world > 1 else ''}, theta={THETA}, a={A_INIT}->{A_END} in "
+                               f"{wl['steps_total']} ln-a steps; timed steps {args.warmup + 1}..{args.warmup + args.steps}"
+                               f" (a={sched[args.warmup]:.4f}..{sched[-1]:.4f})",
+                   "particles_per_gpu": n, "mesh": mesh, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (positions 201 MB, meshes 537 MB each)"},
+        "roofline": {"bound": "hbm", "kernels": "PM: deposit + FFT-Poisson + gather",
+                     "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                     "peak_kind": peak_kind, "algorithmic_bytes_per_step": pm_b,
+                     "traffic": traffic.get("pm_bytes_per_step") if traffic else None},
+        "phase_ms": {k: round(v, 4) for k, v in zip(phase_names, phases)},
+        "phase_steps": nsteps,
+        "tree": {"nodes_last_step": counters["nodes"], "leaf_pairs_last_step": counters["leaf_pairs"],
+                 "node_accepts_last_step": counters["node_accepts"]},
+        "gpu_launches": counters["launches_per_step"] * args.steps,
+        "launches_per_step": counters["launches_per_step"],
+        "clocks": clk,
+        "e2e": e2e,
+    }
+    if snapshots:
+        line["cpu_baseline"] = cpu_baseline(args, snapshots, wl, n)
+    return line
+
+
+def cpu_baseline(args, snapshots: dict, wl: dict, n: int) -> dict:
+    """The oracle (CPU restatement of the reference path, OpenMP on all host cores) timed on one
+    sampled KDK step at the start and at the end of the timed window, from the GPU run's state:
+    every phase on all particles, the tree walk on a random subset scaled to all particles."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as orc
+
+    cores = os.cpu_count() or 1
+    c = orc.cosmology(COSMO["omega_r"], COSMO["omega_m"], COSMO["omega_l"], COSMO["h0"])
+    split = orc.split_with(wl["box"], wl["mesh"], wl["n_side"], SOFT, THETA)
+    frac = args.cpu_walk_fraction
+    rng = np.random.default_rng(0)
+    m = max(1024, int(n * frac))
+    subset = np.sort(rng.choice(n, size=min(m, n), replace=False)).astype(np.uint32)
+    per_step, detail = [], {}
+    for name, (x, p, acc, a0) in snapshots.items():
+        a1 = float(np.float32(a0 * 1.02))
+        t = orc.step_sample(c, wl["box"], wl["mesh"], x, p, acc, a0, a1, split, subset, threads=cores)
+        est = float(t[:5].sum() + t[5] * (n / len(subset)) + t[6])
+        per_step.append(est)
+        detail[name] = {"a": a0, "s_per_step_est": round(est, 3), "phases_s": [round(float(v), 3) for v in t]}
+    mean_step = sum(per_step) / len(per_step)
+    return {"value": n / mean_step, "unit": "particle-steps/s", "cores": cores, "kind": "port",
+            "sample": (f"one oracle KDK step at the start (a={snapshots['start'][3]:.4f}) and end "
+                       f"(a={snapshots['end'][3]:.4f}) of the timed window, from the GPU state; all phases on all "
+                       f"{n} particles except the tree walk, run for a random {len(subset)} ({frac:.4g}) and scaled; "
+                       f"value = N / mean estimated step time"),
+           "detail": detail}
+
+
+# ------------------------------------------------------------------------------------- reference
+
+def run_reference(args, rank: int, world: int) -> dict | None:
+    """The CPU restatement of the reference path (oracle/, OpenMP on all cores), full KDK steps on
+    the same workload from its Zel'dovich ICs (oracle IC generator, same spectrum and seed), timed
+    by wall clock; steps stop once the time budget is spent (at least one)."""
+    if rank != 0:
+        return None
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as orc
+
+    wl = WORKLOADS[args.workload]
+    n_side, mesh, box = wl["n_side"], wl["mesh"], wl["box"]
+    n = n_side ** 3
+    cores = os.cpu_count() or 1
+    os.environ["OMP_NUM_THREADS"] = str(cores)
+    c = orc.cosmology(COSMO["omega_r"], COSMO["omega_m"], COSMO["omega_l"], COSMO["h0"])
+    ps = orc.power_normalized(c, N_S, SIGMA8, 8.0)
+    x, p = orc.zeldovich(n_side, box, c, ps, A_INIT, wl["seed"])
+    split = orc.split_with(box, mesh, n_side, SOFT, THETA)
+    sim = orc.Simulation(c, box, mesh, x, p, A_INIT, split)
+    sched = schedule(wl["steps_total"], max(args.steps, 1) + 1)
+    t0 = time.perf_counter()
+    done = 0
+    for a1 in sched[:args.steps]:
+        sim.step_to(a1)
+        done += 1
+        if time.perf_counter() - t0 > args.ref_budget_s:
+            break
+    wall = time.perf_counter() - t0
+    sim.close()
+    value = n * done / wall
+    sample = (f"{done} full oracle KDK steps (of {args.steps} requested; time budget {args.ref_budget_s:.0f} s) "
+              f"from the z=49 ICs, all {n} particles, {cores} OpenMP threads")
+    return {
+        "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": done,
+        "warmup": 0, "ms_per_step": wall * 1e3 / done, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (Zel'dovich ICs from the oracle IC generator)",
+        "config": {"workload": f"TreePM {n_side}^3 particles, {mesh}^3 mesh, L={box:g} Mpc/h, seed {wl['seed']}, "
+                               f"theta={THETA}; steps from a={A_INIT}"},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=125)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="treepm-256")
+    ap.add_argument("--e2e-steps", type=int, default=0, help="steps in the end-to-end run (0 = same as --steps)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-walk-fraction", type=float, default=1.0 / 64.0)
+    ap.add_argument("--ref-budget-s", type=float, default=120.0)
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        ap.error("--warmup must be >= 3")
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if args.impl == "reference":
+        line = run_reference(args, rank, world)
+    else:
+        if world > 1:
+            import torch
+            import torch.distributed as tdist
+            from datetime import timedelta
+            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+            tdist.init_process_group("nccl", timeout=timedelta(seconds=600))
+            dist = tdist
+        line = run_ours(args, rank, world, dist)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -99,8 +99,11 @@ def lib() -> C.CDLL:
         "cpm_tree_accel": (i, [vp, vp, sz, fl, C.POINTER(ForceSplitC), fl, vp]),
         "cpm_octant_keys": (i, [vp, vp, sz, fl, i, vp, vp]),
         "cpm_tree_stats": (i, [vp, C.POINTER(u64), C.POINTER(u64), C.POINTER(u64), C.POINTER(u32)]),
+        "cpm_ics_zeldovich": (i, [i, fl, C.POINTER(Cosmology), fl, fl, fl, u64, vp, vp]),
         "cpm_sim_create": (i, [C.POINTER(SimParams), vp, vp, fl, C.POINTER(vp)]),
+        "cpm_sim_create_zeldovich": (i, [C.POINTER(SimParams), i, fl, fl, fl, u64, C.POINTER(vp)]),
         "cpm_sim_step_to": (i, [vp, fl]),
+        "cpm_sim_step_host": (i, [vp, fl, vp, vp]),
         "cpm_sim_get_state": (i, [vp, vp, vp, vp, vp, C.POINTER(fl)]),
         "cpm_sim_set_state": (i, [vp, vp, vp]),
         "cpm_sim_phase_times": (i, [vp, vp, C.POINTER(u64), i]),

@@ -215,6 +215,30 @@ def ln_a_schedule(a_start: float, a_end: float, steps: int) -> list[float]:
             for i in range(1, steps + 1)]
 
 
+def zeldovich(n: int, box_size: float, cosmo: Cosmology, n_s: float, sigma8: float, a_init: float,
+              seed: int) -> tuple[np.ndarray, np.ndarray]:
+    """ics.rs:119-182 `zeldovich` with `PowerSpectrum::normalized(cosmo, n_s, sigma8, 8)`, on the GPU.
+    Returns positions and momenta, (n^3, 3) each, in lattice order."""
+    x = np.empty((n ** 3, 3), np.float32)
+    p = np.empty((n ** 3, 3), np.float32)
+    check(nat.lib().cpm_ics_zeldovich(int(n), float(box_size), C.byref(cosmo), float(n_s), float(sigma8),
+                                      float(a_init), int(seed), ptr(x), ptr(p)), sim=True)
+    return x, p
+
+
+def _sim_params(cosmo, box_size, mesh_n, n_particles, split, flags) -> nat.SimParams:
+    prm = nat.SimParams()
+    prm.cosmo = cosmo
+    prm.box_size = float(box_size)
+    prm.mesh_n = int(mesh_n)
+    prm.n_particles = int(n_particles)
+    prm.use_tree = 1 if split is not None else 0
+    if split is not None:
+        prm.split = split.as_c()
+    prm.flags = int(flags)
+    return prm
+
+
 class Simulation:
     """integrator.rs:34-186 `Simulation`, with the state resident on the GPU.
 
@@ -222,32 +246,46 @@ class Simulation:
     """
 
     def __init__(self, cosmo: Cosmology, box_size: float, mesh_n: int, positions, momenta, a: float,
-                 split: ForceSplit | None, flags: int = 0):
-        x = f32c(positions).reshape(-1, 3)
-        p = f32c(momenta).reshape(-1, 3)
-        if x.shape != p.shape:
-            raise CpmError(-1, "positions and momenta must have the same shape")
-        prm = nat.SimParams()
-        prm.cosmo = cosmo
-        prm.box_size = float(box_size)
-        prm.mesh_n = int(mesh_n)
-        prm.n_particles = len(x)
-        prm.use_tree = 1 if split is not None else 0
-        if split is not None:
-            prm.split = split.as_c()
-        prm.flags = int(flags)
-        h = C.c_void_p()
-        check(nat.lib().cpm_sim_create(C.byref(prm), ptr(x), ptr(p), float(a), C.byref(h)), sim=True)
+                 split: ForceSplit | None, flags: int = 0, _handle=None, _n: int = 0):
+        if _handle is None:
+            x = f32c(positions).reshape(-1, 3)
+            p = f32c(momenta).reshape(-1, 3)
+            if x.shape != p.shape:
+                raise CpmError(-1, "positions and momenta must have the same shape")
+            prm = _sim_params(cosmo, box_size, mesh_n, len(x), split, flags)
+            h = C.c_void_p()
+            check(nat.lib().cpm_sim_create(C.byref(prm), ptr(x), ptr(p), float(a), C.byref(h)), sim=True)
+            _n = len(x)
+        else:
+            h = _handle
         self.h = h
-        self.n = len(x)
+        self.n = int(_n)
         self.mesh_n = int(mesh_n)
         self.box_size = float(box_size)
         self.cosmo = cosmo
         self.split = split
 
+    @staticmethod
+    def from_zeldovich(cosmo: Cosmology, box_size: float, mesh_n: int, n_side: int, n_s: float, sigma8: float,
+                       a_init: float, seed: int, split: ForceSplit | None, flags: int = 0) -> "Simulation":
+        """runner.rs:209-225 `init_simulation` with the ICs generated on the GPU (no host round trip)."""
+        prm = _sim_params(cosmo, box_size, mesh_n, n_side ** 3, split, flags)
+        h = C.c_void_p()
+        check(nat.lib().cpm_sim_create_zeldovich(C.byref(prm), int(n_side), float(n_s), float(sigma8),
+                                                 float(a_init), int(seed), C.byref(h)), sim=True)
+        return Simulation(cosmo, box_size, mesh_n, None, None, a_init, split, flags, _handle=h, _n=n_side ** 3)
+
     def step_to(self, a1: float) -> None:
         """integrator.rs:174-186."""
         check(nat.lib().cpm_sim_step_to(self.h, float(a1)), sim=True)
+
+    def step_host(self, a1: float, positions: np.ndarray, momenta: np.ndarray) -> None:
+        """`step_to` for host-owned state: positions and momenta (float32 (N, 3), C order) are
+        uploaded, stepped with the cached acceleration, and overwritten with the new state."""
+        for arr in (positions, momenta):
+            if arr.dtype != np.float32 or not arr.flags.c_contiguous or arr.size != 3 * self.n:
+                raise CpmError(-1, "step_host needs C-contiguous float32 arrays of shape (N, 3)")
+        check(nat.lib().cpm_sim_step_host(self.h, float(a1), ptr(positions), ptr(momenta)), sim=True)
 
     def run(self, a_end: float, steps: int) -> None:
         """integrator.rs:165-171."""

@@ -33,6 +33,10 @@ __device__ __forceinline__ void dev_fail(DevStatus* st, int code, int detail) {
   if (atomicCAS(&st->code, 0, code) == 0) st->detail = detail;
 }
 
+// Kernels launched by this library (every launch site calls count_launch() first).
+unsigned long long launch_count();
+void count_launch();
+
 // ---------------------------------------------------------------------------------------------
 // Reference constants (tree.rs:12-17)
 // ---------------------------------------------------------------------------------------------
@@ -215,5 +219,15 @@ void launch_permute_u32(const uint32_t* in, const uint32_t* perm, size_t n, uint
 void launch_scatter3(const float* in3, const uint32_t* id, size_t n, float* out3, cudaStream_t s);
 // Flags a non-finite coordinate in the status word.
 void launch_check_finite(const float* x3, size_t n, DevStatus* st, cudaStream_t s);
+// id[i] = i
+void launch_iota(uint32_t* id, size_t n, cudaStream_t s);
+
+// ---------------------------------------------------------------------------------------------
+// Initial conditions — ics.cu
+// ---------------------------------------------------------------------------------------------
+// Zel'dovich positions and momenta (AoS f32, lattice order (ix*n + iy)*n + iz) into device memory.
+cudaError_t generate_zeldovich(int n, float box, const cpm_cosmology& c, float n_s, float sigma8, float a_init,
+                               uint64_t seed, float* x3_dev, float* p3_dev, DevBuf& modes, DevBuf& work,
+                               FftPlan& plan, cudaStream_t s);
 
 }  // namespace cpm

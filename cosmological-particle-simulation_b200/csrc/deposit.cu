@@ -128,6 +128,7 @@ void launch_deposit_fixed(const float* x3, size_t n, float mass, int mesh_n, flo
   }
   const float scale = std::ldexp(1.0f, shift);
   const unsigned blocks = (unsigned)((n + DEP_CHUNK - 1) / DEP_CHUNK);
+  count_launch();
   k_deposit_fixed<<<blocks, DEP_THREADS, DEP_SMEM_CELLS * sizeof(unsigned long long), s>>>(x3, n, mass, mesh_n, h,
                                                                                          scale, mesh_fx);
 }
@@ -146,6 +147,7 @@ void launch_fixed_to_f32(const unsigned long long* fx, size_t m, int shift, int 
   if (m == 0) return;
   const float inv_scale = std::ldexp(1.0f, -shift);
   const size_t blocks = std::min<size_t>((m + 255) / 256, 148 * 32);
+  count_launch();
   k_fixed_to_f32<<<(unsigned)blocks, 256, 0, s>>>(fx, m, inv_scale, to_delta, mean, out);
 }
 

@@ -385,10 +385,12 @@ static void c2c_pass(float2* data, long long comp_stride, int ncomp, TileGeo g, 
   if (inverse) {
     auto k = k_fft_pass<N, W_COL, FFT_THREADS, true>;
     set_smem(k, smem);
+    count_launch();
     k<<<grid, FFT_THREADS, smem, s>>>(data, comp_stride, g, tw);
   } else {
     auto k = k_fft_pass<N, W_COL, FFT_THREADS, false>;
     set_smem(k, smem);
+    count_launch();
     k<<<grid, FFT_THREADS, smem, s>>>(data, comp_stride, g, tw);
   }
 }
@@ -437,6 +439,7 @@ static void poisson_n(const FftPlan& p, const PoissonParams& pp, const float* de
     const size_t smem = (size_t)W_ROW * line_ld<N>() * sizeof(float2);
     auto k = k_r2c_z<N, W_ROW, FFT_THREADS>;
     set_smem(k, smem);
+    count_launch();
     k<<<(rows + W_ROW - 1) / W_ROW, FFT_THREADS, smem, s>>>(delta, fx, std::ldexp(1.0f, -fx_shift), mean, s0, rows,
                                                             tw);
   }
@@ -448,6 +451,7 @@ static void poisson_n(const FftPlan& p, const PoissonParams& pp, const float* de
     auto k = k_poisson_x<N, W_PX, FFT_THREADS>;
     set_smem(k, smem);
     dim3 grid(N, (NH + W_PX - 1) / W_PX, 1);
+    count_launch();
     k<<<grid, FFT_THREADS, smem, s>>>(s0, spec, comp, TileGeo{NH, 1, n * NH, NH}, pp, deconv, tw);
   }
   // 4. y inverse on the three component spectra
@@ -458,6 +462,7 @@ static void poisson_n(const FftPlan& p, const PoissonParams& pp, const float* de
     auto k = k_c2r_z<N, W_ROW, FFT_THREADS>;
     set_smem(k, smem);
     dim3 grid((rows + W_ROW - 1) / W_ROW, 1, 3);
+    count_launch();
     k<<<grid, FFT_THREADS, smem, s>>>(spec, comp, gx, gy, gz, pp.scale, rows, tw);
   }
 }

@@ -45,12 +45,14 @@ __global__ void k_interpolate3(const float* __restrict__ gx, const float* __rest
 void launch_interpolate(const float* cells, const float* x3, size_t n, int mesh_n, float h, float* out,
                         cudaStream_t s) {
   if (n == 0) return;
+  count_launch();
   k_interpolate<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(cells, x3, n, mesh_n, h, out);
 }
 
 void launch_interpolate3(const float* gx, const float* gy, const float* gz, const float* x3, size_t n, int mesh_n,
                          float h, float* out3, cudaStream_t s) {
   if (n == 0) return;
+  count_launch();
   k_interpolate3<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(gx, gy, gz, x3, n, mesh_n, h, out3);
 }
 

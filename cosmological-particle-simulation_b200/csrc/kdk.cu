@@ -55,6 +55,11 @@ __global__ void k_check_finite(const float* __restrict__ x3, size_t n3, DevStatu
     if (!isfinite(x3[i])) dev_fail(st, DEV_NONFINITE, (int)(i / 3));
 }
 
+__global__ void k_iota(uint32_t* __restrict__ id, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    id[i] = (uint32_t)i;
+}
+
 static unsigned grid_for(size_t work) {
   size_t b = (work + 255) / 256;
   if (b > 148 * 16) b = 148 * 16;
@@ -63,32 +68,44 @@ static unsigned grid_for(size_t work) {
 
 void launch_kick(float* p3, const float* g3, size_t n, float k, cudaStream_t s) {
   if (n == 0) return;
+  count_launch();
   k_kick<<<grid_for(3 * n), 256, 0, s>>>(p3, g3, 3 * n, k);
 }
 
 void launch_kick_kick_drift(float* x3, float* p3, const float* g3, size_t n, float k_prev, int has_prev, float k1,
                             float d, float box, cudaStream_t s) {
   if (n == 0) return;
+  count_launch();
   k_kick_kick_drift<<<grid_for(3 * n), 256, 0, s>>>(x3, p3, g3, 3 * n, k_prev, has_prev, k1, d, box);
 }
 
 void launch_permute3(const float* in3, const uint32_t* perm, size_t n, float* out3, cudaStream_t s) {
   if (n == 0) return;
+  count_launch();
   k_permute3<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(in3, perm, n, out3);
 }
 
 void launch_permute_u32(const uint32_t* in, const uint32_t* perm, size_t n, uint32_t* out, cudaStream_t s) {
   if (n == 0) return;
+  count_launch();
   k_permute_u32<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(in, perm, n, out);
 }
 
 void launch_scatter3(const float* in3, const uint32_t* id, size_t n, float* out3, cudaStream_t s) {
   if (n == 0) return;
+  count_launch();
   k_scatter3<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(in3, id, n, out3);
+}
+
+void launch_iota(uint32_t* id, size_t n, cudaStream_t s) {
+  if (n == 0) return;
+  count_launch();
+  k_iota<<<grid_for(n), 256, 0, s>>>(id, n);
 }
 
 void launch_check_finite(const float* x3, size_t n, DevStatus* st, cudaStream_t s) {
   if (n == 0) return;
+  count_launch();
   k_check_finite<<<grid_for(3 * n), 256, 0, s>>>(x3, 3 * n, st);
 }
 

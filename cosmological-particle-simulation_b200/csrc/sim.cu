@@ -33,10 +33,15 @@ struct cpm_sim {
   SortScratch sort;
   TreeNodes tree;
   DevBuf x, p, acc, id, x2, p2, id2, keys, vals, fx, gx, gy, gz, spec, status, counters;
-  cudaEvent_t ev[N_PHASES + 1] = {};
+  // Per-step phase events, recorded without host synchronisation into a ring of RING steps and
+  // folded into phase_ms when the ring fills or cpm_sim_phase_times is called.
+  static constexpr int RING = 64;
+  cudaEvent_t ev[RING][N_PHASES] = {};
+  int ring_used = 0;
   double phase_ms[N_PHASES] = {};
   uint64_t timed_steps = 0;
   uint32_t launches = 0;
+  DevBuf host_tmp;  // caller-order staging of cpm_sim_step_host
 };
 
 #define SIM_CU(s, call)                                                                                      \
@@ -65,7 +70,29 @@ static int sim_check(cpm_sim* s) {
 }
 
 static void mark(cpm_sim* s, int phase) {
-  if (s->P.flags & CPM_SIM_TIMING) cudaEventRecord(s->ev[phase], s->stream);
+  if ((s->P.flags & CPM_SIM_TIMING) && s->ring_used < cpm_sim::RING)
+    cudaEventRecord(s->ev[s->ring_used][phase], s->stream);
+}
+
+// Folds the recorded steps into phase_ms. Phases: 0 kick+drift, 1 keys+sort+reorder, 2 deposit,
+// 3 FFT-Poisson, 4 gather, 5 tree build, 6 walk + second kick, 7 whole step.
+static int flush_timing(cpm_sim* s) {
+  if (s->ring_used == 0) return CPM_OK;
+  SIM_CU(s, cudaEventSynchronize(s->ev[s->ring_used - 1][7]));
+  for (int r = 0; r < s->ring_used; ++r) {
+    float ms;
+    for (int ph = 0; ph < 6; ++ph) {
+      cudaEventElapsedTime(&ms, s->ev[r][ph], s->ev[r][ph + 1]);
+      s->phase_ms[ph] += ms;
+    }
+    cudaEventElapsedTime(&ms, s->ev[r][6], s->ev[r][7]);
+    s->phase_ms[6] += ms;
+    cudaEventElapsedTime(&ms, s->ev[r][0], s->ev[r][7]);
+    s->phase_ms[7] += ms;
+  }
+  s->timed_steps += (uint64_t)s->ring_used;
+  s->ring_used = 0;
+  return CPM_OK;
 }
 
 // Sort into key order, then the force: deposit, FFT-Poisson, gather, tree. Phases 1..6.
@@ -108,12 +135,8 @@ static int sim_accelerations(cpm_sim* s, float a) {
   return CPM_OK;
 }
 
-extern "C" {
-
-int cpm_sim_create(const cpm_sim_params* params, const float* x3, const float* p3, float a0, cpm_sim** out) {
-  if (!out) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_create: out is NULL");
-  *out = nullptr;
-  if (!params || !x3 || !p3) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_create: null pointer");
+// Validates the parameters and allocates every device buffer of a simulation.
+static int sim_new(const cpm_sim_params* params, float a0, cpm_sim** out) {
   const cpm_sim_params& P = *params;
   if (P.n_particles == 0 || P.n_particles > 0x7FFFFFFFull)
     return set_error(nullptr, CPM_E_INVALID, "cpm_sim_create: n_particles must be in [1, 2^31)");
@@ -138,8 +161,10 @@ int cpm_sim_create(const cpm_sim_params* params, const float* x3, const float* p
     return code;
   };
   if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(CPM_E_CUDA);
-  for (auto& e : s->ev)
-    if (cudaEventCreate(&e) != cudaSuccess) return fail(CPM_E_CUDA);
+  if (P.flags & CPM_SIM_TIMING)
+    for (auto& row : s->ev)
+      for (auto& e : row)
+        if (cudaEventCreate(&e) != cudaSuccess) return fail(CPM_E_CUDA);
   const size_t n = s->n;
   const size_t half = (size_t)P.mesh_n * P.mesh_n * (P.mesh_n / 2 + 1);
   bool ok = true;
@@ -158,7 +183,58 @@ int cpm_sim_create(const cpm_sim_params* params, const float* x3, const float* p
   }
   cudaMemsetAsync(s->status.p, 0, sizeof(DevStatus), s->stream);
   cudaMemsetAsync(s->counters.p, 0, 2 * sizeof(unsigned long long), s->stream);
+  *out = s;
+  return CPM_OK;
+}
+
+extern "C" {
+
+int cpm_sim_create(const cpm_sim_params* params, const float* x3, const float* p3, float a0, cpm_sim** out) {
+  if (!out) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_create: out is NULL");
+  *out = nullptr;
+  if (!params || !x3 || !p3) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_create: null pointer");
+  cpm_sim* s = nullptr;
+  int rc = sim_new(params, a0, &s);
+  if (rc) return rc;
   if ((rc = cpm_sim_set_state(s, x3, p3)) != CPM_OK) {
+    g_last_error = s->err;
+    cpm_sim_destroy(s);
+    return rc;
+  }
+  *out = s;
+  return CPM_OK;
+}
+
+int cpm_sim_create_zeldovich(const cpm_sim_params* params, int n_side, float n_s, float sigma8, float a0,
+                             uint64_t seed, cpm_sim** out) {
+  if (!out) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_create_zeldovich: out is NULL");
+  *out = nullptr;
+  if (!params) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_create_zeldovich: params is NULL");
+  if (!fft_supported(n_side) || (size_t)n_side * n_side * n_side != params->n_particles)
+    return set_error(nullptr, CPM_E_INVALID,
+                     "cpm_sim_create_zeldovich: n_side must be a power of two in [4, 1024] with n_side^3 == n_particles");
+  if (!(sigma8 > 0.0f)) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_create_zeldovich: sigma8 must be > 0");
+  cpm_sim* s = nullptr;
+  int rc = sim_new(params, a0, &s);
+  if (rc) return rc;
+  DevBuf modes, work;
+  FftPlan plan;
+  cudaError_t e = generate_zeldovich(n_side, s->box, s->P.cosmo, n_s, sigma8, a0, seed, as<float>(s->x),
+                                     as<float>(s->p), modes, work, plan, s->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  release(modes);
+  release(work);
+  fft_plan_free(plan);
+  if (e != cudaSuccess) {
+    set_error(&s->err, e == cudaErrorMemoryAllocation ? CPM_E_NOMEM : CPM_E_CUDA,
+              std::string("cpm_sim_create_zeldovich: ") + cudaGetErrorString(e));
+    cpm_sim_destroy(s);
+    return e == cudaErrorMemoryAllocation ? CPM_E_NOMEM : CPM_E_CUDA;
+  }
+  launch_iota(as<uint32_t>(s->id), s->n, s->stream);
+  rc = sim_accelerations(s, s->a);
+  if (rc == CPM_OK) rc = sim_check(s);
+  if (rc) {
     g_last_error = s->err;
     cpm_sim_destroy(s);
     return rc;
@@ -190,27 +266,49 @@ int cpm_sim_step_to(cpm_sim* s, float a1) {
   const float k1 = kick_factor(c, a0, am);
   const float d = drift_factor(c, a0, a1);
   const float k2 = kick_factor(c, am, a1);
+  if ((s->P.flags & CPM_SIM_TIMING) && s->ring_used == cpm_sim::RING) {
+    int rc = flush_timing(s);
+    if (rc) return rc;
+  }
+  const unsigned long long l0 = launch_count();
   mark(s, 0);
   launch_kick_kick_drift(as<float>(s->x), as<float>(s->p), as<float>(s->acc), s->n, 0.0f, 0, k1, d, s->box, s->stream);
   int rc = sim_accelerations(s, a1);
   if (rc) return rc;
   launch_kick(as<float>(s->p), as<float>(s->acc), s->n, k2, s->stream);
   mark(s, 7);
+  s->launches = (uint32_t)(launch_count() - l0);
+  if (s->P.flags & CPM_SIM_TIMING) s->ring_used += 1;
   s->a = a1;
-  if (s->P.flags & CPM_SIM_TIMING) {
-    SIM_CU(s, cudaEventSynchronize(s->ev[7]));
-    float ms;
-    // phases: 0 kick/drift [ev0, ev1], 1 sort [ev1, ev2], 2 deposit [ev2, ev3], 3 poisson [ev3, ev4],
-    // 4 gather [ev4, ev5], 5 tree build [ev5, ev6], 6 walk + kick2 [ev6, ev7], 7 whole [ev0, ev7]
-    for (int ph = 0; ph < 7; ++ph) {
-      cudaEventElapsedTime(&ms, s->ev[ph], s->ev[ph + 1]);
-      s->phase_ms[ph] += ms;
-    }
-    cudaEventElapsedTime(&ms, s->ev[0], s->ev[7]);
-    s->phase_ms[7] += ms;
-    s->timed_steps += 1;
-  }
   return CPM_OK;
+}
+
+// Scatter caller-order host data through the staging buffer into key order: dst[i] = src[id[i]].
+static int upload_caller_order(cpm_sim* s, const float* host3, float* dst3) {
+  const size_t n = s->n;
+  SIM_CU(s, ensure(s->host_tmp, 3 * n * sizeof(float)));
+  SIM_CU(s, cudaMemcpyAsync(s->host_tmp.p, host3, 3 * n * sizeof(float), cudaMemcpyHostToDevice, s->stream));
+  launch_permute3(as<float>(s->host_tmp), as<uint32_t>(s->id), n, dst3, s->stream);
+  return CPM_OK;
+}
+
+static int download_caller_order(cpm_sim* s, const float* src3, float* host3) {
+  const size_t n = s->n;
+  SIM_CU(s, ensure(s->host_tmp, 3 * n * sizeof(float)));
+  launch_scatter3(src3, as<uint32_t>(s->id), n, as<float>(s->host_tmp), s->stream);
+  SIM_CU(s, cudaMemcpyAsync(host3, s->host_tmp.p, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+  return CPM_OK;
+}
+
+int cpm_sim_step_host(cpm_sim* s, float a1, float* x3, float* p3) {
+  if (!s || !x3 || !p3) return set_error(s ? &s->err : nullptr, CPM_E_INVALID, "cpm_sim_step_host: null pointer");
+  int rc = upload_caller_order(s, x3, as<float>(s->x));
+  if (!rc) rc = upload_caller_order(s, p3, as<float>(s->p));
+  if (!rc) rc = cpm_sim_step_to(s, a1);
+  if (!rc) rc = download_caller_order(s, as<float>(s->x), x3);
+  if (!rc) rc = download_caller_order(s, as<float>(s->p), p3);
+  if (rc) return rc;
+  return sim_check(s);
 }
 
 int cpm_sim_get_state(cpm_sim* s, float* x3, float* p3, float* acc3, float* delta, float* a) {
@@ -234,6 +332,8 @@ int cpm_sim_get_state(cpm_sim* s, float* x3, float* p3, float* acc3, float* delt
 
 int cpm_sim_phase_times(cpm_sim* s, double* ms8, uint64_t* steps, int reset) {
   if (!s) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_phase_times: sim is NULL");
+  int rc = flush_timing(s);
+  if (rc) return rc;
   if (ms8)
     for (int i = 0; i < N_PHASES; ++i) ms8[i] = s->timed_steps ? s->phase_ms[i] / (double)s->timed_steps : 0.0;
   if (steps) *steps = s->timed_steps;
@@ -274,8 +374,10 @@ int cpm_sim_destroy(cpm_sim* s) {
                     &s->acc, &s->id, &s->x2, &s->p2, &s->id2, &s->keys, &s->vals, &s->fx, &s->gx, &s->gy, &s->gz,
                     &s->spec, &s->status, &s->counters})
     release(*b);
-  for (auto& e : s->ev)
-    if (e) cudaEventDestroy(e);
+  release(s->host_tmp);
+  for (auto& row : s->ev)
+    for (auto& e : row)
+      if (e) cudaEventDestroy(e);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
   return CPM_OK;

@@ -2,10 +2,15 @@
 // pairs, and exclusive scans. HBM-bound integer work: coalesced tiles, per-warp ranking with
 // __match_any_sync, no tensor cores.
 #include <algorithm>
+#include <atomic>
 
 #include "cpm_internal.cuh"
 
 namespace cpm {
+
+static std::atomic<unsigned long long> g_launches{0};
+unsigned long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 cudaError_t ensure(DevBuf& b, size_t bytes) {
   if (b.p != nullptr && b.bytes >= bytes) return cudaSuccess;
@@ -57,6 +62,7 @@ void launch_octant_keys(const float* x3, size_t n, float box, int levels, uint64
                         DevStatus* st, cudaStream_t s) {
   if (n == 0) return;
   const int T = 256;
+  count_launch();
   k_octant_keys<<<(unsigned)((n + T - 1) / T), T, 0, s>>>(x3, n, box / 2.0f, levels, keys, vals, st);
 }
 
@@ -142,13 +148,16 @@ static size_t scan_tmp_words(size_t n) {
 static void scan_rec(const uint32_t* in, uint32_t* out, size_t n, uint32_t* tmp, cudaStream_t s) {
   if (n == 0) return;
   if (n <= (size_t)SC_TILE) {
+    count_launch();
     k_scan_tile<<<1, SC_THREADS, 0, s>>>(in, out, n, nullptr);
     return;
   }
   const size_t nb = (n + SC_TILE - 1) / SC_TILE;
   uint32_t* partial = tmp;
+  count_launch();
   k_scan_reduce<<<(unsigned)nb, SC_THREADS, 0, s>>>(in, n, partial);
   scan_rec(partial, partial, nb, tmp + nb + 64, s);
+  count_launch();
   k_scan_tile<<<(unsigned)nb, SC_THREADS, 0, s>>>(in, out, n, partial);
 }
 
@@ -259,8 +268,10 @@ cudaError_t radix_sort_pairs(uint64_t* keys, uint32_t* vals, size_t n, int bits,
   const int passes = (bits + 7) / 8;
   for (int p = 0; p < passes; ++p) {
     const int shift = 8 * p;
+    count_launch();
     k_radix_hist<<<nblocks, RS_THREADS, 0, s>>>(ka, n, shift, hist, nblocks);
     if ((e = exclusive_scan_u32(hist, hist, (size_t)RS_BINS * nblocks, sc.scan_tmp, s)) != cudaSuccess) return e;
+    count_launch();
     k_radix_scatter<<<nblocks, RS_THREADS, 0, s>>>(ka, va, kb, vb, n, shift, hist, nblocks);
     std::swap(ka, kb);
     std::swap(va, vb);

@@ -254,15 +254,22 @@ cudaError_t tree_build(TreeNodes& t, const uint64_t* sorted_keys, const float* s
   uint4* link = as<uint4>(t.link);
   float4* geo = as<float4>(t.geo);
   uint32_t* counters = as<uint32_t>(t.counters);
+  count_launch();
   k_tree_root<<<1, CNT_WORDS, 0, s>>>(link, geo, counters, (uint32_t)n, box / 2.0f);
-  for (int d = 0; d <= KEY_LEVELS; ++d)
+  for (int d = 0; d <= KEY_LEVELS; ++d) {
+    count_launch();
     k_tree_level<<<BUILD_BLOCKS, BUILD_THREADS, 0, s>>>(d, sorted_keys, link, geo, counters, (uint32_t)t.capacity, st);
+  }
 
   D3* partial = as<D3>(t.scan_tmp);
   double* P = as<double>(t.prefix);
+  count_launch();
   k_pos_reduce<<<(unsigned)nb, PS_THREADS, 0, s>>>(sorted_x3, n, partial);
+  count_launch();
   k_partial_scan<<<1, PS_THREADS, 0, s>>>(partial, nb);
+  count_launch();
   k_pos_prefix<<<(unsigned)nb, PS_THREADS, 0, s>>>(sorted_x3, n, partial, P);
+  count_launch();
   k_tree_com<<<BUILD_BLOCKS, BUILD_THREADS, 0, s>>>(link, P, as<float4>(t.mass), counters, (uint32_t)t.capacity);
   return cudaGetLastError();
 }
@@ -445,6 +452,7 @@ void launch_tree_walk(const TreeNodes& t, const float* sorted_x3, size_t n, floa
   w.k = k;
   const size_t groups = (n + 31) / 32;
   const unsigned blocks = (unsigned)((groups + WALK_WARPS - 1) / WALK_WARPS);
+  count_launch();
   k_tree_walk<<<blocks, WALK_THREADS, 0, s>>>(static_cast<const uint4*>(t.link.p), static_cast<const float4*>(t.geo.p),
                                               static_cast<const float4*>(t.mass.p), sorted_x3, n, w, acc3, accumulate,
                                               reinterpret_cast<unsigned long long*>(counters), st);

@@ -129,6 +129,14 @@ int cpm_octant_keys(cpm_ctx* ctx, const float* x3, size_t n, float box_size, int
  * accepted-node interaction counts, maximum depth. Any pointer may be NULL. */
 int cpm_tree_stats(cpm_ctx* ctx, uint64_t* nodes, uint64_t* leaf_pairs, uint64_t* node_accepts, uint32_t* max_depth);
 
+/* ics.rs:119-182 `zeldovich(n, L, &cosmo, &ps, a_init, seed)` with
+ * ps = `PowerSpectrum::normalized(&cosmo, n_s, sigma8, 8.0)` (ics.rs:56-63): n_side^3 particles on a
+ * lattice (index (ix*n+iy)*n+iz), positions and momenta AoS [n^3][3]. The white noise is this
+ * library's Philox-4x32-10 (counter = cell index, key = seed) with Box-Muller, not the reference's
+ * rand::StdRng stream. */
+int cpm_ics_zeldovich(int n_side, float box_size, const cpm_cosmology* cosmo, float n_s, float sigma8, float a_init,
+                      uint64_t seed, float* x3, float* p3);
+
 /* ------------------------------------------------------------------ device-resident simulation */
 /* Replaces `Simulation` (integrator.rs:34-186) under a `cuda` feature: state stays in HBM and
  * `step_to` runs one KDK step (kick, drift, deposit, FFT-Poisson, gather, tree build and walk,
@@ -156,9 +164,21 @@ typedef struct {
 /* integrator.rs:54-79 `Simulation::new`: uploads x3, p3 (AoS [n][3]) and computes the initial
  * acceleration at a0. */
 int cpm_sim_create(const cpm_sim_params* params, const float* x3, const float* p3, float a0, cpm_sim** out);
+/* runner.rs:209-225 `init_simulation` without the host round trip: Zel'dovich ICs of n_side^3
+ * particles (ics.rs:119-182, spectrum PowerSpectrum::normalized(cosmo, n_s, sigma8, 8), ics.rs:56)
+ * generated on the GPU into the simulation, then `Simulation::new` (integrator.rs:54-79) at a0.
+ * params->n_particles must equal n_side^3. White noise: Philox-4x32-10 + Box-Muller (see
+ * cpm_ics_zeldovich). */
+int cpm_sim_create_zeldovich(const cpm_sim_params* params, int n_side, float n_s, float sigma8, float a0,
+                             uint64_t seed, cpm_sim** out);
 /* integrator.rs:174-186 `Simulation::step_to(a1)`. Kick and drift factors are the reference's f32
  * Simpson/bisection values (integrator.rs:263-297), computed on the host. */
 int cpm_sim_step_to(cpm_sim* sim, float a1);
+/* `Simulation::step_to(a1)` for a caller that owns the state on the host (the reference's pub
+ * `positions` and `momenta`, integrator.rs:39-40): uploads x3 and p3 (caller order), runs one step
+ * with the simulation's cached acceleration for the first half-kick (the reference's private
+ * `accel`), and writes the new x3 and p3 back. Synchronous. */
+int cpm_sim_step_host(cpm_sim* sim, float a1, float* x3, float* p3);
 /* Reads the state in the caller's particle order. Any pointer may be NULL. delta is n^3. */
 int cpm_sim_get_state(cpm_sim* sim, float* x3, float* p3, float* acc3, float* delta, float* a);
 /* Overwrites positions and momenta (caller's order) and recomputes the acceleration at the current a. */

@@ -296,6 +296,7 @@ struct Node {  // tree.rs:68-80
 struct Tree {
   const float* pos;  // AoS [n][3]
   float box;
+  int com_f64 = 0;   // 0: f32 sequential sum (tree.rs:190-200); 1: FP64 sum rounded once (diagnostic)
   std::vector<uint32_t> order;
   std::vector<Node> nodes;
 
@@ -316,12 +317,21 @@ struct Tree {
   uint32_t build_node(size_t start, size_t end, const float* center, float half, uint32_t depth) {
     const uint32_t idx = (uint32_t)nodes.size();
     float com[3] = {0.0f, 0.0f, 0.0f};
-    for (size_t t = start; t < end; ++t) {
-      const float* p = pos + 3 * (size_t)order[t];
-      for (int k = 0; k < 3; ++k) com[k] += p[k];
+    if (com_f64) {
+      double sd[3] = {0.0, 0.0, 0.0};
+      for (size_t t = start; t < end; ++t) {
+        const float* p = pos + 3 * (size_t)order[t];
+        for (int k = 0; k < 3; ++k) sd[k] += (double)p[k];
+      }
+      for (int k = 0; k < 3; ++k) com[k] = (float)(sd[k] / (double)(end - start));
+    } else {
+      for (size_t t = start; t < end; ++t) {
+        const float* p = pos + 3 * (size_t)order[t];
+        for (int k = 0; k < 3; ++k) com[k] += p[k];
+      }
+      const float count = (float)(end - start);
+      for (int k = 0; k < 3; ++k) com[k] /= count;
     }
-    const float count = (float)(end - start);
-    for (int k = 0; k < 3; ++k) com[k] /= count;
     Node nd;
     for (int k = 0; k < 3; ++k) {
       nd.center[k] = center[k];
@@ -834,6 +844,19 @@ void orc_tree_accelerations(const float* x3, size_t n, float box, const orc_spli
   tree_accelerations(x3, n, box, *s, k, acc3, nullptr, nullptr);
 }
 
+// Diagnostic twin of orc_tree_accelerations with the centre of mass summed in FP64.
+void orc_tree_accelerations_com64(const float* x3, size_t n, float box, const orc_split* s, float k, float* acc3) {
+  Tree tree;
+  tree.com_f64 = 1;
+  tree.build(x3, n, box);
+#pragma omp parallel
+  {
+    std::vector<uint32_t> stack;
+#pragma omp for schedule(dynamic, 256)
+    for (long long i = 0; i < (long long)n; ++i) tree.accel_on((size_t)i, *s, k, stack, acc3 + 3 * (size_t)i, nullptr);
+  }
+}
+
 void orc_tree_accelerations_builtin(const float* x3, size_t n, float box, const orc_split* s, float k,
                                     float* acc3) {
   Tree tree;
@@ -1079,6 +1102,66 @@ void orc_sim_free(orc_sim* s) { delete s; }
 
 void orc_sim_last_timings(const orc_sim* s, double* t6) {
   for (int i = 0; i < 6; ++i) t6[i] = s->t[i];
+}
+
+void orc_step_sample(const orc_cosmology* c, float box, int mesh_n, const float* x3, const float* p3,
+                     const float* acc3, size_t n, float a0, float a1, const orc_split* split,
+                     const uint32_t* subset, size_t m, int threads, double* t7) {
+#ifdef _OPENMP
+  if (threads > 0) omp_set_num_threads(threads);
+#else
+  (void)threads;
+#endif
+  std::vector<float> x(x3, x3 + 3 * n), p(p3, p3 + 3 * n);
+  const size_t mm = (size_t)mesh_n * mesh_n * mesh_n;
+  std::vector<float> delta(mm), g(3 * mm), acc(3 * n);
+  const double t0 = now_s();
+  const float am = midpoint(*c, a0, a1);
+  const float k1 = kick_factor(*c, a0, am);
+  kick(p.data(), acc3, n, k1);
+  const float d = drift_factor(*c, a0, a1);
+  drift(x.data(), p.data(), n, d, box);
+  const double t1 = now_s();
+  orc_density_contrast(mesh_n, box, x.data(), n, delta.data());
+  const double t2 = now_s();
+  poisson_accel(mesh_n, box, delta.data(), c->omega_m, a1, split ? split->r_split : 0.0f, g.data(), g.data() + mm,
+                g.data() + 2 * mm);
+  const double t3 = now_s();
+#pragma omp parallel for schedule(static)
+  for (long long i = 0; i < (long long)n; ++i)
+    for (int q = 0; q < 3; ++q)
+      acc[3 * (size_t)i + q] = interpolate(mesh_n, box, g.data() + (size_t)q * mm, x.data() + 3 * (size_t)i);
+  const double t4 = now_s();
+  double t5 = t4, t6 = t4;
+  if (split) {
+    Tree tree;
+    tree.build(x.data(), n, box);
+    t5 = now_s();
+    const float L = box;
+    const float kc = 1.5f * c->omega_m * (L * L * L) / (4.0f * (float)3.14159265358979323846 * a1 * (float)n);
+#pragma omp parallel
+    {
+      std::vector<uint32_t> stack;
+#pragma omp for schedule(dynamic, 64)
+      for (long long t = 0; t < (long long)m; ++t) {
+        float sr[3];
+        const size_t i = subset[t];
+        tree.accel_on(i, *split, kc, stack, sr, nullptr);
+        for (int q = 0; q < 3; ++q) acc[3 * i + q] += sr[q];
+      }
+    }
+    t6 = now_s();
+  }
+  const float k2 = kick_factor(*c, am, a1);
+  kick(p.data(), acc.data(), n, k2);
+  const double t7e = now_s();
+  t7[0] = t1 - t0;
+  t7[1] = t2 - t1;
+  t7[2] = t3 - t2;
+  t7[3] = t4 - t3;
+  t7[4] = t5 - t4;
+  t7[5] = t6 - t5;
+  t7[6] = t7e - t6;
 }
 
 float orc_power(const orc_cosmology* c, const orc_pspec* ps, float k) { return power(*c, *ps, k); }

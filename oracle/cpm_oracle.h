@@ -60,6 +60,8 @@ orc_split orc_split_with(float box, size_t mesh_n, size_t pps, float soft_scale,
 float orc_short_range_factor(float r, float r_split);                          /* :54-57 */
 void orc_tree_accelerations(const float* x3, size_t n, float box, const orc_split* s, float k,
                             float* acc3);                                       /* :314-323 */
+/* Diagnostic: the same walk with node centres of mass summed in FP64 (rounded once to f32). */
+void orc_tree_accelerations_com64(const float* x3, size_t n, float box, const orc_split* s, float k, float* acc3);
 void orc_tree_accelerations_builtin(const float* x3, size_t n, float box, const orc_split* s, float k,
                                     float* acc3);                               /* BuiltTree::accel_on :103-150 */
 void orc_brute_force(const float* x3, size_t n, float box, const orc_split* s, float k, float* acc3); /* :352-370 */
@@ -102,6 +104,15 @@ void orc_sim_accelerations(const orc_sim* s, float a, float* acc3, float* delta)
 void orc_sim_free(orc_sim* s);
 /* Wall-clock seconds spent in the last step's phases: kick+drift, deposit, poisson, gather, tree build, walk. */
 void orc_sim_last_timings(const orc_sim* s, double* t6);
+
+/* Timed sample of one KDK step of the reference path (integrator.rs:174-186) on the state (x3, p3, acc3)
+ * at a0 -> a1, for the CPU baseline. Every phase runs on all n particles except the tree walk, which
+ * runs for the m particles listed in `subset` (the caller scales it by n / m). The state is not
+ * modified. t7 receives seconds for: kick+drift, deposit, Poisson, gather, tree build, walk of the
+ * subset, second kick. `threads` > 0 sets the OpenMP thread count. */
+void orc_step_sample(const orc_cosmology* c, float box, int mesh_n, const float* x3, const float* p3,
+                     const float* acc3, size_t n, float a0, float a1, const orc_split* split,
+                     const uint32_t* subset, size_t m, int threads, double* t7);
 
 /* ics.rs */
 float orc_power(const orc_cosmology* c, const orc_pspec* ps, float k);           /* :27-33 */

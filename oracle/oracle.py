@@ -72,6 +72,7 @@ def lib() -> C.CDLL:
         "orc_short_range_factor": (fl, [fl, fl]),
         "orc_tree_accelerations": (None, [f32p, sz, fl, C.POINTER(Split), fl, f32p]),
         "orc_tree_accelerations_builtin": (None, [f32p, sz, fl, C.POINTER(Split), fl, f32p]),
+        "orc_tree_accelerations_com64": (None, [f32p, sz, fl, C.POINTER(Split), fl, f32p]),
         "orc_brute_force": (None, [f32p, sz, fl, C.POINTER(Split), fl, f32p]),
         "orc_tree_build": (sz, [f32p, sz, fl] + [C.c_void_p] * 9),
         "orc_tree_walk_stats": (None, [f32p, sz, fl, C.POINTER(Split), C.POINTER(C.c_uint64),
@@ -102,6 +103,8 @@ def lib() -> C.CDLL:
         "orc_zeldovich": (None, [i, fl, C.POINTER(Cosmology), C.POINTER(PSpec), fl, C.c_uint64, f32p, f32p]),
         "orc_power_spectrum": (None, [f32p, sz, fl, i, i, f64p, f64p, u64p]),
         "orc_num_threads": (i, []),
+        "orc_step_sample": (None, [C.POINTER(Cosmology), fl, i, f32p, f32p, f32p, sz, fl, fl, C.c_void_p, u32p, sz,
+                                   i, f64p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -211,6 +214,14 @@ def tree_accelerations(x, box: float, split: Split, k: float) -> np.ndarray:
     x = _f32(x)
     out = np.empty((len(x), 3), np.float32)
     lib().orc_tree_accelerations(x, len(x), box, C.byref(split), k, out)
+    return out
+
+
+def tree_accelerations_com64(x, box: float, split: Split, k: float) -> np.ndarray:
+    """Diagnostic twin of tree_accelerations with FP64 centre-of-mass sums."""
+    x = _f32(x)
+    out = np.empty((len(x), 3), np.float32)
+    lib().orc_tree_accelerations_com64(x, len(x), box, C.byref(split), k, out)
     return out
 
 
@@ -403,6 +414,19 @@ def power_spectrum(x, box: float, n: int, n_shells: int):
 
 def num_threads() -> int:
     return lib().orc_num_threads()
+
+
+def step_sample(c: Cosmology, box: float, mesh_n: int, x, p, acc, a0: float, a1: float, split: Split | None,
+                subset, threads: int = 0) -> np.ndarray:
+    """Seconds of each phase of one reference KDK step on (x, p, acc); the walk runs for `subset` only.
+    Returns [kick+drift, deposit, poisson, gather, tree build, walk(subset), second kick]."""
+    x, p, acc = _f32(x), _f32(p), _f32(acc)
+    sub = np.ascontiguousarray(subset, dtype=np.uint32)
+    t = np.zeros(7, np.float64)
+    lib().orc_step_sample(C.byref(c), box, mesh_n, x, p, acc, len(x), a0, a1,
+                          C.cast(C.pointer(split), C.c_void_p) if split is not None else None, sub, len(sub),
+                          threads, t)
+    return t
 
 
 os.environ.setdefault("OMP_PROC_BIND", "false")

@@ -124,6 +124,56 @@ def test_treepm_pair_force_matches_newton(cpm, orc):
     assert abs(acc[0, 0] - newton) / newton < 0.05 and abs(acc[1, 0] + newton) / newton < 0.05
 
 
+@pytest.mark.parametrize("n,box,seed", [(16, 64.0, 42), (32, 128.0, 7)])
+def test_zeldovich_ics_match_oracle(cpm, orc, n, box, seed):
+    """ics.rs:78-182 on the GPU vs the oracle: same Philox noise, same f32 scalars; FFT round-off only."""
+    c = orc.cosmology(0.0, 0.3, 0.7, 70.0)
+    ps = orc.power_normalized(c, 0.96, 0.8, 8.0)
+    xr, pr = orc.zeldovich(n, box, c, ps, 0.02, seed)
+    xg, pg = cpm.zeldovich(n, box, cpm.Cosmology(0.0, 0.3, 0.7, 70.0), 0.96, 0.8, 0.02, seed)
+    assert periodic_max_diff(xg, xr, box) < 1e-5 * box
+    assert rel_rms(pg, pr) < 1e-5
+
+
+def test_sim_from_device_ics_equals_host_ics(cpm, orc):
+    cc = cpm.Cosmology(0.0, 0.3, 0.7, 70.0)
+    split = cpm.ForceSplit.with_(32.0, 32, 16, 1.0 / 30.0, 0.5)
+    x, p = cpm.zeldovich(16, 32.0, cc, 0.96, 0.8, 0.02, 5)
+    a = cpm.Simulation(cc, 32.0, 32, x, p, 0.02, split)
+    b = cpm.Simulation.from_zeldovich(cc, 32.0, 32, 16, 0.96, 0.8, 0.02, 5, split)
+    sa, sb = a.state(), b.state()
+    assert np.array_equal(sa["x"], sb["x"]) and np.array_equal(sa["p"], sb["p"])
+    assert np.array_equal(sa["acc"], sb["acc"])
+
+
+def test_step_host_equals_step_to(cpm):
+    """cpm_sim_step_host (host-owned state) gives bit-identical results to the resident step."""
+    cc = cpm.Cosmology(0.0, 0.3, 0.7, 70.0)
+    split = cpm.ForceSplit.with_(32.0, 32, 16, 1.0 / 30.0, 0.5)
+    a = cpm.Simulation.from_zeldovich(cc, 32.0, 32, 16, 0.96, 0.8, 0.02, 9, split)
+    b = cpm.Simulation.from_zeldovich(cc, 32.0, 32, 16, 0.96, 0.8, 0.02, 9, split)
+    st = b.state()
+    xh, ph = st["x"].copy(), st["p"].copy()
+    for a1 in cpm.ln_a_schedule(0.02, 0.3, 6)[:3]:
+        a.step_to(a1)
+        b.step_host(a1, xh, ph)
+    sa = a.state()
+    assert np.array_equal(sa["x"], xh) and np.array_equal(sa["p"], ph)
+
+
+def test_phase_timing_and_counters(cpm):
+    cc = cpm.Cosmology(0.0, 0.3, 0.7, 70.0)
+    split = cpm.ForceSplit.with_(32.0, 32, 16, 1.0 / 30.0, 0.5)
+    s = cpm.Simulation.from_zeldovich(cc, 32.0, 32, 16, 0.96, 0.8, 0.02, 9, split, flags=cpm._native.SIM_TIMING)
+    for a1 in cpm.ln_a_schedule(0.02, 0.3, 6)[:4]:
+        s.step_to(a1)
+    ms, steps = s.phase_times()
+    assert steps == 4 and np.all(ms >= 0) and ms[7] > 0
+    assert abs(ms[:7].sum() - ms[7]) < 0.05 * ms[7] + 1e-3
+    c = s.counters()
+    assert c["nodes"] > 0 and c["leaf_pairs"] > 0 and c["launches_per_step"] > 10
+
+
 def test_sim_rejects_bad_arguments(cpm):
     x = np.zeros((8, 3), np.float32)
     with pytest.raises(cpm.CpmError) as e:
