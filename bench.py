@@ -40,6 +40,10 @@ WORKLOADS = {
     "treepm-256": dict(n_side=256, mesh=512, box=256.0, seed=7, steps_total=128),
     # the reference's CPU-runnable case: 32^3 particles, 64^3 mesh, 64 Mpc/h, seed 42, 64 steps.
     "treepm-32": dict(n_side=32, mesh=64, box=64.0, seed=42, steps_total=64),
+    # profiling case: same physics at 128^3 particles (a few GB on the device).
+    "treepm-128": dict(n_side=128, mesh=256, box=128.0, seed=7, steps_total=128),
+    # profiling case for the PM kernels: full-size 512^3 mesh, 128^3 particles.
+    "pm512-128": dict(n_side=128, mesh=512, box=128.0, seed=7, steps_total=128),
 }
 COSMO = dict(omega_r=0.0, omega_m=0.3, omega_l=0.7, h0=70.0)
 N_S, SIGMA8, A_INIT, A_END, THETA, SOFT = 0.96, 0.8, 0.02, 1.0, 0.5, 1.0 / 30.0
@@ -152,8 +156,17 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
     torch.cuda.set_device(dev)
 
-    sim = cpm.Simulation.from_zeldovich(cosmo, box, mesh, n_side, N_S, SIGMA8, A_INIT, wl["seed"] + rank, split,
-                                        flags=cpm._native.SIM_TIMING)
+    if args.load_state:
+        # continue the schedule from a saved state (profiling of a given epoch, e.g. z = 0)
+        st0 = np.load(args.load_state)
+        a_saved = float(st0["a"])
+        sim = cpm.Simulation(cosmo, box, mesh, st0["x"], st0["p"], a_saved, split, flags=cpm._native.SIM_TIMING)
+        full = schedule(wl["steps_total"], wl["steps_total"] + args.warmup + args.steps + 1)
+        i0 = int(np.searchsorted(np.asarray(full, np.float32), np.float32(a_saved), side="right"))
+        sched = full[i0:i0 + args.warmup + args.steps]
+    else:
+        sim = cpm.Simulation.from_zeldovich(cosmo, box, mesh, n_side, N_S, SIGMA8, A_INIT, wl["seed"] + rank, split,
+                                            flags=cpm._native.SIM_TIMING)
     stream = torch.cuda.ExternalStream(sim.stream())
     for a1 in sched[:args.warmup]:
         sim.step_to(a1)
@@ -185,6 +198,9 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
         ms = ms_local
     phases, nsteps = sim.phase_times()
     counters = sim.counters()
+    if args.save_state and rank == 0:
+        st = sim.state()
+        np.savez(args.save_state, x=st["x"], p=st["p"], a=np.float32(st["a"]))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         st = sim.state()
         snapshots["end"] = (st["x"], st["p"], st["acc"], sched[-1])
@@ -352,6 +368,8 @@ def main() -> int:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-walk-fraction", type=float, default=1.0 / 64.0)
     ap.add_argument("--ref-budget-s", type=float, default=120.0)
+    ap.add_argument("--save-state", default="", help="write the state after the timed steps (npz: x, p, a)")
+    ap.add_argument("--load-state", default="", help="start from a saved state and continue its schedule")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         ap.error("--warmup must be >= 3")
