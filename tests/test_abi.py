@@ -61,3 +61,17 @@ def test_invalid_arguments_fail_without_a_device(native):
     assert "n_mesh" in native.last_error()
     assert native.lib().cpm_ctx_create(8, 1.0, 0, 0, None) == -1
     assert native.lib().cpm_mesh_deposit(None, None, 0, 1.0, None) == -1
+
+
+def _compile_mirror(native, out_dir):
+    root = native.HERE.parent
+    exe = out_dir / "mirror_check"
+    cmd = ["g++", "-std=c++17", "-O1", "-I", str(root / "include"), str(root / "tests" / "cpp" / "mirror_check.cpp"),
+           "-o", str(exe), "-L", str(native.HERE), "-lcpm_cuda", f"-Wl,-rpath,{native.HERE}"]
+    subprocess.run(cmd, check=True, capture_output=True, text=True)
+    return exe
+
+
+def test_cpp_mirror_compiles_and_links(native, tmp_path):
+    """include/cpm.hpp (the C++ mirror of the reference interface) builds against the library."""
+    assert _compile_mirror(native, tmp_path).exists()
