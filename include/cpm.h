@@ -79,6 +79,19 @@ int cpm_ctx_destroy(cpm_ctx* ctx);
  * depend on particle order and is the exactly-rounded sum of the reference's f32 weights. */
 int cpm_mesh_deposit(cpm_ctx* ctx, const float* x3, size_t n, float mass, float* cells_out);
 
+/* No counterpart in the reference. A variant of cpm_mesh_deposit for callers that cannot call
+ * cudaMalloc — code running while a CUDA stream is captured into a graph, or programs whose device
+ * memory belongs to their own allocator. Positions (x3_dev, AoS [n][3]) and the output mesh
+ * (cells_dev, n_mesh^3) are device pointers; the work is enqueued on `stream` (a cudaStream_t, NULL
+ * for the default stream) and the call returns without waiting. The only scratch is a static
+ * device array of 64^3 u64 cells (2 MiB per GPU, kept until exit): n_mesh above 64 returns
+ * CPM_E_CAPACITY. Nothing is allocated. The first call on each device looks up the array's address
+ * (cudaGetSymbolAddress): make it before any stream capture. All calls on a device share the array
+ * (cleared by every call); calls that overlap on the GPU race on it. Results equal
+ * cpm_mesh_deposit's. */
+int cpm_mesh_deposit_noalloc(const float* x3_dev, size_t n, int n_mesh, float box_size, float mass, float* cells_dev,
+                             void* stream);
+
 /* integrator.rs:117-126 `Simulation::density_contrast`: deposit of unit masses, then
  * delta = c / (N / n^3) - 1 in f32. */
 int cpm_density_contrast(cpm_ctx* ctx, const float* x3, size_t n, float* delta_out);
