@@ -269,7 +269,8 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
         "phase_ms": {k: round(v, 4) for k, v in zip(phase_names, phases)},
         "phase_steps": nsteps,
         "tree": {"nodes_last_step": counters["nodes"], "leaf_pairs_last_step": counters["leaf_pairs"],
-                 "node_accepts_last_step": counters["node_accepts"]},
+                 "node_accepts_last_step": counters["node_accepts"],
+                 "candidates_last_step": counters["candidates"]},
         "gpu_launches": counters["launches_per_step"] * args.steps,
         "launches_per_step": counters["launches_per_step"],
         "clocks": clk,

@@ -108,6 +108,8 @@ def lib() -> C.CDLL:
         "cpm_sim_set_state": (i, [vp, vp, vp]),
         "cpm_sim_phase_times": (i, [vp, vp, C.POINTER(u64), i]),
         "cpm_sim_counters": (i, [vp, C.POINTER(u64), C.POINTER(u64), C.POINTER(u64), C.POINTER(u32)]),
+        "cpm_sim_walk_candidates": (i, [vp, C.POINTER(u64)]),
+        "cpm_walk_kernel_fit_error": (i, [fl, fl, i, C.POINTER(C.c_double)]),
         "cpm_sim_stream": (vp, [vp]),
         "cpm_sim_destroy": (i, [vp]),
     }

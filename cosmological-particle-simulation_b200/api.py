@@ -333,7 +333,10 @@ class Simulation:
     def counters(self) -> dict:
         nn, lp, na, ln = C.c_uint64(), C.c_uint64(), C.c_uint64(), C.c_uint32()
         check(nat.lib().cpm_sim_counters(self.h, C.byref(nn), C.byref(lp), C.byref(na), C.byref(ln)), sim=True)
-        return dict(nodes=nn.value, leaf_pairs=lp.value, node_accepts=na.value, launches_per_step=ln.value)
+        cand = C.c_uint64()
+        check(nat.lib().cpm_sim_walk_candidates(self.h, C.byref(cand)), sim=True)
+        return dict(nodes=nn.value, leaf_pairs=lp.value, node_accepts=na.value, launches_per_step=ln.value,
+                    candidates=cand.value)
 
     def stream(self) -> int:
         return nat.lib().cpm_sim_stream(self.h) or 0

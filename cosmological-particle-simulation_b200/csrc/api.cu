@@ -127,7 +127,7 @@ int cpm_ctx_destroy(cpm_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   fft_plan_free(c->plan);
   for (DevBuf* b : {&c->sort.keys_alt, &c->sort.vals_alt, &c->sort.block_hist, &c->sort.scan_tmp, &c->tree.geo,
-                    &c->tree.mass, &c->tree.link, &c->tree.counters, &c->tree.prefix, &c->tree.scan_tmp, &c->x,
+                    &c->tree.mass, &c->tree.link, &c->tree.counters, &c->tree.prefix, &c->tree.scan_tmp, &c->tree.x4, &c->x,
                     &c->x_sorted, &c->keys, &c->vals, &c->acc, &c->acc_sorted, &c->out, &c->mesh_fx, &c->mesh_a,
                     &c->mesh_b, &c->mesh_c, &c->mesh_d, &c->spec, &c->status, &c->tree_counters})
     release(*b);
@@ -316,8 +316,8 @@ int cpm_tree_accel(cpm_ctx* c, const float* x3, size_t n, float box_size, const 
   CPM_CU(c, ensure(c->x_sorted, 3 * n * sizeof(float)));
   CPM_CU(c, ensure(c->acc_sorted, 3 * n * sizeof(float)));
   CPM_CU(c, ensure(c->acc, 3 * n * sizeof(float)));
-  CPM_CU(c, ensure(c->tree_counters, 2 * sizeof(unsigned long long)));
-  CPM_CU(c, cudaMemsetAsync(c->tree_counters.p, 0, 2 * sizeof(unsigned long long), c->stream));
+  CPM_CU(c, ensure(c->tree_counters, sizeof(TreeCounters)));
+  CPM_CU(c, cudaMemsetAsync(c->tree_counters.p, 0, sizeof(TreeCounters), c->stream));
   launch_octant_keys(as<float>(c->x), n, box_size, KEY_LEVELS, as<uint64_t>(c->keys), as<uint32_t>(c->vals),
                      as<DevStatus>(c->status), c->stream);
   CPM_CU(c, radix_sort_pairs(as<uint64_t>(c->keys), as<uint32_t>(c->vals), n, 3 * KEY_LEVELS, c->sort, c->stream));
@@ -334,7 +334,7 @@ int cpm_tree_accel(cpm_ctx* c, const float* x3, size_t n, float box_size, const 
   CPM_CU(c, cudaMemcpy(cnt, c->tree.counters.p, sizeof(cnt), cudaMemcpyDeviceToHost));
   uint64_t nodes = 0;
   for (int d = 0; d <= KEY_LEVELS; ++d) nodes += cnt[d];
-  unsigned long long tc[2];
+  unsigned long long tc[4];
   CPM_CU(c, cudaMemcpy(tc, c->tree_counters.p, sizeof(tc), cudaMemcpyDeviceToHost));
   c->last_nodes = nodes;
   c->last_pairs = tc[0];

@@ -189,11 +189,14 @@ struct TreeNodes {
   DevBuf counters;  // u32[64]: per-level allocation counts, totals
   DevBuf prefix;    // double prefix sums of sorted positions (3 per particle + 3)
   DevBuf scan_tmp;
+  DevBuf x4;        // float4 copy of the sorted positions for the walk
   size_t capacity = 0;
 };
 struct TreeCounters {
-  unsigned long long leaf_pairs;
-  unsigned long long node_accepts;
+  unsigned long long leaf_pairs;    // pairs within r_cut summed directly
+  unsigned long long node_accepts;  // accepted centres of mass
+  unsigned long long candidates;    // (particle, source) pairs tested against r_cut in direct nodes
+  unsigned long long reserved;
 };
 // Builds the octree over sorted keys/positions (sorted x as AoS f32). Returns the node count
 // through the counters buffer (read by tree_node_count).

@@ -125,7 +125,7 @@ static int sim_accelerations(cpm_sim* s, float a) {
     SIM_CU(s, tree_build(s->tree, as<uint64_t>(s->keys), as<float>(s->x), n, s->box, as<DevStatus>(s->status),
                          s->stream));
     mark(s, 6);
-    SIM_CU(s, cudaMemsetAsync(s->counters.p, 0, 2 * sizeof(unsigned long long), s->stream));
+    SIM_CU(s, cudaMemsetAsync(s->counters.p, 0, sizeof(TreeCounters), s->stream));
     const float k = tree_coupling(s->P.cosmo.omega_m, s->box, a, n);
     launch_tree_walk(s->tree, as<float>(s->x), n, s->box, s->P.split, k, as<float>(s->acc), 1,
                      as<TreeCounters>(s->counters), as<DevStatus>(s->status), s->stream);
@@ -175,14 +175,14 @@ static int sim_new(const cpm_sim_params* params, float a0, cpm_sim** out) {
   for (DevBuf* b : {&s->gx, &s->gy, &s->gz}) ok = ok && ensure(*b, m * sizeof(float)) == cudaSuccess;
   ok = ok && ensure(s->spec, 3 * half * sizeof(float2)) == cudaSuccess;
   ok = ok && ensure(s->status, sizeof(DevStatus)) == cudaSuccess;
-  ok = ok && ensure(s->counters, 2 * sizeof(unsigned long long)) == cudaSuccess;
+  ok = ok && ensure(s->counters, sizeof(TreeCounters)) == cudaSuccess;
   ok = ok && fft_plan_init(s->plan, P.mesh_n) == cudaSuccess;
   if (!ok) {
     s->err = "cpm_sim_create: device allocation failed";
     return fail(CPM_E_NOMEM);
   }
   cudaMemsetAsync(s->status.p, 0, sizeof(DevStatus), s->stream);
-  cudaMemsetAsync(s->counters.p, 0, 2 * sizeof(unsigned long long), s->stream);
+  cudaMemsetAsync(s->counters.p, 0, sizeof(TreeCounters), s->stream);
   *out = s;
   return CPM_OK;
 }
@@ -344,11 +344,20 @@ int cpm_sim_phase_times(cpm_sim* s, double* ms8, uint64_t* steps, int reset) {
   return CPM_OK;
 }
 
+int cpm_sim_walk_candidates(cpm_sim* s, uint64_t* candidates) {
+  if (!s || !candidates) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_walk_candidates: null pointer");
+  SIM_CU(s, cudaStreamSynchronize(s->stream));
+  unsigned long long tc[4] = {0, 0, 0, 0};
+  SIM_CU(s, cudaMemcpy(tc, s->counters.p, sizeof(tc), cudaMemcpyDeviceToHost));
+  *candidates = tc[2];
+  return CPM_OK;
+}
+
 int cpm_sim_counters(cpm_sim* s, uint64_t* nodes, uint64_t* leaf_pairs, uint64_t* node_accepts,
                      uint32_t* launches_per_step) {
   if (!s) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_counters: sim is NULL");
   SIM_CU(s, cudaStreamSynchronize(s->stream));
-  unsigned long long tc[2] = {0, 0};
+  unsigned long long tc[4] = {0, 0, 0, 0};
   SIM_CU(s, cudaMemcpy(tc, s->counters.p, sizeof(tc), cudaMemcpyDeviceToHost));
   uint64_t nn = 0;
   if (s->tree.counters.p) {
@@ -370,7 +379,7 @@ int cpm_sim_destroy(cpm_sim* s) {
   if (s->stream) cudaStreamSynchronize(s->stream);
   fft_plan_free(s->plan);
   for (DevBuf* b : {&s->sort.keys_alt, &s->sort.vals_alt, &s->sort.block_hist, &s->sort.scan_tmp, &s->tree.geo,
-                    &s->tree.mass, &s->tree.link, &s->tree.counters, &s->tree.prefix, &s->tree.scan_tmp, &s->x, &s->p,
+                    &s->tree.mass, &s->tree.link, &s->tree.counters, &s->tree.prefix, &s->tree.scan_tmp, &s->tree.x4, &s->x, &s->p,
                     &s->acc, &s->id, &s->x2, &s->p2, &s->id2, &s->keys, &s->vals, &s->fx, &s->gx, &s->gy, &s->gz,
                     &s->spec, &s->status, &s->counters})
     release(*b);

@@ -1,4 +1,4 @@
-// tree.cu — octree build from sorted octant keys and the short-range walk (tree.rs:171-323).
+// tree.cu — octree build from sorted octant keys (tree.rs:171-250). The walk is in walk.cu.
 //
 // Build. Particles are sorted by their 63-bit octant key (21 digits of the reference's descent,
 // tree.rs:186-250), so every node of the reference's tree is a contiguous range of the sorted
@@ -13,17 +13,6 @@
 // Centres of mass come from an FP64 exclusive prefix sum of the sorted positions: the sum over a
 // node is P[end] - P[start], divided by the count and rounded once to f32. (The reference sums
 // in f32 sequentially in input order; the difference is f32 round-off of that sum.)
-//
-// Walk. One warp walks for 32 consecutive sorted particles with one shared LIFO stack of
-// (node, lane mask) entries. A lane is in a node's mask exactly when its own reference walk
-// (tree.rs:264-310) would pop that node; each lane applies the reference's tests for itself:
-// prune when |min_image(centre - x)| > r_cut + sqrt(3) half; direct sum over the node's particles
-// when its octant-0 child is missing (`children[0] == NO_CHILD`, which includes leaves); else
-// accept the centre of mass when 2 half < theta |min_image(com - x)|, or push the children 0..7
-// for the lanes that opened it. Popping order is the reference's (7 first), so each lane adds its
-// contributions in the reference's node order. The tests use separately rounded f32 operations
-// and an exact minimum image, so accept/prune/cutoff decisions match the reference for equal
-// inputs.
 #include <algorithm>
 #include <vector>
 
@@ -272,190 +261,6 @@ cudaError_t tree_build(TreeNodes& t, const uint64_t* sorted_keys, const float* s
   count_launch();
   k_tree_com<<<BUILD_BLOCKS, BUILD_THREADS, 0, s>>>(link, P, as<float4>(t.mass), counters, (uint32_t)t.capacity);
   return cudaGetLastError();
-}
-
-// ---------------------------------------------------------------------------------------------
-// Walk
-// ---------------------------------------------------------------------------------------------
-constexpr int WALK_WARPS = 4;
-constexpr int WALK_THREADS = WALK_WARPS * 32;
-constexpr int STACK_CAP = 8 * (KEY_LEVELS + 2);
-
-struct WalkParams {
-  float box;
-  float half_box_guard;  // |x| below this: round(x / L) == 0 exactly
-  float r_cut;
-  float cut2;            // r_cut * r_cut
-  float theta;
-  float r_split;
-  float two_rs;          // 2 * r_split
-  float eps2;            // softening^2
-  float k;               // Newtonian coupling
-};
-
-// tree.rs:253-261: d = x - L round(x / L), with x = a - b. For |x| < 0.49 L the quotient rounds
-// to 0 whatever its last bit, so only the remaining cases need the IEEE division.
-__device__ __forceinline__ float min_image1(float a, float b, const WalkParams& w) {
-  const float x = __fsub_rn(a, b);
-  if (fabsf(x) < w.half_box_guard) return x;
-  const float q = roundf(__fdiv_rn(x, w.box));
-  return __fsub_rn(x, __fmul_rn(w.box, q));
-}
-
-__device__ __forceinline__ float norm2(float a, float b, float c) {
-  return __fadd_rn(__fadd_rn(__fmul_rn(a, a), __fmul_rn(b, b)), __fmul_rn(c, c));
-}
-
-// tree.rs:54-66: f = -K m S(r) / (r^2 + eps^2)^{3/2}, S(r) = erfc(u) + (2/sqrt(pi)) u e^{-u^2}, u = r/(2 r_s)
-__device__ __forceinline__ void add_pair(float d0, float d1, float d2, float r2, float mass, const WalkParams& w,
-                                         float& a0, float& a1, float& a2) {
-  const float s = __fadd_rn(r2, w.eps2);
-  const float r = sqrtf(r2);
-  const float u = __fdiv_rn(r, w.two_rs);
-  const float S = __fadd_rn(erfcf(u), __fmul_rn(__fmul_rn(TWO_OVER_SQRT_PI, u), expf(__fmul_rn(-u, u))));
-  const float f = __fdiv_rn(__fmul_rn(__fmul_rn(-w.k, mass), S), __fmul_rn(s, sqrtf(s)));
-  a0 = __fadd_rn(a0, __fmul_rn(d0, f));
-  a1 = __fadd_rn(a1, __fmul_rn(d1, f));
-  a2 = __fadd_rn(a2, __fmul_rn(d2, f));
-}
-
-__global__ void __launch_bounds__(WALK_THREADS) k_tree_walk(const uint4* __restrict__ link,
-                                                            const float4* __restrict__ geo,
-                                                            const float4* __restrict__ mass,
-                                                            const float* __restrict__ x3, size_t n, WalkParams w,
-                                                            float* __restrict__ acc3, int accumulate,
-                                                            unsigned long long* counters, DevStatus* st) {
-  __shared__ uint2 stack[WALK_WARPS][STACK_CAP];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const size_t i = ((size_t)blockIdx.x * WALK_WARPS + warp) * 32 + lane;
-  const bool valid = i < n;
-  const unsigned group = __ballot_sync(0xffffffffu, valid);
-  if (group == 0) return;
-  float x0 = 0.0f, x1 = 0.0f, x2 = 0.0f;
-  if (valid) {
-    x0 = x3[3 * i];
-    x1 = x3[3 * i + 1];
-    x2 = x3[3 * i + 2];
-  }
-  float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
-  unsigned long long n_pairs = 0, n_accepts = 0;
-  uint2* stk = stack[warp];
-  int sp = 0;
-  if (lane == 0) stk[0] = make_uint2(0u, group);
-  sp = 1;
-  __syncwarp();
-  while (sp > 0) {
-    --sp;
-    const uint2 top = stk[sp];
-    __syncwarp();
-    const uint32_t node = top.x;
-    const bool act = (top.y >> lane) & 1u;
-    const float4 G = __ldg(geo + node);
-    bool live = false;
-    if (act) {
-      const float t0 = min_image1(G.x, x0, w), t1 = min_image1(G.y, x1, w), t2 = min_image1(G.z, x2, w);
-      const float max_r = __fadd_rn(w.r_cut, __fmul_rn(SQRT_3, G.w));
-      live = !(norm2(t0, t1, t2) > __fmul_rn(max_r, max_r));
-    }
-    const unsigned live_mask = __ballot_sync(0xffffffffu, live);
-    if (live_mask == 0) continue;
-    const uint4 L = __ldg(link + node);
-    if ((L.w & 1u) == 0u) {
-      // children[0] == NO_CHILD: direct sum over the node's particles (tree.rs:286-298)
-      for (uint32_t b0 = L.x; b0 < L.y; b0 += 32) {
-        const uint32_t j = b0 + lane;
-        float s0 = 0.0f, s1 = 0.0f, s2 = 0.0f;
-        if (j < L.y) {
-          s0 = __ldg(x3 + 3 * (size_t)j);
-          s1 = __ldg(x3 + 3 * (size_t)j + 1);
-          s2 = __ldg(x3 + 3 * (size_t)j + 2);
-        }
-        const int cnt = (int)min(32u, L.y - b0);
-        for (int t = 0; t < cnt; ++t) {
-          const float y0 = __shfl_sync(0xffffffffu, s0, t);
-          const float y1 = __shfl_sync(0xffffffffu, s1, t);
-          const float y2 = __shfl_sync(0xffffffffu, s2, t);
-          if (live && (size_t)(b0 + t) != i) {
-            const float d0 = min_image1(x0, y0, w), d1 = min_image1(x1, y1, w), d2 = min_image1(x2, y2, w);
-            const float r2 = norm2(d0, d1, d2);
-            if (!(r2 > w.cut2)) {
-              add_pair(d0, d1, d2, r2, 1.0f, w, a0, a1, a2);
-              ++n_pairs;
-            }
-          }
-        }
-      }
-    } else {
-      bool open = false;
-      if (live) {
-        const float4 M = __ldg(mass + node);
-        const float t0 = min_image1(M.x, x0, w), t1 = min_image1(M.y, x1, w), t2 = min_image1(M.z, x2, w);
-        const float r2 = norm2(t0, t1, t2);
-        const float r = sqrtf(r2);
-        if (__fmul_rn(2.0f, G.w) < __fmul_rn(w.theta, r)) {
-          add_pair(-t0, -t1, -t2, r2, M.w, w, a0, a1, a2);
-          ++n_accepts;
-        } else {
-          open = true;
-        }
-      }
-      const unsigned open_mask = __ballot_sync(0xffffffffu, open);
-      if (open_mask) {
-        const uint32_t cmask = L.w & 0xFFu;
-        const int nch = __popc(cmask);
-        if (sp + nch > STACK_CAP) {
-          if (lane == 0) dev_fail(st, DEV_STACK_OVERFLOW, (int)node);
-          break;
-        }
-        if (lane < nch) stk[sp + lane] = make_uint2(L.z + (uint32_t)lane, open_mask);
-        sp += nch;
-        __syncwarp();
-      }
-    }
-  }
-  if (valid) {
-    if (accumulate) {
-      acc3[3 * i] = __fadd_rn(acc3[3 * i], a0);
-      acc3[3 * i + 1] = __fadd_rn(acc3[3 * i + 1], a1);
-      acc3[3 * i + 2] = __fadd_rn(acc3[3 * i + 2], a2);
-    } else {
-      acc3[3 * i] = a0;
-      acc3[3 * i + 1] = a1;
-      acc3[3 * i + 2] = a2;
-    }
-  }
-  if (counters) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      n_pairs += __shfl_xor_sync(0xffffffffu, n_pairs, o);
-      n_accepts += __shfl_xor_sync(0xffffffffu, n_accepts, o);
-    }
-    if (lane == 0) {
-      atomicAdd(&counters[0], n_pairs);
-      atomicAdd(&counters[1], n_accepts);
-    }
-  }
-}
-
-void launch_tree_walk(const TreeNodes& t, const float* sorted_x3, size_t n, float box, const cpm_force_split& split,
-                      float k, float* acc3, int accumulate, TreeCounters* counters, DevStatus* st, cudaStream_t s) {
-  if (n == 0) return;
-  WalkParams w;
-  w.box = box;
-  w.half_box_guard = 0.49f * box;
-  w.r_cut = split.r_cut;
-  w.cut2 = split.r_cut * split.r_cut;
-  w.theta = split.theta;
-  w.r_split = split.r_split;
-  w.two_rs = 2.0f * split.r_split;
-  w.eps2 = split.softening * split.softening;
-  w.k = k;
-  const size_t groups = (n + 31) / 32;
-  const unsigned blocks = (unsigned)((groups + WALK_WARPS - 1) / WALK_WARPS);
-  count_launch();
-  k_tree_walk<<<blocks, WALK_THREADS, 0, s>>>(static_cast<const uint4*>(t.link.p), static_cast<const float4*>(t.geo.p),
-                                              static_cast<const float4*>(t.mass.p), sorted_x3, n, w, acc3, accumulate,
-                                              reinterpret_cast<unsigned long long*>(counters), st);
 }
 
 }  // namespace cpm

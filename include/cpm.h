@@ -200,6 +200,13 @@ int cpm_sim_set_state(cpm_sim* sim, const float* x3, const float* p3);
  * [0] kick+drift, [1] keys+sort+reorder, [2] deposit, [3] FFT-Poisson, [4] gather, [5] tree build,
  * [6] tree walk, [7] whole step. Also the number of steps averaged. */
 int cpm_sim_phase_times(cpm_sim* sim, double* ms8, uint64_t* steps, int reset);
+/* (particle, source) pairs the last step's walk tested against r_cut inside direct-summed nodes
+ * (leaf pairs are the subset within r_cut). */
+int cpm_sim_walk_candidates(cpm_sim* sim, uint64_t* candidates);
+/* Self-check of the walk's pair kernel (host only): largest relative error of its fitted
+ * S(r) = erfc(u) + (2/sqrt(pi)) u e^{-u^2}, u = r / (2 r_split) (tree.rs:54-57), against a
+ * double-precision evaluation on `samples` points of [0, r_cut]. */
+int cpm_walk_kernel_fit_error(float r_split, float r_cut, int samples, double* max_rel_err);
 /* Device-side counters of the last step: nodes, leaf pairs, accepted nodes, kernels launched per step. */
 int cpm_sim_counters(cpm_sim* sim, uint64_t* nodes, uint64_t* leaf_pairs, uint64_t* node_accepts,
                      uint32_t* launches_per_step);

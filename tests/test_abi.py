@@ -75,3 +75,11 @@ def _compile_mirror(native, out_dir):
 def test_cpp_mirror_compiles_and_links(native, tmp_path):
     """include/cpm.hpp (the C++ mirror of the reference interface) builds against the library."""
     assert _compile_mirror(native, tmp_path).exists()
+
+
+@pytest.mark.parametrize("r_split,r_cut", [(0.625, 2.8125), (0.5, 2.0), (0.5, 2.5), (0.4, 1.8), (1.0, 9.0)])
+def test_walk_pair_kernel_fit_is_accurate(native, r_split, r_cut):
+    """The walk's fitted S(r) (tree.rs:54-57) stays within 5e-7 relative of double precision."""
+    err = C.c_double()
+    assert native.lib().cpm_walk_kernel_fit_error(r_split, r_cut, 20001, C.byref(err)) == 0
+    assert err.value < 5e-7, err.value
