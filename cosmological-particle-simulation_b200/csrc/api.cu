@@ -261,14 +261,14 @@ int cpm_poisson_accel(cpm_ctx* c, const float* delta, int n, const cpm_cosmology
   if (!c) return set_error(nullptr, CPM_E_INVALID, "context is NULL");
   if (!delta || !cosmo || !gx || !gy || !gz) return set_error(&c->err, CPM_E_INVALID, "poisson: null pointer");
   if (n != c->n_mesh) return set_error(&c->err, CPM_E_MESH_MISMATCH, "poisson: mesh size must match the solver");
-  if (!fft_supported(n))
-    return set_error(&c->err, CPM_E_UNSUPPORTED, "poisson: n = " + std::to_string(n) + " is not a power of two in [4, 1024]");
+  if (!poisson_supported(n))
+    return set_error(&c->err, CPM_E_UNSUPPORTED, "poisson: n = " + std::to_string(n) + " is not a power of two in [4, 512]");
   if (!(a > 0.0f)) return set_error(&c->err, CPM_E_INVALID, "poisson: a must be > 0");
   int rc = reset_status(c);
   if (rc) return rc;
   CPM_CU(c, fft_plan_init(c->plan, n));
   const size_t m = (size_t)n * n * n;
-  const size_t half = (size_t)n * n * (n / 2 + 1);
+  const size_t half = half_spectrum_elems(n);
   CPM_CU(c, ensure(c->mesh_d, m * sizeof(float)));
   CPM_CU(c, ensure(c->mesh_a, m * sizeof(float)));
   CPM_CU(c, ensure(c->mesh_b, m * sizeof(float)));

@@ -147,10 +147,15 @@ void launch_fixed_to_f32(const unsigned long long* fx, size_t m, int shift, int 
 // FFT / Poisson — fft.cu
 // ---------------------------------------------------------------------------------------------
 bool fft_supported(int n);
+// Mesh sizes the fused Poisson pass supports (its two shared-memory tiles must fit one SM).
+bool poisson_supported(int n);
 struct FftPlan {
   int n = 0;
   DevBuf twiddle;  // exp(-2 pi i m / n), m < n, float2 built from double
+  DevBuf deconv;   // per-axis 1 / sinc^4(pi m / n): CIC window of deposit and gather, squared
 };
+// Elements of one half spectrum [n][n][n/2+2] (one padding column per row).
+size_t half_spectrum_elems(int n);
 cudaError_t fft_plan_init(FftPlan& p, int n);
 void fft_plan_free(FftPlan& p);
 // In-place unnormalised c2c n^3 transform (z, then y, then x lines).

@@ -1,31 +1,55 @@
 // fft.cu — shared-memory Stockham FFTs and the PM Poisson solve (fft.rs:40-95, poisson.rs:33-88).
 //
-// Layouts
-//   real mesh      f32  [n][n][n]          (ix*n + iy)*n + iz, z fastest (mesh.rs:11)
-//   half spectrum  c32  [n][n][n/2+1]      kz in [0, n/2]; the rest follows from Hermitian symmetry
+// Layouts in HBM
+//   real mesh      f32  [n][n][n]            (ix*n + iy)*n + iz, z fastest (mesh.rs:11)
+//   half spectrum  c32  [n][n][n/2+2]        kz in [0, n/2]; one padding column keeps rows 16-byte
+//                                            aligned; the rest of kz follows from Hermitian symmetry
 //
-// Every pass moves a tile of lines between HBM and shared memory once: lines along the
-// contiguous z axis are loaded as rows; lines along y or x are loaded as W adjacent columns, so
-// each row segment of the tile is a contiguous W*8-byte run. Inside shared memory the lines are
-// transformed by radix-8/4/2 Stockham stages (in place: each stage reads its butterflies into
-// registers, synchronises, then writes them to their autosorted positions). Twiddles come from a
-// table exp(-2 pi i m / n) built in double precision on the host.
+// Every pass moves tiles of W = 16 lines between HBM and shared memory once. In shared memory
+// element t of line l sits at t*(W+1) + l ("transposed", line index fastest):
+//   - FFT stages give the line index to consecutive lanes, so each half-warp touches 16
+//     consecutive elements (one 128-byte row) whatever the stage's stride: no bank conflicts;
+//   - transfers of contiguous z rows give t to consecutive lanes; the odd stride W+1 spreads those
+//     16 elements over all banks, again without conflicts;
+//   - transfers of strided y/x lines give the line (the contiguous kz column) to consecutive
+//     lanes, so global accesses are 128-byte rows.
+// Each pass is a persistent kernel that walks its tiles with two shared-memory buffers: while one
+// tile is transformed, the next one streams in with cp.async, so HBM stays busy during the
+// shared-memory work. Lines are transformed by radix-8/4/2 Stockham stages in place (each stage
+// reads its butterflies into registers, synchronises, writes them to their autosorted positions).
+// Twiddles come from a table exp(-2 pi i m / n) built in double precision on the host.
+//
+// Real z lines use the half-length complex transform: z[m] = x[2m] + i x[2m+1] is transformed
+// with n/2 points and split into the n/2+1 outputs with the twiddles of length n (and the
+// reverse for C2R), which halves the arithmetic and shared memory of the z passes.
 //
 // The Poisson solve runs as
-//   1. z pass: R2C of each z row (the input is either f32 delta or the u64 fixed-point mass mesh,
-//      converted to delta = c/mean - 1 on load, integrator.rs:117-126);
+//   1. z pass: R2C of each z row; the input is the f32 delta or the u64 fixed-point mass mesh,
+//      converted in shared memory to delta = c/mean - 1 (integrator.rs:117-126);
 //   2. y pass: forward c2c along y;
-//   3. x pass: forward c2c along x, then the Green's function (poisson.rs:52-74, same f32
-//      operation order) applied once, then for each force component the gradient factor -i k_a
-//      and the inverse c2c along x — three half spectra written;
+//   3. x pass: forward c2c along x, the Green's function of poisson.rs:52-74 in the reference's f32
+//      operation order (optionally divided by the CIC window squared), then two inverse x
+//      transforms: of -i k_x phi (x component) and of phi, which gives the y and z components after
+//      multiplying by -i k_y and -i k_z (constant along an x line) — three half spectra written;
 //   4. y pass: inverse c2c along y of the three spectra;
 //   5. z pass: C2R of each row, scaled by 1/n^3 (poisson.rs:77-87), into three f32 meshes.
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
 #include "cpm_internal.cuh"
 
 namespace cpm {
+
+constexpr int TW = 16;       // lines per tile
+constexpr int TLD = TW + 1;  // shared-memory row pitch (elements)
+constexpr size_t SMEM_LIMIT = 227 * 1024;
+
+// Threads of a CTA that transforms TW lines of length L: one radix-8 butterfly each, 256..1024.
+template <int L>
+constexpr int threads_for() {
+  return TW * L / 8 < 256 ? 256 : (TW * L / 8 > 1024 ? 1024 : TW * L / 8);
+}
 
 // ---------------------------------------------------------------------------------------------
 // Complex helpers and small DFTs
@@ -35,6 +59,7 @@ __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
+__device__ __forceinline__ float2 conjf2(float2 a) { return make_float2(a.x, -a.y); }
 // multiply by exp(sign i pi/2): -i for the forward transform, +i for the inverse
 template <bool INV>
 __device__ __forceinline__ float2 rot90(float2 a) {
@@ -86,33 +111,26 @@ __device__ __forceinline__ void dft(float2* v) {
   else dft8<INV>(v);
 }
 
-// Shared-memory leading dimension of a line (odd float2 stride spreads columns over banks).
-template <int N>
-__host__ __device__ constexpr int line_ld() {
-  return N + 1;
-}
-
-// One Stockham stage of radix R on W lines of length N held in shared memory.
-template <int N, int R, int NS, int W, int THREADS, bool INV>
+// One Stockham stage of radix R on the TW lines of a tile (element t of line l at t*TLD + l),
+// T threads. Twiddle exp(-2 pi i m / N) is tw[m * TS] (TS = 2 when the table is for length 2N).
+template <int N, int R, int NS, bool INV, int T, int TS>
 __device__ __forceinline__ void stockham_stage(float2* sm, const float2* __restrict__ tw) {
   constexpr int NB = N / R;
-  constexpr int TOTAL = W * NB;
-  constexpr int BPT = (TOTAL + THREADS - 1) / THREADS;
-  constexpr int LD = line_ld<N>();
+  constexpr int TOTAL = TW * NB;
+  constexpr int BPT = (TOTAL + T - 1) / T;
   float2 v[BPT][R];
 #pragma unroll
   for (int q = 0; q < BPT; ++q) {
-    const int b = threadIdx.x + q * THREADS;
-    if (TOTAL % THREADS == 0 || b < TOTAL) {
-      const int l = b / NB, j = b % NB;
-      const float2* line = sm + l * LD;
+    const int b = threadIdx.x + q * T;
+    if (TOTAL % T == 0 || b < TOTAL) {
+      const int l = b % TW, j = b / TW;
 #pragma unroll
-      for (int r = 0; r < R; ++r) v[q][r] = line[j + r * NB];
+      for (int r = 0; r < R; ++r) v[q][r] = sm[(j + r * NB) * TLD + l];
       if constexpr (NS > 1) {
         const int k = j % NS;
 #pragma unroll
         for (int r = 1; r < R; ++r) {
-          float2 w = __ldg(tw + r * k * (N / (NS * R)));
+          float2 w = __ldg(tw + r * k * (N / (NS * R)) * TS);
           if (INV) w.y = -w.y;
           v[q][r] = cmul(v[q][r], w);
         }
@@ -123,233 +141,386 @@ __device__ __forceinline__ void stockham_stage(float2* sm, const float2* __restr
   __syncthreads();
 #pragma unroll
   for (int q = 0; q < BPT; ++q) {
-    const int b = threadIdx.x + q * THREADS;
-    if (TOTAL % THREADS == 0 || b < TOTAL) {
-      const int l = b / NB, j = b % NB;
+    const int b = threadIdx.x + q * T;
+    if (TOTAL % T == 0 || b < TOTAL) {
+      const int l = b % TW, j = b / TW;
       const int k = j % NS;
-      float2* line = sm + l * LD;
       const int base = (j / NS) * NS * R + k;
 #pragma unroll
-      for (int r = 0; r < R; ++r) line[base + r * NS] = v[q][r];
+      for (int r = 0; r < R; ++r) sm[(base + r * NS) * TLD + l] = v[q][r];
     }
   }
   __syncthreads();
 }
 
-// Full length-N transform of W lines: radix-8 stages, then a final radix-4 or radix-2 stage.
-template <int N, int W, int THREADS, bool INV>
+// Full length-N transform of the tile: radix-8 stages, then a final radix-4 or radix-2 stage.
+template <int N, bool INV, int T, int TS = 1>
 __device__ __forceinline__ void fft_lines(float2* sm, const float2* __restrict__ tw) {
   static_assert((N & (N - 1)) == 0 && N >= 2 && N <= 1024, "power-of-two lengths 2..1024");
   if constexpr (N == 2) {
-    stockham_stage<N, 2, 1, W, THREADS, INV>(sm, tw);
+    stockham_stage<N, 2, 1, INV, T, TS>(sm, tw);
   } else if constexpr (N == 4) {
-    stockham_stage<N, 4, 1, W, THREADS, INV>(sm, tw);
+    stockham_stage<N, 4, 1, INV, T, TS>(sm, tw);
   } else {
-    stockham_stage<N, 8, 1, W, THREADS, INV>(sm, tw);
-    if constexpr (N == 16) stockham_stage<N, 2, 8, W, THREADS, INV>(sm, tw);
-    if constexpr (N == 32) stockham_stage<N, 4, 8, W, THREADS, INV>(sm, tw);
-    if constexpr (N >= 64) stockham_stage<N, 8, 8, W, THREADS, INV>(sm, tw);
-    if constexpr (N == 128) stockham_stage<N, 2, 64, W, THREADS, INV>(sm, tw);
-    if constexpr (N == 256) stockham_stage<N, 4, 64, W, THREADS, INV>(sm, tw);
-    if constexpr (N >= 512) stockham_stage<N, 8, 64, W, THREADS, INV>(sm, tw);
-    if constexpr (N == 1024) stockham_stage<N, 2, 512, W, THREADS, INV>(sm, tw);
+    stockham_stage<N, 8, 1, INV, T, TS>(sm, tw);
+    if constexpr (N == 16) stockham_stage<N, 2, 8, INV, T, TS>(sm, tw);
+    if constexpr (N == 32) stockham_stage<N, 4, 8, INV, T, TS>(sm, tw);
+    if constexpr (N >= 64) stockham_stage<N, 8, 8, INV, T, TS>(sm, tw);
+    if constexpr (N == 128) stockham_stage<N, 2, 64, INV, T, TS>(sm, tw);
+    if constexpr (N == 256) stockham_stage<N, 4, 64, INV, T, TS>(sm, tw);
+    if constexpr (N >= 512) stockham_stage<N, 8, 64, INV, T, TS>(sm, tw);
+    if constexpr (N == 1024) stockham_stage<N, 2, 512, INV, T, TS>(sm, tw);
   }
 }
 
 // ---------------------------------------------------------------------------------------------
-// Tile geometry: element t of line l of tile (o, c) is at
-//   base = o * outer_stride + (c * W + l) * line_stride + t * elem_stride.
-// With line_stride == 1 the W lines are adjacent columns (coalesced rows of W elements); with
-// elem_stride == 1 each line is a contiguous row.
+// Asynchronous global -> shared copies (cp.async, completion tracked per thread by groups)
 // ---------------------------------------------------------------------------------------------
-struct TileGeo {
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int PENDING>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(PENDING) : "memory");
+}
+
+// ---------------------------------------------------------------------------------------------
+// Tile geometry. Strided passes: element t of column c of tile (o, ct) is at
+//   o * outer_stride + (ct * TW + c) + t * elem_stride   (columns contiguous in memory).
+// Row passes: tile r covers rows r*TW .. r*TW + TW - 1, each contiguous.
+// ---------------------------------------------------------------------------------------------
+struct ColGeo {
   long long outer_stride;
-  long long line_stride;
   long long elem_stride;
-  int lines;  // number of lines along the tiled direction
+  int cols;       // valid columns along the contiguous axis
+  int col_tiles;  // ceil(cols / TW)
+  int outer;      // number of outer indices
 };
 
-template <int N, int W, int THREADS>
-__device__ __forceinline__ void load_tile(float2* sm, const float2* __restrict__ src, const TileGeo& g, int valid) {
-  constexpr int LD = line_ld<N>();
-  const long long base = (long long)blockIdx.x * g.outer_stride + (long long)blockIdx.y * W * g.line_stride;
-  for (int q = threadIdx.x; q < N * W; q += THREADS) {
-    int t, l;
-    if (g.line_stride == 1) {
-      l = q % W;
-      t = q / W;
+// Row transfers: chunks of TT = min(L, 16) consecutive t go to consecutive lanes, chunk-major
+// over the TW rows: work item q -> (t, l) with t < L, l < TW.
+template <int L>
+__device__ __forceinline__ int row_t(int q) {
+  constexpr int TT = L < 16 ? L : 16;
+  return (q % TT) + TT * (q / (TT * TW));
+}
+template <int L>
+__device__ __forceinline__ int row_l(int q) {
+  constexpr int TT = L < 16 ? L : 16;
+  return (q / TT) % TW;
+}
+// Work items that cover t < count on every row.
+template <int L>
+__device__ __forceinline__ int row_span(int count) {
+  constexpr int TT = L < 16 ? L : 16;
+  return TT * TW * ((count + TT - 1) / TT);
+}
+
+template <int N, int T>
+__device__ __forceinline__ void async_load_cols(float2* buf, const float2* src, long long base, long long es,
+                                                int valid) {
+  for (int q = threadIdx.x; q < N * TW; q += T) {
+    const int l = q % TW, t = q / TW;
+    if (l < valid) cp_async8(buf + t * TLD + l, src + base + l + (long long)t * es);
+  }
+}
+
+template <int N, int T>
+__device__ __forceinline__ void store_cols(const float2* buf, float2* dst, long long base, long long es, int valid) {
+#pragma unroll 4
+  for (int q = threadIdx.x; q < N * TW; q += T) {
+    const int l = q % TW, t = q / TW;
+    if (l < valid) dst[base + l + (long long)t * es] = buf[t * TLD + l];
+  }
+}
+
+// Persistent pipeline: each CTA walks tiles blockIdx.x, +gridDim.x, ...; with NBUF = 2 the next
+// tile's copies are in flight while the current one is processed. `tile_elems` is the size of one
+// buffer in float2 units.
+template <int NBUF, typename Load, typename Work>
+__device__ __forceinline__ void pipeline(float2* smem, int tile_elems, int total, Load load, Work work) {
+  int k = 0;
+  int tile = blockIdx.x;
+  if (tile < total) load(smem, tile);
+  cp_async_commit();
+  for (; tile < total; tile += gridDim.x, ++k) {
+    const int next = tile + gridDim.x;
+    float2* cur = smem + (NBUF == 2 ? (k & 1) * tile_elems : 0);
+    if constexpr (NBUF == 2) {
+      if (next < total) load(smem + ((k + 1) & 1) * tile_elems, next);
+      cp_async_commit();
+      cp_async_wait<1>();
     } else {
-      t = q % N;
-      l = q / N;
-    }
-    if (l < valid) sm[l * LD + t] = src[base + (long long)l * g.line_stride + (long long)t * g.elem_stride];
-  }
-}
-
-template <int N, int W, int THREADS>
-__device__ __forceinline__ void store_tile(const float2* sm, float2* __restrict__ dst, const TileGeo& g, int valid) {
-  constexpr int LD = line_ld<N>();
-  const long long base = (long long)blockIdx.x * g.outer_stride + (long long)blockIdx.y * W * g.line_stride;
-  for (int q = threadIdx.x; q < N * W; q += THREADS) {
-    int t, l;
-    if (g.line_stride == 1) {
-      l = q % W;
-      t = q / W;
-    } else {
-      t = q % N;
-      l = q / N;
-    }
-    if (l < valid) dst[base + (long long)l * g.line_stride + (long long)t * g.elem_stride] = sm[l * LD + t];
-  }
-}
-
-// Generic c2c pass over one axis (gridDim.z selects one of up to 3 arrays spaced by comp_stride).
-template <int N, int W, int THREADS, bool INV>
-__global__ void __launch_bounds__(THREADS) k_fft_pass(float2* data, long long comp_stride, TileGeo g,
-                                                      const float2* __restrict__ tw) {
-  extern __shared__ float2 sm[];
-  float2* d = data + (long long)blockIdx.z * comp_stride;
-  const int valid = min(W, g.lines - (int)blockIdx.y * W);
-  load_tile<N, W, THREADS>(sm, d, g, valid);
-  __syncthreads();
-  fft_lines<N, W, THREADS, INV>(sm, tw);
-  store_tile<N, W, THREADS>(sm, d, g, valid);
-}
-
-// z pass, forward: W real rows of length N -> N/2+1 complex each. Input is either f32 delta or
-// the u64 fixed-point mass mesh (cell mass c = fx * 2^-k in f32, delta = c / mean - 1).
-template <int N, int W, int THREADS>
-__global__ void __launch_bounds__(THREADS) k_r2c_z(const float* __restrict__ delta,
-                                                   const unsigned long long* __restrict__ fx, float inv_scale,
-                                                   float mean, float2* __restrict__ spec, int rows,
-                                                   const float2* __restrict__ tw) {
-  extern __shared__ float2 sm[];
-  constexpr int LD = line_ld<N>();
-  constexpr int NH = N / 2 + 1;
-  const int row0 = blockIdx.x * W;
-  const int valid = min(W, rows - row0);
-  for (int q = threadIdx.x; q < N * W; q += THREADS) {
-    const int l = q / N, t = q % N;
-    if (l < valid) {
-      const size_t gi = (size_t)(row0 + l) * N + t;
-      float v;
-      if (fx) {
-        const float c = __fmul_rn(__ull2float_rn(fx[gi]), inv_scale);
-        v = __fsub_rn(__fdiv_rn(c, mean), 1.0f);
-      } else {
-        v = delta[gi];
-      }
-      sm[l * LD + t] = make_float2(v, 0.0f);
-    }
-  }
-  __syncthreads();
-  fft_lines<N, W, THREADS, false>(sm, tw);
-  for (int q = threadIdx.x; q < NH * W; q += THREADS) {
-    const int l = q / NH, t = q % NH;
-    if (l < valid) spec[(size_t)(row0 + l) * NH + t] = sm[l * LD + t];
-  }
-}
-
-// z pass, inverse: N/2+1 complex per row -> N real values (Hermitian extension), times scale.
-template <int N, int W, int THREADS>
-__global__ void __launch_bounds__(THREADS) k_c2r_z(const float2* __restrict__ spec, long long comp_stride,
-                                                   float* __restrict__ out0, float* __restrict__ out1,
-                                                   float* __restrict__ out2, float scale, int rows,
-                                                   const float2* __restrict__ tw) {
-  extern __shared__ float2 sm[];
-  constexpr int LD = line_ld<N>();
-  constexpr int NH = N / 2 + 1;
-  const float2* sp = spec + (long long)blockIdx.z * comp_stride;
-  float* out = blockIdx.z == 0 ? out0 : (blockIdx.z == 1 ? out1 : out2);
-  const int row0 = blockIdx.x * W;
-  const int valid = min(W, rows - row0);
-  for (int q = threadIdx.x; q < NH * W; q += THREADS) {
-    const int l = q / NH, t = q % NH;
-    if (l < valid) {
-      const float2 v = sp[(size_t)(row0 + l) * NH + t];
-      sm[l * LD + t] = v;
-      if (t > 0 && t < N / 2) sm[l * LD + (N - t)] = make_float2(v.x, -v.y);
-    }
-  }
-  __syncthreads();
-  fft_lines<N, W, THREADS, true>(sm, tw);
-  for (int q = threadIdx.x; q < N * W; q += THREADS) {
-    const int l = q / N, t = q % N;
-    if (l < valid) out[(size_t)(row0 + l) * N + t] = __fmul_rn(sm[l * LD + t].x, scale);
-  }
-}
-
-// x pass of the Poisson solve: forward c2c along x of W kz-columns at fixed ky, the Green's
-// function of poisson.rs:52-74, then per component the factor -i k_a and the inverse c2c along x.
-// blockIdx.x = iy, blockIdx.y = kz tile. spec_in: forward half spectrum after the y pass.
-// spec_out: 3 half spectra (component stride comp_stride).
-template <int N, int W, int THREADS>
-__global__ void __launch_bounds__(THREADS) k_poisson_x(const float2* __restrict__ spec_in, float2* spec_out,
-                                                       long long comp_stride, TileGeo g, PoissonParams pp,
-                                                       const float* __restrict__ deconv,
-                                                       const float2* __restrict__ tw) {
-  extern __shared__ float2 sm[];
-  constexpr int LD = line_ld<N>();
-  float2* phi = sm;
-  float2* work = sm + W * LD;
-  const int valid = min(W, g.lines - (int)blockIdx.y * W);
-  load_tile<N, W, THREADS>(phi, spec_in, g, valid);
-  __syncthreads();
-  fft_lines<N, W, THREADS, false>(phi, tw);
-
-  const int iy = blockIdx.x;
-  const int z0 = blockIdx.y * W;
-  const float ky = wavenumber(iy, N, pp.two_pi_over_l);
-  // phi_k = delta_k * (-prefactor / k^2 * exp(-k^2 r_s^2)), k = 0 skipped (left zero).
-  for (int q = threadIdx.x; q < N * W; q += THREADS) {
-    const int l = q / N, t = q % N;
-    if (l >= valid) continue;
-    const float kx = wavenumber(t, N, pp.two_pi_over_l);
-    const float kz = wavenumber(z0 + l, N, pp.two_pi_over_l);
-    float k2 = -0.0f;
-    k2 = __fadd_rn(k2, __fmul_rn(kx, kx));
-    k2 = __fadd_rn(k2, __fmul_rn(ky, ky));
-    k2 = __fadd_rn(k2, __fmul_rn(kz, kz));
-    float2 v = phi[l * LD + t];
-    if (k2 == 0.0f) {
-      v = make_float2(0.0f, 0.0f);
-    } else {
-      const float filter = expf(__fmul_rn(__fmul_rn(-k2, pp.r_split), pp.r_split));
-      float sc = __fmul_rn(__fdiv_rn(-pp.prefactor, k2), filter);
-      if (deconv) sc = __fmul_rn(sc, __fmul_rn(__fmul_rn(deconv[t], deconv[iy]), deconv[z0 + l]));
-      v = make_float2(__fmul_rn(v.x, sc), __fmul_rn(v.y, sc));
-    }
-    phi[l * LD + t] = v;
-  }
-  __syncthreads();
-  for (int comp = 0; comp < 3; ++comp) {
-    // g_k = phi_k * (0 - i k_a): re = phi.re*0 - phi.im*(-k_a), im = phi.re*(-k_a) + phi.im*0
-    for (int q = threadIdx.x; q < N * W; q += THREADS) {
-      const int l = q / N, t = q % N;
-      if (l >= valid) continue;
-      float ka;
-      if (comp == 0) ka = wavenumber(t, N, pp.two_pi_over_l);
-      else if (comp == 1) ka = ky;
-      else ka = wavenumber(z0 + l, N, pp.two_pi_over_l);
-      const float2 p = phi[l * LD + t];
-      const float nk = -ka;
-      work[l * LD + t] = make_float2(__fsub_rn(__fmul_rn(p.x, 0.0f), __fmul_rn(p.y, nk)),
-                                     __fadd_rn(__fmul_rn(p.x, nk), __fmul_rn(p.y, 0.0f)));
+      cp_async_wait<0>();
     }
     __syncthreads();
-    fft_lines<N, W, THREADS, true>(work, tw);
-    store_tile<N, W, THREADS>(work, spec_out + (long long)comp * comp_stride, g, valid);
+    work(cur, tile);
     __syncthreads();
+    if constexpr (NBUF == 1) {
+      if (next < total) load(cur, next);
+      cp_async_commit();
+    }
   }
+  cp_async_wait<0>();
+}
+
+// c2c pass over a strided axis; tile -> (comp, outer, column tile).
+template <int N, bool INV, int NBUF, int T>
+__global__ void __launch_bounds__(T) k_fft_cols(float2* data, long long comp_stride, ColGeo g, int ncomp,
+                                                const float2* __restrict__ tw) {
+  extern __shared__ float2 smem[];
+  const int per_comp = g.outer * g.col_tiles;
+  auto locate = [&](int tile, long long& base, int& valid, float2*& d) {
+    const int comp = tile / per_comp, rest = tile % per_comp;
+    const int o = rest / g.col_tiles, ct = rest % g.col_tiles;
+    d = data + (long long)comp * comp_stride;
+    base = (long long)o * g.outer_stride + (long long)ct * TW;
+    valid = min(TW, g.cols - ct * TW);
+  };
+  pipeline<NBUF>(
+      smem, N * TLD, ncomp * per_comp,
+      [&](float2* buf, int tile) {
+        long long base;
+        int valid;
+        float2* d;
+        locate(tile, base, valid, d);
+        async_load_cols<N, T>(buf, d, base, g.elem_stride, valid);
+      },
+      [&](float2* cur, int tile) {
+        long long base;
+        int valid;
+        float2* d;
+        locate(tile, base, valid, d);
+        fft_lines<N, INV, T>(cur, tw);
+        store_cols<N, T>(cur, d, base, g.elem_stride, valid);
+      });
+}
+
+// c2c pass over contiguous rows (the z lines of a full complex n^3 array).
+template <int N, bool INV, int NBUF, int T>
+__global__ void __launch_bounds__(T) k_fft_rows(float2* data, int rows, const float2* __restrict__ tw) {
+  extern __shared__ float2 smem[];
+  pipeline<NBUF>(
+      smem, N * TLD, (rows + TW - 1) / TW,
+      [&](float2* buf, int tile) {
+        const int row0 = tile * TW, valid = min(TW, rows - row0);
+        for (int q = threadIdx.x; q < N * TW; q += T) {
+          const int t = row_t<N>(q), l = row_l<N>(q);
+          if (l < valid) cp_async8(buf + t * TLD + l, data + (size_t)(row0 + l) * N + t);
+        }
+      },
+      [&](float2* cur, int tile) {
+        const int row0 = tile * TW, valid = min(TW, rows - row0);
+        fft_lines<N, INV, T>(cur, tw);
+#pragma unroll 4
+        for (int q = threadIdx.x; q < N * TW; q += T) {
+          const int t = row_t<N>(q), l = row_l<N>(q);
+          if (l < valid) data[(size_t)(row0 + l) * N + t] = cur[t * TLD + l];
+        }
+      });
+}
+
+// z pass, forward: TW real rows of length N -> N/2+1 complex each (rows of the padded half
+// spectrum), as an N/2-point complex transform of z[m] = x[2m] + i x[2m+1]. Input: f32 delta, or
+// the u64 fixed-point mass mesh (c = fx * 2^-k in f32, delta = c / mean - 1). The raw pairs land
+// in 16-byte slots of a staging buffer and are converted into the complex tile.
+// Shared memory: NBUF staging buffers of M*TLD 16-byte slots, then the M*TLD complex tile.
+template <int N, int NBUF, int T>
+__global__ void __launch_bounds__(T) k_r2c_z(const float* __restrict__ delta,
+                                             const unsigned long long* __restrict__ fx, float inv_scale, float mean,
+                                             float2* __restrict__ spec, int rows, const float2* __restrict__ tw) {
+  extern __shared__ float2 smem[];
+  constexpr int M = N / 2, NH = N / 2 + 1, NHP = N / 2 + 2;
+  float2* cplx = smem + NBUF * 2 * M * TLD;
+  pipeline<NBUF>(
+      smem, 2 * M * TLD, (rows + TW - 1) / TW,
+      [&](float2* buf, int tile) {
+        const int row0 = tile * TW, valid = min(TW, rows - row0);
+        for (int q = threadIdx.x; q < M * TW; q += T) {
+          const int m = row_t<M>(q), l = row_l<M>(q);
+          if (l >= valid) continue;
+          const size_t gi = (size_t)(row0 + l) * N + 2 * m;
+          if (fx)
+            cp_async16(buf + 2 * (m * TLD + l), fx + gi);
+          else
+            cp_async8(buf + 2 * (m * TLD + l), delta + gi);
+        }
+      },
+      [&](float2* raw, int tile) {
+        const int row0 = tile * TW, valid = min(TW, rows - row0);
+        for (int q = threadIdx.x; q < M * TW; q += T) {
+          const int l = q % TW, m = q / TW;
+          float2 v = make_float2(0.0f, 0.0f);
+          if (l < valid) {
+            if (fx) {
+              const ulonglong2 u = reinterpret_cast<const ulonglong2*>(raw)[m * TLD + l];
+              const float c0 = __fmul_rn(__ull2float_rn(u.x), inv_scale);
+              const float c1 = __fmul_rn(__ull2float_rn(u.y), inv_scale);
+              v = make_float2(__fsub_rn(__fdiv_rn(c0, mean), 1.0f), __fsub_rn(__fdiv_rn(c1, mean), 1.0f));
+            } else {
+              v = raw[2 * (m * TLD + l)];
+            }
+          }
+          cplx[m * TLD + l] = v;
+        }
+        __syncthreads();
+        fft_lines<M, false, T, 2>(cplx, tw);
+        // X[k] = (Z[k] + conj(Z[M-k]))/2 + w^k (Z[k] - conj(Z[M-k]))/(2i), w = exp(-2 pi i / N)
+        for (int q = threadIdx.x; q < row_span<M>(NH); q += T) {
+          const int k = row_t<M>(q), l = row_l<M>(q);
+          if (l >= valid || k >= NH) continue;
+          const float2 zk = cplx[(k & (M - 1)) * TLD + l];
+          const float2 zm = cplx[((M - k) & (M - 1)) * TLD + l];
+          const float2 fe = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+          const float2 fo = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+          spec[(size_t)(row0 + l) * NHP + k] = cadd(fe, cmul(__ldg(tw + k), fo));
+        }
+      });
+}
+
+// z pass, inverse: N/2+1 complex per row -> N real values times scale, as an N/2-point complex
+// inverse transform of Z'[k] = (X[k] + conj(X[M-k])) + i (X[k] - conj(X[M-k])) conj(w^k), whose
+// output is x[2m] + i x[2m+1]. tile -> (comp, row tile). Shared memory: NBUF tiles of (M+1)*TLD.
+template <int N, int NBUF, int T>
+__global__ void __launch_bounds__(T) k_c2r_z(const float2* __restrict__ spec, long long comp_stride,
+                                             float* __restrict__ out0, float* __restrict__ out1,
+                                             float* __restrict__ out2, float scale, int rows,
+                                             const float2* __restrict__ tw) {
+  extern __shared__ float2 smem[];
+  constexpr int M = N / 2, NH = N / 2 + 1, NHP = N / 2 + 2;
+  const int row_tiles = (rows + TW - 1) / TW;
+  pipeline<NBUF>(
+      smem, (M + 1) * TLD, 3 * row_tiles,
+      [&](float2* buf, int tile) {
+        const int comp = tile / row_tiles, row0 = (tile % row_tiles) * TW, valid = min(TW, rows - row0);
+        const float2* sp = spec + (long long)comp * comp_stride;
+        for (int q = threadIdx.x; q < row_span<M>(NH); q += T) {
+          const int t = row_t<M>(q), l = row_l<M>(q);
+          if (l < valid && t < NH) cp_async8(buf + t * TLD + l, sp + (size_t)(row0 + l) * NHP + t);
+        }
+      },
+      [&](float2* cur, int tile) {
+        const int comp = tile / row_tiles, row0 = (tile % row_tiles) * TW, valid = min(TW, rows - row0);
+        float* out = comp == 0 ? out0 : (comp == 1 ? out1 : out2);
+        for (int q = threadIdx.x; q < (M / 2 + 1) * TW; q += T) {
+          const int l = q % TW, k = q / TW;
+          float2 xk = cur[k * TLD + l], xm = cur[(M - k) * TLD + l];
+          // X[0] and X[M] enter the real output through their real parts only (as in Re of a
+          // full complex inverse); their imaginary parts are round-off of the Hermitian planes.
+          if (k == 0) xk.y = xm.y = 0.0f;
+          const float2 wk = __ldg(tw + k);
+          // Z'[k] and, for 0 < k < M/2, Z'[M-k] (w^(M-k) = -conj(w^k))
+          const float2 a = cadd(xk, conjf2(xm)), b = csub(xk, conjf2(xm));
+          const float2 bw = cmul(b, conjf2(wk));
+          cur[k * TLD + l] = make_float2(a.x - bw.y, a.y + bw.x);
+          if (k > 0 && 2 * k < M) {
+            const float2 a2 = cadd(xm, conjf2(xk)), b2 = csub(xm, conjf2(xk));
+            const float2 bw2 = cmul(b2, make_float2(-wk.x, -wk.y));
+            cur[(M - k) * TLD + l] = make_float2(a2.x - bw2.y, a2.y + bw2.x);
+          }
+        }
+        __syncthreads();
+        fft_lines<M, true, T, 2>(cur, tw);
+#pragma unroll 4
+        for (int q = threadIdx.x; q < M * TW; q += T) {
+          const int m = row_t<M>(q), l = row_l<M>(q);
+          if (l < valid) {
+            const float2 v = cur[m * TLD + l];
+            reinterpret_cast<float2*>(out + (size_t)(row0 + l) * N)[m] =
+                make_float2(__fmul_rn(v.x, scale), __fmul_rn(v.y, scale));
+          }
+        }
+      });
+}
+
+// x pass of the Poisson solve for TW kz columns at fixed ky (tile -> (iy, column tile)): forward
+// c2c along x, the Green's function of poisson.rs:52-74, then
+//   x component: inverse x transform of -i k_x phi;
+//   y, z components: -i k_y and -i k_z times the inverse x transform of phi (k_y, k_z constant
+//   along the line, so the factor commutes with the transform).
+// The gradient factor is the reference's (phi * (0 - i k_a), poisson.rs:70); for y and z it
+// multiplies the transformed phi instead, which differs only in round-off.
+// Shared memory: NBUF input tiles, then one work tile for -i k_x phi.
+template <int N, int NBUF, int T>
+__global__ void __launch_bounds__(T) k_poisson_x(const float2* __restrict__ spec_in, float2* spec_out,
+                                                 long long comp_stride, ColGeo g, PoissonParams pp,
+                                                 const float* __restrict__ deconv, const float2* __restrict__ tw) {
+  extern __shared__ float2 smem[];
+  float2* gxb = smem + NBUF * N * TLD;
+  pipeline<NBUF>(
+      smem, N * TLD, g.outer * g.col_tiles,
+      [&](float2* buf, int tile) {
+        const int iy = tile / g.col_tiles, ct = tile % g.col_tiles;
+        const long long base = (long long)iy * g.outer_stride + (long long)ct * TW;
+        async_load_cols<N, T>(buf, spec_in, base, g.elem_stride, min(TW, g.cols - ct * TW));
+      },
+      [&](float2* phi, int tile) {
+        const int iy = tile / g.col_tiles, ct = tile % g.col_tiles;
+        const int valid = min(TW, g.cols - ct * TW);
+        const long long base = (long long)iy * g.outer_stride + (long long)ct * TW;
+        const int z0 = ct * TW;
+        fft_lines<N, false, T>(phi, tw);
+        const float ky = wavenumber(iy, N, pp.two_pi_over_l);
+        for (int q = threadIdx.x; q < N * TW; q += T) {
+          const int l = q % TW, t = q / TW;
+          const float kx = wavenumber(t, N, pp.two_pi_over_l);
+          const float kz = wavenumber(min(z0 + l, N / 2), N, pp.two_pi_over_l);
+          float k2 = -0.0f;
+          k2 = __fadd_rn(k2, __fmul_rn(kx, kx));
+          k2 = __fadd_rn(k2, __fmul_rn(ky, ky));
+          k2 = __fadd_rn(k2, __fmul_rn(kz, kz));
+          float2 v = phi[t * TLD + l];
+          if (k2 == 0.0f || l >= valid) {
+            v = make_float2(0.0f, 0.0f);
+          } else {
+            // phi_k = delta_k * (-prefactor / k^2 * exp(-k^2 r_s^2)), k = 0 skipped (left zero)
+            const float filter = expf(__fmul_rn(__fmul_rn(-k2, pp.r_split), pp.r_split));
+            float sc = __fmul_rn(__fdiv_rn(-pp.prefactor, k2), filter);
+            if (deconv) sc = __fmul_rn(sc, __fmul_rn(__fmul_rn(deconv[t], deconv[iy]), deconv[z0 + l]));
+            v = make_float2(__fmul_rn(v.x, sc), __fmul_rn(v.y, sc));
+          }
+          phi[t * TLD + l] = v;
+          // -i k_x phi: re = phi.re*0 - phi.im*(-k_x), im = phi.re*(-k_x) + phi.im*0
+          const float nk = -kx;
+          gxb[t * TLD + l] = make_float2(__fsub_rn(__fmul_rn(v.x, 0.0f), __fmul_rn(v.y, nk)),
+                                         __fadd_rn(__fmul_rn(v.x, nk), __fmul_rn(v.y, 0.0f)));
+        }
+        __syncthreads();
+        fft_lines<N, true, T>(gxb, tw);
+        fft_lines<N, true, T>(phi, tw);
+        const float nky = -ky;
+#pragma unroll 2
+        for (int q = threadIdx.x; q < N * TW; q += T) {
+          const int l = q % TW, t = q / TW;
+          if (l >= valid) continue;
+          const long long gi = base + l + (long long)t * g.elem_stride;
+          spec_out[gi] = gxb[t * TLD + l];
+          const float2 p = phi[t * TLD + l];
+          const float nkz = -wavenumber(z0 + l, N, pp.two_pi_over_l);
+          spec_out[comp_stride + gi] = make_float2(__fsub_rn(__fmul_rn(p.x, 0.0f), __fmul_rn(p.y, nky)),
+                                                   __fadd_rn(__fmul_rn(p.x, nky), __fmul_rn(p.y, 0.0f)));
+          spec_out[2 * comp_stride + gi] = make_float2(__fsub_rn(__fmul_rn(p.x, 0.0f), __fmul_rn(p.y, nkz)),
+                                                       __fadd_rn(__fmul_rn(p.x, nkz), __fmul_rn(p.y, 0.0f)));
+        }
+      });
 }
 
 // ---------------------------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------------------------
 bool fft_supported(int n) { return n >= 4 && n <= 1024 && (n & (n - 1)) == 0; }
+bool poisson_supported(int n) { return fft_supported(n) && n <= 512; }
+
+size_t half_spectrum_elems(int n) { return (size_t)n * n * (size_t)(n / 2 + 2); }
 
 cudaError_t fft_plan_init(FftPlan& p, int n) {
-  if (p.n == n && p.twiddle.p) return cudaSuccess;
+  if (p.n == n && p.twiddle.p && p.deconv.p) return cudaSuccess;
   p.n = n;
   std::vector<float2> tw(n);
   const double two_pi = 6.283185307179586476925286766559;
@@ -357,53 +528,82 @@ cudaError_t fft_plan_init(FftPlan& p, int n) {
     const double a = -two_pi * (double)m / (double)n;
     tw[m] = make_float2((float)std::cos(a), (float)std::sin(a));
   }
+  // CIC deconvolution per axis: 1 / W(k)^2 with W = sinc^2(pi m / n) (deposit and gather)
+  std::vector<float> dc(n);
+  for (int i = 0; i < n; ++i) {
+    const int m = i <= n / 2 ? i : i - n;
+    const double x = 3.14159265358979323846 * (double)m / (double)n;
+    const double s = m == 0 ? 1.0 : std::sin(x) / x;
+    dc[i] = (float)(1.0 / (s * s * s * s));
+  }
   cudaError_t e = ensure(p.twiddle, n * sizeof(float2));
-  if (e != cudaSuccess) return e;
-  return cudaMemcpy(p.twiddle.p, tw.data(), n * sizeof(float2), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = ensure(p.deconv, n * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemcpy(p.twiddle.p, tw.data(), n * sizeof(float2), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(p.deconv.p, dc.data(), n * sizeof(float), cudaMemcpyHostToDevice);
+  return e;
 }
 
 void fft_plan_free(FftPlan& p) {
   release(p.twiddle);
+  release(p.deconv);
   p.n = 0;
 }
 
-constexpr int FFT_THREADS = 256;
-constexpr int W_COL = 16;  // columns per tile for y/x passes
-constexpr int W_ROW = 8;   // rows per tile for z passes
-constexpr int W_PX = 8;    // columns per tile for the fused Poisson x pass
-
-template <typename K>
-static void set_smem(K kernel, size_t bytes) {
-  if (bytes > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+static int num_sms() {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+  }
+  return sms;
 }
 
+// Persistent launch: as many CTAs as fit on all SMs at once, at most one per tile.
+template <typename K, typename... Args>
+static void launch_persistent(K kernel, int threads, size_t smem, int total, cudaStream_t s, Args... args) {
+  if (smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int per_sm = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  const int grid = std::max(1, std::min(total, per_sm * num_sms()));
+  count_launch();
+  kernel<<<grid, threads, smem, s>>>(args...);
+}
+
+constexpr size_t c_tile(int rows_of_tile) { return (size_t)rows_of_tile * TLD * sizeof(float2); }
+
 template <int N>
-static void c2c_pass(float2* data, long long comp_stride, int ncomp, TileGeo g, int outer, int inverse,
-                     const float2* tw, cudaStream_t s) {
-  const size_t smem = (size_t)W_COL * line_ld<N>() * sizeof(float2);
-  dim3 grid(outer, (g.lines + W_COL - 1) / W_COL, ncomp);
-  if (inverse) {
-    auto k = k_fft_pass<N, W_COL, FFT_THREADS, true>;
-    set_smem(k, smem);
-    count_launch();
-    k<<<grid, FFT_THREADS, smem, s>>>(data, comp_stride, g, tw);
-  } else {
-    auto k = k_fft_pass<N, W_COL, FFT_THREADS, false>;
-    set_smem(k, smem);
-    count_launch();
-    k<<<grid, FFT_THREADS, smem, s>>>(data, comp_stride, g, tw);
-  }
+static void cols_pass(float2* data, long long comp_stride, int ncomp, ColGeo g, int inverse, const float2* tw,
+                      cudaStream_t s) {
+  constexpr int T = threads_for<N>();
+  constexpr int NB = 2 * c_tile(N) <= SMEM_LIMIT ? 2 : 1;
+  const size_t smem = NB * c_tile(N);
+  g.col_tiles = (g.cols + TW - 1) / TW;
+  const int total = ncomp * g.outer * g.col_tiles;
+  if (inverse)
+    launch_persistent(k_fft_cols<N, true, NB, T>, T, smem, total, s, data, comp_stride, g, ncomp, tw);
+  else
+    launch_persistent(k_fft_cols<N, false, NB, T>, T, smem, total, s, data, comp_stride, g, ncomp, tw);
 }
 
 template <int N>
 static void fft3_c2c_n(float2* data, int inverse, const float2* tw, cudaStream_t s) {
+  constexpr int T = threads_for<N>();
+  constexpr int NB = 2 * c_tile(N) <= SMEM_LIMIT ? 2 : 1;
+  const size_t smem = NB * c_tile(N);
   const long long n = N;
-  // z lines: contiguous rows; tile = W_COL rows of one x-plane
-  c2c_pass<N>(data, 0, 1, TileGeo{n * n, n, 1, N}, N, inverse, tw, s);
-  // y lines: elements n apart, columns along z adjacent
-  c2c_pass<N>(data, 0, 1, TileGeo{n * n, 1, n, N}, N, inverse, tw, s);
-  // x lines: elements n*n apart; outer index = y
-  c2c_pass<N>(data, 0, 1, TileGeo{n, 1, n * n, N}, N, inverse, tw, s);
+  const int rows = N * N;
+  const int total = (rows + TW - 1) / TW;
+  if (inverse)
+    launch_persistent(k_fft_rows<N, true, NB, T>, T, smem, total, s, data, rows, tw);
+  else
+    launch_persistent(k_fft_rows<N, false, NB, T>, T, smem, total, s, data, rows, tw);
+  // y lines: elements n apart, columns along z adjacent, outer = x
+  cols_pass<N>(data, 0, 1, ColGeo{n * n, n, N, 0, N}, inverse, tw, s);
+  // x lines: elements n*n apart, outer = y
+  cols_pass<N>(data, 0, 1, ColGeo{n, n * n, N, 0, N}, inverse, tw, s);
 }
 
 void launch_fft3_c2c(const FftPlan& p, float2* data, int inverse, cudaStream_t s) {
@@ -424,62 +624,54 @@ void launch_fft3_c2c(const FftPlan& p, float2* data, int inverse, cudaStream_t s
 
 template <int N>
 static void poisson_n(const FftPlan& p, const PoissonParams& pp, const float* delta, const unsigned long long* fx,
-                      int fx_shift, float mean, float2* spec, float* gx, float* gy, float* gz,
-                      const float* deconv, cudaStream_t s) {
+                      int fx_shift, float mean, float2* spec, float* gx, float* gy, float* gz, cudaStream_t s) {
   const float2* tw = static_cast<const float2*>(p.twiddle.p);
-  constexpr int NH = N / 2 + 1;
+  const float* deconv = pp.deconvolve ? static_cast<const float*>(p.deconv.p) : nullptr;
+  constexpr int M = N / 2, NH = N / 2 + 1, NHP = N / 2 + 2;
   const long long n = N;
-  const long long comp = n * n * NH;  // elements per half spectrum
+  const long long comp = n * n * NHP;  // elements per half spectrum
   const int rows = N * N;
+  const int row_tiles = (rows + TW - 1) / TW;
   // Slot 0 holds the forward spectrum; the x pass reads each tile of it before writing the
   // same tile of slots 0..2, and tiles are disjoint, so the update in place is safe.
   float2* s0 = spec;
-  // 1. z: R2C into slot 0
-  {
-    const size_t smem = (size_t)W_ROW * line_ld<N>() * sizeof(float2);
-    auto k = k_r2c_z<N, W_ROW, FFT_THREADS>;
-    set_smem(k, smem);
-    count_launch();
-    k<<<(rows + W_ROW - 1) / W_ROW, FFT_THREADS, smem, s>>>(delta, fx, std::ldexp(1.0f, -fx_shift), mean, s0, rows,
-                                                            tw);
+  {  // 1. z: R2C into slot 0 (staging buffers of 16-byte slots + one complex tile)
+    constexpr int T = threads_for<M>();
+    constexpr int NB = 4 * c_tile(M) + c_tile(M) <= SMEM_LIMIT ? 2 : 1;
+    const size_t smem = (2 * NB + 1) * c_tile(M);
+    launch_persistent(k_r2c_z<N, NB, T>, T, smem, row_tiles, s, delta, fx, std::ldexp(1.0f, -fx_shift), mean, s0,
+                      rows, tw);
   }
-  // 2. y forward on slot 0: lines along y (stride NH), columns along kz adjacent, outer = x
-  c2c_pass<N>(s0, 0, 1, TileGeo{n * NH, 1, NH, NH}, N, 0, tw, s);
-  // 3. x forward + Green + gradient + x inverse -> slots 0..2; outer = y
-  {
-    const size_t smem = (size_t)2 * W_PX * line_ld<N>() * sizeof(float2);
-    auto k = k_poisson_x<N, W_PX, FFT_THREADS>;
-    set_smem(k, smem);
-    dim3 grid(N, (NH + W_PX - 1) / W_PX, 1);
-    count_launch();
-    k<<<grid, FFT_THREADS, smem, s>>>(s0, spec, comp, TileGeo{NH, 1, n * NH, NH}, pp, deconv, tw);
+  // 2. y forward on slot 0: lines along y (stride NHP), columns along kz adjacent, outer = x
+  cols_pass<N>(s0, 0, 1, ColGeo{n * NHP, NHP, NH, 0, N}, 0, tw, s);
+  {  // 3. x forward + Green + gradient + x inverse -> slots 0..2; outer = y
+    constexpr int T = threads_for<N>();
+    constexpr int NBX = 3 * c_tile(N) <= SMEM_LIMIT ? 2 : 1;
+    const size_t smem = (NBX + 1) * c_tile(N);
+    ColGeo g{NHP, n * NHP, NH, (NH + TW - 1) / TW, N};
+    launch_persistent(k_poisson_x<N, NBX, T>, T, smem, g.outer * g.col_tiles, s, s0, spec, comp, g, pp, deconv, tw);
   }
   // 4. y inverse on the three component spectra
-  c2c_pass<N>(spec, comp, 3, TileGeo{n * NH, 1, NH, NH}, N, 1, tw, s);
-  // 5. z: C2R with 1/n^3
-  {
-    const size_t smem = (size_t)W_ROW * line_ld<N>() * sizeof(float2);
-    auto k = k_c2r_z<N, W_ROW, FFT_THREADS>;
-    set_smem(k, smem);
-    dim3 grid((rows + W_ROW - 1) / W_ROW, 1, 3);
-    count_launch();
-    k<<<grid, FFT_THREADS, smem, s>>>(spec, comp, gx, gy, gz, pp.scale, rows, tw);
+  cols_pass<N>(spec, comp, 3, ColGeo{n * NHP, NHP, NH, 0, N}, 1, tw, s);
+  {  // 5. z: C2R with 1/n^3
+    constexpr int T = threads_for<M>();
+    constexpr int NB = 2 * c_tile(M + 1) <= SMEM_LIMIT ? 2 : 1;
+    const size_t smem = NB * c_tile(M + 1);
+    launch_persistent(k_c2r_z<N, NB, T>, T, smem, 3 * row_tiles, s, spec, comp, gx, gy, gz, pp.scale, rows, tw);
   }
 }
 
 void launch_poisson(const FftPlan& p, const PoissonParams& pp, const float* delta, const unsigned long long* fx,
                     int fx_shift, float mean, float2* spec, float* gx, float* gy, float* gz, cudaStream_t s) {
-  const float* deconv = nullptr;
   switch (p.n) {
-    case 4: poisson_n<4>(p, pp, delta, fx, fx_shift, mean, spec, gx, gy, gz, deconv, s); break;
-    case 8: poisson_n<8>(p, pp, delta, fx, fx_shift, mean, spec, gx, gy, gz, deconv, s); break;
-    case 16: poisson_n<16>(p, pp, delta, fx, fx_shift, mean, spec, gx, gy, gz, deconv, s); break;
-    case 32: poisson_n<32>(p, pp, delta, fx, fx_shift, mean, spec, gx, gy, gz, deconv, s); break;
-    case 64: poisson_n<64>(p, pp, delta, fx, fx_shift, mean, spec, gx, gy, gz, deconv, s); break;
-    case 128: poisson_n<128>(p, pp, delta, fx, fx_shift, mean, spec, gx, gy, gz, deconv, s); break;
-    case 256: poisson_n<256>(p, pp, delta, fx, fx_shift, mean, spec, gx, gy, gz, deconv, s); break;
-    case 512: poisson_n<512>(p, pp, delta, fx, fx_shift, mean, spec, gx, gy, gz, deconv, s); break;
-    case 1024: poisson_n<1024>(p, pp, delta, fx, fx_shift, mean, spec, gx, gy, gz, deconv, s); break;
+    case 4: poisson_n<4>(p, pp, delta, fx, fx_shift, mean, spec, gx, gy, gz, s); break;
+    case 8: poisson_n<8>(p, pp, delta, fx, fx_shift, mean, spec, gx, gy, gz, s); break;
+    case 16: poisson_n<16>(p, pp, delta, fx, fx_shift, mean, spec, gx, gy, gz, s); break;
+    case 32: poisson_n<32>(p, pp, delta, fx, fx_shift, mean, spec, gx, gy, gz, s); break;
+    case 64: poisson_n<64>(p, pp, delta, fx, fx_shift, mean, spec, gx, gy, gz, s); break;
+    case 128: poisson_n<128>(p, pp, delta, fx, fx_shift, mean, spec, gx, gy, gz, s); break;
+    case 256: poisson_n<256>(p, pp, delta, fx, fx_shift, mean, spec, gx, gy, gz, s); break;
+    case 512: poisson_n<512>(p, pp, delta, fx, fx_shift, mean, spec, gx, gy, gz, s); break;
     default: break;
   }
 }

@@ -141,9 +141,9 @@ static int sim_new(const cpm_sim_params* params, float a0, cpm_sim** out) {
   if (P.n_particles == 0 || P.n_particles > 0x7FFFFFFFull)
     return set_error(nullptr, CPM_E_INVALID, "cpm_sim_create: n_particles must be in [1, 2^31)");
   if (!(P.box_size > 0.0f) || !(a0 > 0.0f)) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_create: box and a0 must be > 0");
-  if (!fft_supported(P.mesh_n))
+  if (!poisson_supported(P.mesh_n))
     return set_error(nullptr, CPM_E_UNSUPPORTED,
-                     "cpm_sim_create: mesh_n = " + std::to_string(P.mesh_n) + " is not a power of two in [4, 1024]");
+                     "cpm_sim_create: mesh_n = " + std::to_string(P.mesh_n) + " is not a power of two in [4, 512]");
   int rc = check_device_once(nullptr);
   if (rc) return rc;
   cpm_sim* s = new cpm_sim();
@@ -166,7 +166,7 @@ static int sim_new(const cpm_sim_params* params, float a0, cpm_sim** out) {
       for (auto& e : row)
         if (cudaEventCreate(&e) != cudaSuccess) return fail(CPM_E_CUDA);
   const size_t n = s->n;
-  const size_t half = (size_t)P.mesh_n * P.mesh_n * (P.mesh_n / 2 + 1);
+  const size_t half = half_spectrum_elems(P.mesh_n);
   bool ok = true;
   for (DevBuf* b : {&s->x, &s->p, &s->acc, &s->x2, &s->p2}) ok = ok && ensure(*b, 3 * n * sizeof(float)) == cudaSuccess;
   for (DevBuf* b : {&s->id, &s->id2, &s->vals}) ok = ok && ensure(*b, n * sizeof(uint32_t)) == cudaSuccess;
