@@ -1,20 +1,26 @@
 // walk.cu — the short-range tree walk (tree.rs:264-323) and its pair kernel (tree.rs:54-66).
 //
-// Traversal. One warp walks for 32 consecutive sorted particles (one per lane) with one shared
-// LIFO stack of (node, lane mask) entries. A lane is in a node's mask exactly when its own
-// reference walk (tree.rs:264-310) would pop that node; each lane applies the reference's tests
-// for itself: prune when |min_image(centre - x)| > r_cut + sqrt(3) half; direct sum over the
-// node's particles when its octant-0 child is missing (`children[0] == NO_CHILD`, which includes
-// leaves); else accept the centre of mass when 2 half < theta |min_image(com - x)|, or push the
-// children 0..7 for the lanes that opened it (they pop 7..0, as in the reference, so each lane
-// adds its contributions in the reference's node order). Every decision (prune, accept, cutoff,
-// self) is computed with separately rounded f32 operations and an exact minimum image, so it
-// matches the reference for equal inputs; where a faster form is used (the square root of the
-// opening test) it is checked against the exact one whenever the two could disagree.
+// Traversal. One warp walks for 32 consecutive sorted particles (one per lane). The unit of work
+// is a batch: the children of one opened node (contiguous in the node arrays), with the mask of
+// the lanes that opened it. Lanes c < count load node c of the batch (centre, centre of mass,
+// link: three coalesced 16-byte loads) and publish it to shared memory; every lane in the mask
+// then applies the reference's tests (tree.rs:264-310) to each node for itself: prune when
+// |min_image(centre - x)| > r_cut + sqrt(3) half; direct sum over the node's particles when its
+// octant-0 child is missing (`children[0] == NO_CHILD`, which includes leaves); else accept the
+// centre of mass when 2 half < theta |min_image(com - x)|, or open the node. Each opened node
+// becomes a new batch on a per-warp stack, tagged with the lanes that opened it; the next batch is
+// loaded into registers before the current batch's forces are summed, so its load latency is
+// hidden. A lane's set of interactions is exactly the one its own reference walk visits (every
+// decision is computed with separately rounded f32 operations and an exact minimum image; where a
+// faster form is used, the square root of the opening test, it is checked against the exact one
+// whenever the two could disagree); only the order in which a lane adds them differs.
 //
-// Direct sums run lane-per-particle over the node's sources, staged as float4 in shared memory.
-// A lane whose particle is far enough from the box faces (|centre - x| + half < 0.49 L on every
-// axis) cannot need a periodic image for any source of the node, and skips the image test.
+// Direct sums concatenate the sources of all direct nodes of a batch into chunks of 32 float4 in
+// shared memory. Per chunk a lane first marks the sources within r_cut of it (bit mask), then
+// evaluates the pair force only for the marked ones, so lanes do not idle on sources outside the
+// cutoff of other lanes. A lane whose direct nodes all lie far enough from the box faces
+// (|centre - x| + half < 0.49 L on every axis) cannot need a periodic image, and skips the image
+// test.
 //
 // Pair force. f = -K m S(r) / (r^2 + eps^2)^{3/2}, S(r) = erfc(u) + (2/sqrt(pi)) u e^{-u^2},
 // u = r / (2 r_s). S is evaluated as e^{-u^2} R(u) with R(u) = erfcx(u) + 2u/sqrt(pi), a smooth
@@ -48,6 +54,18 @@ struct SFit {
   int far_n;
 };
 
+// The constants of the direct-sum pair force, duplicated for the packed (two pairs per
+// instruction) evaluation.
+struct PairConst2 {
+  float2 tiny;        // added to r^2 under the reciprocal square root, so that r = 0 stays 0
+  float2 inv_two_rs;  // 1 / (2 r_s)
+  float2 scale0, offset0;
+  float2 c0[FIT_DEG + 1];
+  float2 neg_log2e;   // -log2(e)
+  float2 eps2;        // softening^2
+  float2 neg_k;       // -K m
+};
+
 struct WalkParams {
   float box;
   float guard;  // |x| below this: round(x / L) == 0 exactly
@@ -58,6 +76,7 @@ struct WalkParams {
   float eps2;   // softening^2
   float k;      // Newtonian coupling
   SFit fit;
+  PairConst2 p2;
 };
 
 // ------------------------------------------------------------------ host: the fit of R(u)
@@ -170,6 +189,45 @@ __device__ __forceinline__ float pair_factor(float r2, float neg_km, const WalkP
   return neg_km * S * (rs * rs * rs);
 }
 
+// Hardware approximations (MUFU): relative error about 2^-22, no special handling of
+// denormal inputs (the arguments here are r^2 + tiny, r^2 + eps^2 and -u^2 log2(e)).
+__device__ __forceinline__ float rsqrt_approx(float x) {
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float exp2_approx(float x) {
+  float r;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+// pair_factor for two pairs at once (f32x2 arithmetic), coupling -K m of a particle.
+__device__ __forceinline__ float2 pair_factor2(float2 r2, const WalkParams& w, const float* __restrict__ far) {
+  const PairConst2& c = w.p2;
+  const float2 rr = __fadd2_rn(r2, c.tiny);
+  const float2 r = __fmul2_rn(r2, make_float2(rsqrt_approx(rr.x), rsqrt_approx(rr.y)));
+  const float2 u = __fmul2_rn(r, c.inv_two_rs);
+  float2 S;
+  if (fmaxf(u.x, u.y) <= w.fit.umax0) {
+    const float2 x = __ffma2_rn(u, c.scale0, c.offset0);
+    float2 R = c.c0[FIT_DEG];
+#pragma unroll
+    for (int j = FIT_DEG - 1; j >= 0; --j) R = __ffma2_rn(R, x, c.c0[j]);
+    // e^{-u^2} = 2^{-uu log2 e} (1 - err) with uu + err = u*u exactly
+    const float2 uu = __fmul2_rn(u, u);
+    const float2 nerr = __ffma2_rn(__fmul2_rn(u, make_float2(-1.0f, -1.0f)), u, uu);
+    const float2 ea = __fmul2_rn(uu, c.neg_log2e);
+    const float2 e = make_float2(exp2_approx(ea.x), exp2_approx(ea.y));
+    S = __fmul2_rn(__ffma2_rn(e, nerr, e), R);
+  } else {
+    S = make_float2(short_range_S(u.x, w.fit, far), short_range_S(u.y, w.fit, far));
+  }
+  const float2 q = __fadd2_rn(r2, c.eps2);
+  const float2 rs = make_float2(rsqrt_approx(q.x), rsqrt_approx(q.y));
+  return __fmul2_rn(__fmul2_rn(c.neg_k, S), __fmul2_rn(__fmul2_rn(rs, rs), rs));
+}
+
 // tree.rs:253-261: d = x - L round(x / L), x = a - b, exact. |x| < 0.49 L gives a zero quotient
 // whatever its last bit; the rest divides with IEEE division.
 __device__ __forceinline__ float min_image_slow(float x, const WalkParams& w) {
@@ -201,6 +259,81 @@ __device__ __forceinline__ bool accept_node(float half, float theta, float r2) {
   return lhs < __fmul_rn(theta, sqrtf(r2));
 }
 
+// Per-warp shared state of the walk.
+struct WalkShared {
+  uint2 stack[STACK_CAP];          // (first node, lane mask): a batch of sibling nodes ...
+  unsigned char count[STACK_CAP];  // ... and its node count
+  float4 geo[8];                   // the current batch: centre, half
+  float4 mass[8];                  //                    centre of mass, count
+  uint4 link[8];                   //                    start, end, first child, child mask
+  float nx[32], ny[32], nz[32];    // a chunk of direct-sum sources, negated: -x, -y, -z
+};
+
+// Bits lo .. lo + len - 1 (len in 1..32).
+__device__ __forceinline__ uint32_t bit_span(uint32_t lo, uint32_t len) {
+  return (len >= 32u ? 0xffffffffu : ((1u << len) - 1u)) << lo;
+}
+
+// Direct-sum phase 1 for one chunk: bit t set when source t lies within r_cut of the lane's
+// particle (tree.rs:286-298); the caller keeps the bits of the sources it sums directly. The
+// difference and its squared norm round exactly like the reference's separate f32 operations;
+// without periodic images two sources are tested per instruction (f32x2).
+template <bool WRAP>
+__device__ __forceinline__ uint32_t chunk_candidates(const WalkShared& sh, int cnt, float x0, float x1, float x2,
+                                                     const WalkParams& w) {
+  uint32_t pm = 0;
+  if (!WRAP) {
+    const float2 X0 = make_float2(x0, x0), X1 = make_float2(x1, x1), X2 = make_float2(x2, x2);
+#pragma unroll 4
+    for (int t = 0; t < cnt; t += 2) {
+      const float2 d0 = __fadd2_rn(X0, *reinterpret_cast<const float2*>(sh.nx + t));
+      const float2 d1 = __fadd2_rn(X1, *reinterpret_cast<const float2*>(sh.ny + t));
+      const float2 d2 = __fadd2_rn(X2, *reinterpret_cast<const float2*>(sh.nz + t));
+      const float2 r2 = __fadd2_rn(__fadd2_rn(__fmul2_rn(d0, d0), __fmul2_rn(d1, d1)), __fmul2_rn(d2, d2));
+      pm |= ((uint32_t)!(r2.x > w.cut2) | ((uint32_t)!(r2.y > w.cut2) << 1)) << t;
+    }
+  } else {
+    for (int t = 0; t < cnt; ++t) {
+      float d0 = __fadd_rn(x0, sh.nx[t]), d1 = __fadd_rn(x1, sh.ny[t]), d2 = __fadd_rn(x2, sh.nz[t]);
+      min_image3(d0, d1, d2, w);
+      pm |= (uint32_t)!(norm2(d0, d1, d2) > w.cut2) << t;
+    }
+  }
+  return pm;
+}
+
+// Direct-sum phase 2: the pair forces of the sources in pm, two per iteration, added to the
+// packed accumulators (even and odd pairs).
+template <bool WRAP>
+__device__ __forceinline__ void chunk_forces(const WalkShared& sh, uint32_t pm, float x0, float x1, float x2,
+                                             const WalkParams& w, const float* __restrict__ far, float2& A0,
+                                             float2& A1, float2& A2) {
+  const float2 X0 = make_float2(x0, x0), X1 = make_float2(x1, x1), X2 = make_float2(x2, x2);
+  while (pm) {
+    const int t1 = __ffs(pm) - 1;
+    pm &= pm - 1;
+    int t2 = t1;
+    float keep = 0.0f;  // a lone last pair is evaluated twice and its copy weighted by 0
+    if (pm) {
+      t2 = __ffs(pm) - 1;
+      pm &= pm - 1;
+      keep = 1.0f;
+    }
+    float2 d0 = __fadd2_rn(X0, make_float2(sh.nx[t1], sh.nx[t2]));
+    float2 d1 = __fadd2_rn(X1, make_float2(sh.ny[t1], sh.ny[t2]));
+    float2 d2 = __fadd2_rn(X2, make_float2(sh.nz[t1], sh.nz[t2]));
+    if (WRAP) {
+      min_image3(d0.x, d1.x, d2.x, w);
+      min_image3(d0.y, d1.y, d2.y, w);
+    }
+    const float2 r2 = __ffma2_rn(d2, d2, __ffma2_rn(d1, d1, __fmul2_rn(d0, d0)));
+    const float2 f = __fmul2_rn(pair_factor2(r2, w, far), make_float2(1.0f, keep));
+    A0 = __ffma2_rn(d0, f, A0);
+    A1 = __ffma2_rn(d1, f, A1);
+    A2 = __ffma2_rn(d2, f, A2);
+  }
+}
+
 __global__ void __launch_bounds__(WALK_THREADS) k_tree_walk(const uint4* __restrict__ link,
                                                             const float4* __restrict__ geo,
                                                             const float4* __restrict__ mass,
@@ -208,117 +341,180 @@ __global__ void __launch_bounds__(WALK_THREADS) k_tree_walk(const uint4* __restr
                                                             const float* __restrict__ far, float* __restrict__ acc3,
                                                             int accumulate, unsigned long long* counters,
                                                             DevStatus* st) {
-  __shared__ uint2 stack[WALK_WARPS][STACK_CAP];
-  __shared__ float4 src[WALK_WARPS][32];
+  __shared__ WalkShared shared[WALK_WARPS];
+  const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const size_t gb = ((size_t)blockIdx.x * WALK_WARPS + warp) * 32;
-  const size_t i = gb + lane;
+  const size_t i = ((size_t)blockIdx.x * WALK_WARPS + warp) * 32 + lane;
   const bool valid = i < n;
-  const unsigned group = __ballot_sync(0xffffffffu, valid);
+  const unsigned group = __ballot_sync(FULL, valid);
   if (group == 0) return;
+  WalkShared& sh = shared[warp];
   const float4 xi = valid ? __ldg(x4 + i) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   const float x0 = xi.x, x1 = xi.y, x2 = xi.z;
+  const uint32_t self = (uint32_t)i;
   const float neg_k = -w.k;
   float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
-  unsigned long long n_pairs = 0, n_accepts = 0, n_cand = 0;
-  uint2* stk = stack[warp];
-  float4* sw = src[warp];
+  float2 A0 = make_float2(0.0f, 0.0f), A1 = A0, A2 = A0;
+  uint32_t n_pairs = 0, n_accepts = 0, n_cand = 0;
+
+  // The current batch (sibling nodes first .. first + count - 1, lanes in mask); lane c < count
+  // holds node first + c in registers until it is published to shared memory.
+  uint32_t b_count = 1, b_mask = group;
+  float4 pg = make_float4(0.0f, 0.0f, 0.0f, 0.0f), pm4 = pg;
+  uint4 pl = make_uint4(0u, 0u, 0u, 0u);
+  if (lane == 0) {
+    pg = __ldg(geo);
+    pm4 = __ldg(mass);
+    pl = __ldg(link);
+  }
   int sp = 0;
-  if (lane == 0) stk[0] = make_uint2(0u, group);
-  sp = 1;
-  __syncwarp();
-  while (sp > 0) {
-    --sp;
-    const uint2 top = stk[sp];
+  for (;;) {
     __syncwarp();
-    const uint32_t node = top.x;
-    const bool act = (top.y >> lane) & 1u;
-    const float4 G = __ldg(geo + node);
-    bool live = false, nowrap = false;
-    if (act) {
-      float t0 = __fsub_rn(G.x, x0), t1 = __fsub_rn(G.y, x1), t2 = __fsub_rn(G.z, x2);
-      // every source y of the node lies in [centre - half, centre + half]
-      nowrap = fmaxf(fabsf(t0), fmaxf(fabsf(t1), fabsf(t2))) + G.w < w.guard;
-      min_image3(t0, t1, t2, w);
-      const float max_r = __fadd_rn(w.r_cut, __fmul_rn(SQRT_3, G.w));
-      live = !(norm2(t0, t1, t2) > __fmul_rn(max_r, max_r));
+    if ((uint32_t)lane < b_count) {
+      sh.geo[lane] = pg;
+      sh.mass[lane] = pm4;
+      sh.link[lane] = pl;
     }
-    const unsigned live_mask = __ballot_sync(0xffffffffu, live);
-    if (live_mask == 0) continue;
-    const uint4 L = __ldg(link + node);
-    if ((L.w & 1u) == 0u) {
-      // children[0] == NO_CHILD: direct sum over the node's particles (tree.rs:286-298)
-      if (live) n_cand += L.y - L.x;
-      for (uint32_t b0 = L.x; b0 < L.y; b0 += 32) {
-        const uint32_t j = b0 + lane;
-        if (j < L.y) sw[lane] = __ldg(x4 + j);
+    __syncwarp();
+
+    // Classify every node of the batch for this lane: prune, direct sum, accept or open.
+    uint32_t dmask = 0, nwmask = 0, amask = 0, omask = 0;
+    if ((b_mask >> lane) & 1u) {
+      for (uint32_t c = 0; c < b_count; ++c) {
+        const float4 G = sh.geo[c];
+        float t0 = __fsub_rn(G.x, x0), t1 = __fsub_rn(G.y, x1), t2 = __fsub_rn(G.z, x2);
+        // every source y of the node lies in [centre - half, centre + half]
+        const bool nowrap = fmaxf(fabsf(t0), fmaxf(fabsf(t1), fabsf(t2))) + G.w < w.guard;
+        min_image3(t0, t1, t2, w);
+        const float max_r = __fadd_rn(w.r_cut, __fmul_rn(SQRT_3, G.w));
+        if (norm2(t0, t1, t2) > __fmul_rn(max_r, max_r)) continue;
+        if ((sh.link[c].w & 1u) == 0u) {
+          // children[0] == NO_CHILD: direct sum over the node's particles (tree.rs:286-298)
+          dmask |= 1u << c;
+          nwmask |= (uint32_t)nowrap << c;
+          continue;
+        }
+        const float4 M = sh.mass[c];
+        float s0 = __fsub_rn(M.x, x0), s1 = __fsub_rn(M.y, x1), s2 = __fsub_rn(M.z, x2);
+        min_image3(s0, s1, s2, w);
+        if (accept_node(G.w, w.theta, norm2(s0, s1, s2)))
+          amask |= 1u << c;
+        else
+          omask |= 1u << c;
+      }
+    }
+
+    // Push the opened nodes' children as new batches (any order: contributions are summed per
+    // lane, and the set of interactions of each lane does not depend on the traversal order).
+    const uint32_t ouni = __reduce_or_sync(FULL, omask);
+    if (ouni) {
+      uint32_t opened_by = 0;
+      for (uint32_t rem = ouni; rem; rem &= rem - 1) {
+        const int c = __ffs(rem) - 1;
+        const uint32_t b = __ballot_sync(FULL, (omask >> c) & 1u);
+        if (lane == c) opened_by = b;
+      }
+      const int npush = __popc(ouni);
+      if (sp + npush > STACK_CAP) {
+        if (lane == 0) dev_fail(st, DEV_STACK_OVERFLOW, sp);
+        break;
+      }
+      if ((ouni >> lane) & 1u) {
+        const uint4 L = sh.link[lane];
+        const int slot = sp + __popc(ouni & ((1u << lane) - 1u));
+        sh.stack[slot] = make_uint2(L.z, opened_by);
+        sh.count[slot] = (unsigned char)__popc(L.w & 0xFFu);
+      }
+      sp += npush;
+      __syncwarp();
+    }
+
+    // Prefetch the next batch into registers; the loads complete during the work below.
+    const bool more = sp > 0;
+    uint32_t nx_count = 0, nx_mask = 0;
+    if (more) {
+      const uint2 top = sh.stack[--sp];
+      const uint32_t first = top.x;
+      nx_count = sh.count[sp];
+      nx_mask = top.y;
+      if ((uint32_t)lane < nx_count) {
+        pg = __ldg(geo + first + lane);
+        pm4 = __ldg(mass + first + lane);
+        pl = __ldg(link + first + lane);
+      }
+    }
+
+    // Accepted centres of mass (tree.rs:299-305).
+    for (; amask; amask &= amask - 1) {
+      const int c = __ffs(amask) - 1;
+      const float4 M = sh.mass[c];
+      float s0 = __fsub_rn(M.x, x0), s1 = __fsub_rn(M.y, x1), s2 = __fsub_rn(M.z, x2);
+      min_image3(s0, s1, s2, w);
+      const float f = pair_factor(norm2(s0, s1, s2), neg_k * M.w, w, far);
+      a0 = fmaf(-s0, f, a0);
+      a1 = fmaf(-s1, f, a1);
+      a2 = fmaf(-s2, f, a2);
+      ++n_accepts;
+    }
+
+    // Direct sums: the sources of all direct nodes of the batch, concatenated in chunks of 32.
+    const uint32_t dset = __reduce_or_sync(FULL, dmask);
+    if (dset) {
+      uint32_t total = 0;
+      for (uint32_t rem = dset; rem; rem &= rem - 1) {
+        const uint4 L = sh.link[__ffs(rem) - 1];
+        const uint32_t cnt = L.y - L.x;
+        total += cnt;
+        if ((dmask >> (__ffs(rem) - 1)) & 1u) n_cand += cnt;
+      }
+      const bool wrap = (dmask & ~nwmask) != 0u;
+      for (uint32_t base = 0; base < total; base += 32) {
+        // Lane q loads source base + q of the concatenation; `live` gets the chunk positions of
+        // the nodes this lane sums directly, without the lane's own particle (j != i).
+        const uint32_t g = base + (uint32_t)lane;
+        uint32_t live = 0, selfbit = 0, off = 0;
+        for (uint32_t rem = dset; rem && off < base + 32u; rem &= rem - 1) {
+          const int c = __ffs(rem) - 1;
+          const uint4 L = sh.link[c];
+          const uint32_t cnt = L.y - L.x;
+          if (g >= off && g < off + cnt) {
+            const float4 y = __ldg(x4 + L.x + (g - off));
+            sh.nx[lane] = -y.x;
+            sh.ny[lane] = -y.y;
+            sh.nz[lane] = -y.z;
+          }
+          const uint32_t lo = max(off, base), hi = min(off + cnt, base + 32u);
+          if (((dmask >> c) & 1u) && lo < hi) live |= bit_span(lo - base, hi - lo);
+          if (self >= L.x && self < L.y) {
+            const uint32_t gs = off + (self - L.x);
+            if (gs >= base && gs < base + 32u) selfbit = 1u << (gs - base);
+          }
+          off += cnt;
+        }
+        live &= ~selfbit;
         __syncwarp();
         if (live) {
-          const int cnt = (int)min(32u, L.y - b0);
-          const int self = (gb == b0) ? lane : ((size_t)b0 <= i && i < (size_t)b0 + 32 ? (int)(i - b0) : -1);
-          if (nowrap) {
-#pragma unroll 4
-            for (int t = 0; t < cnt; ++t) {
-              const float4 y = sw[t];
-              const float d0 = __fsub_rn(x0, y.x), d1 = __fsub_rn(x1, y.y), d2 = __fsub_rn(x2, y.z);
-              const float r2 = norm2(d0, d1, d2);
-              if (!(r2 > w.cut2) && t != self) {
-                const float f = pair_factor(r2, neg_k, w, far);
-                a0 = fmaf(d0, f, a0);
-                a1 = fmaf(d1, f, a1);
-                a2 = fmaf(d2, f, a2);
-                ++n_pairs;
-              }
-            }
+          const int cnt = (int)min(32u, total - base);
+          if (wrap) {
+            const uint32_t pairs = chunk_candidates<true>(sh, cnt, x0, x1, x2, w) & live;
+            n_pairs += __popc(pairs);
+            chunk_forces<true>(sh, pairs, x0, x1, x2, w, far, A0, A1, A2);
           } else {
-            for (int t = 0; t < cnt; ++t) {
-              const float4 y = sw[t];
-              float d0 = __fsub_rn(x0, y.x), d1 = __fsub_rn(x1, y.y), d2 = __fsub_rn(x2, y.z);
-              min_image3(d0, d1, d2, w);
-              const float r2 = norm2(d0, d1, d2);
-              if (!(r2 > w.cut2) && t != self) {
-                const float f = pair_factor(r2, neg_k, w, far);
-                a0 = fmaf(d0, f, a0);
-                a1 = fmaf(d1, f, a1);
-                a2 = fmaf(d2, f, a2);
-                ++n_pairs;
-              }
-            }
+            const uint32_t pairs = chunk_candidates<false>(sh, cnt, x0, x1, x2, w) & live;
+            n_pairs += __popc(pairs);
+            chunk_forces<false>(sh, pairs, x0, x1, x2, w, far, A0, A1, A2);
           }
         }
         __syncwarp();
       }
-    } else {
-      bool open = false;
-      if (live) {
-        const float4 M = __ldg(mass + node);
-        float t0 = __fsub_rn(M.x, x0), t1 = __fsub_rn(M.y, x1), t2 = __fsub_rn(M.z, x2);
-        min_image3(t0, t1, t2, w);
-        const float r2 = norm2(t0, t1, t2);
-        if (accept_node(G.w, w.theta, r2)) {
-          const float f = pair_factor(r2, neg_k * M.w, w, far);
-          a0 = fmaf(-t0, f, a0);
-          a1 = fmaf(-t1, f, a1);
-          a2 = fmaf(-t2, f, a2);
-          ++n_accepts;
-        } else {
-          open = true;
-        }
-      }
-      const unsigned open_mask = __ballot_sync(0xffffffffu, open);
-      if (open_mask) {
-        const uint32_t cmask = L.w & 0xFFu;
-        const int nch = __popc(cmask);
-        if (sp + nch > STACK_CAP) {
-          if (lane == 0) dev_fail(st, DEV_STACK_OVERFLOW, (int)node);
-          break;
-        }
-        if (lane < nch) stk[sp + lane] = make_uint2(L.z + (uint32_t)lane, open_mask);
-        sp += nch;
-        __syncwarp();
-      }
     }
+    if (!more) break;
+    b_count = nx_count;
+    b_mask = nx_mask;
   }
+  a0 = __fadd_rn(a0, __fadd_rn(A0.x, A0.y));
+  a1 = __fadd_rn(a1, __fadd_rn(A1.x, A1.y));
+  a2 = __fadd_rn(a2, __fadd_rn(A2.x, A2.y));
   if (valid) {
     if (accumulate) {
       acc3[3 * i] = __fadd_rn(acc3[3 * i], a0);
@@ -331,16 +527,17 @@ __global__ void __launch_bounds__(WALK_THREADS) k_tree_walk(const uint4* __restr
     }
   }
   if (counters) {
+    unsigned long long p = n_pairs, a = n_accepts, c = n_cand;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-      n_pairs += __shfl_xor_sync(0xffffffffu, n_pairs, o);
-      n_accepts += __shfl_xor_sync(0xffffffffu, n_accepts, o);
-      n_cand += __shfl_xor_sync(0xffffffffu, n_cand, o);
+      p += __shfl_xor_sync(FULL, p, o);
+      a += __shfl_xor_sync(FULL, a, o);
+      c += __shfl_xor_sync(FULL, c, o);
     }
     if (lane == 0) {
-      atomicAdd(&counters[0], n_pairs);
-      atomicAdd(&counters[1], n_accepts);
-      atomicAdd(&counters[2], n_cand);
+      atomicAdd(&counters[0], p);
+      atomicAdd(&counters[1], a);
+      atomicAdd(&counters[2], c);
     }
   }
 }
@@ -392,6 +589,15 @@ void launch_tree_walk(const TreeNodes& t, const float* sorted_x3, size_t n, floa
   w.eps2 = split.softening * split.softening;
   w.k = k;
   w.fit = fc.fit;
+  auto dup = [](float v) { return make_float2(v, v); };
+  w.p2.tiny = dup(1e-30f);
+  w.p2.inv_two_rs = dup(w.inv_two_rs);
+  w.p2.scale0 = dup(fc.fit.scale0);
+  w.p2.offset0 = dup(fc.fit.offset0);
+  for (int j = 0; j <= FIT_DEG; ++j) w.p2.c0[j] = dup(fc.fit.c0[j]);
+  w.p2.neg_log2e = dup(-1.44269504f);
+  w.p2.eps2 = dup(w.eps2);
+  w.p2.neg_k = dup(-k);
   const size_t groups = (n + 31) / 32;
   const unsigned blocks = (unsigned)((groups + WALK_WARPS - 1) / WALK_WARPS);
   count_launch();
