@@ -263,12 +263,18 @@ __device__ __forceinline__ bool accept_node(float half, float theta, float r2) {
 struct WalkShared {
   uint2 stack[STACK_CAP];          // (first node, lane mask): a batch of sibling nodes ...
   unsigned char count[STACK_CAP];  // ... and its node count
-  float4 geo[8];                   // the current batch: centre, half
-  float4 mass[8];                  //                    centre of mass, count
-  uint4 link[8];                   //                    start, end, first child, child mask
+  float4 geo[2][8];                // the current and the next batch: centre, half
+  float4 mass[2][8];               //                                 centre of mass, count
+  uint4 link[2][8];                //                                 start, end, first child, child mask
   float nx[32], ny[32], nz[32];    // a chunk of direct-sum sources, negated: -x, -y, -z
+  float4 box_c, box_h;             // the warp's bounding box: centre, half extent (+ tolerance)
 };
 
+// 16-byte asynchronous copy global -> shared (completion awaited with cp.async.wait_all).
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(a), "l"(gmem) : "memory");
+}
 // Bits lo .. lo + len - 1 (len in 1..32).
 __device__ __forceinline__ uint32_t bit_span(uint32_t lo, uint32_t len) {
   return (len >= 32u ? 0xffffffffu : ((1u << len) - 1u)) << lo;
@@ -353,48 +359,84 @@ __global__ void __launch_bounds__(WALK_THREADS) k_tree_walk(const uint4* __restr
   const float x0 = xi.x, x1 = xi.y, x2 = xi.z;
   const uint32_t self = (uint32_t)i;
   const float neg_k = -w.k;
-  float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
+
+  // Bounding box of the warp's particles (centre cg, half extent hg), for a conservative
+  // warp-level prune test: a node farther than r_cut + sqrt(3) half from the whole box is pruned
+  // by every lane, whose own test is then skipped.
+  float lo0 = valid ? x0 : INFINITY, lo1 = valid ? x1 : INFINITY, lo2 = valid ? x2 : INFINITY;
+  float hi0 = valid ? x0 : -INFINITY, hi1 = valid ? x1 : -INFINITY, hi2 = valid ? x2 : -INFINITY;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lo0 = fminf(lo0, __shfl_xor_sync(FULL, lo0, o));
+    lo1 = fminf(lo1, __shfl_xor_sync(FULL, lo1, o));
+    lo2 = fminf(lo2, __shfl_xor_sync(FULL, lo2, o));
+    hi0 = fmaxf(hi0, __shfl_xor_sync(FULL, hi0, o));
+    hi1 = fmaxf(hi1, __shfl_xor_sync(FULL, hi1, o));
+    hi2 = fmaxf(hi2, __shfl_xor_sync(FULL, hi2, o));
+  }
+  if (lane == 0) {
+    const float tol = 1e-5f * w.box;  // far above the rounding of positions and differences
+    sh.box_c = make_float4(0.5f * (lo0 + hi0), 0.5f * (lo1 + hi1), 0.5f * (lo2 + hi2), 0.0f);
+    sh.box_h = make_float4(0.5f * (hi0 - lo0) + tol, 0.5f * (hi1 - lo1) + tol, 0.5f * (hi2 - lo2) + tol, 0.0f);
+  }
+  // Accumulators of the even and odd pairs (x: even pairs and accepted nodes).
   float2 A0 = make_float2(0.0f, 0.0f), A1 = A0, A2 = A0;
   uint32_t n_pairs = 0, n_accepts = 0, n_cand = 0;
 
-  // The current batch (sibling nodes first .. first + count - 1, lanes in mask); lane c < count
-  // holds node first + c in registers until it is published to shared memory.
+  // The current batch: sibling nodes first .. first + count - 1, walked by the lanes in mask.
+  // Lane c < count copies node first + c into shared buffer `cur` asynchronously; the next batch
+  // is copied into the other buffer while the current one is summed.
   uint32_t b_count = 1, b_mask = group;
-  float4 pg = make_float4(0.0f, 0.0f, 0.0f, 0.0f), pm4 = pg;
-  uint4 pl = make_uint4(0u, 0u, 0u, 0u);
+  int cur = 0;
   if (lane == 0) {
-    pg = __ldg(geo);
-    pm4 = __ldg(mass);
-    pl = __ldg(link);
+    cp_async16(&sh.geo[0][0], geo);
+    cp_async16(&sh.mass[0][0], mass);
+    cp_async16(&sh.link[0][0], link);
   }
   int sp = 0;
   for (;;) {
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncwarp();
-    if ((uint32_t)lane < b_count) {
-      sh.geo[lane] = pg;
-      sh.mass[lane] = pm4;
-      sh.link[lane] = pl;
-    }
-    __syncwarp();
+    const float4* bgeo = sh.geo[cur];
+    const float4* bmass = sh.mass[cur];
+    const uint4* blink = sh.link[cur];
 
-    // Classify every node of the batch for this lane: prune, direct sum, accept or open.
+    // Warp-level prune test, lane c for node c. It applies where no lane can need a periodic
+    // image (|centre - x| < 0.49 L on every axis for the whole box), so that the lanes' own
+    // distances are the raw differences; it keeps a node unless even the box's nearest point is
+    // beyond r_cut + sqrt(3) half by a relative margin of 1e-5.
+    bool keep = false;
+    if ((uint32_t)lane < b_count) {
+      const float4 bc = sh.box_c, bh = sh.box_h, pg = bgeo[lane];
+      const float e0 = fabsf(pg.x - bc.x), e1 = fabsf(pg.y - bc.y), e2 = fabsf(pg.z - bc.z);
+      keep = true;
+      if (fmaxf(e0 + bh.x, fmaxf(e1 + bh.y, e2 + bh.z)) < w.guard) {
+        const float g0 = fmaxf(e0 - bh.x, 0.0f), g1 = fmaxf(e1 - bh.y, 0.0f), g2 = fmaxf(e2 - bh.z, 0.0f);
+        const float mr = w.r_cut + SQRT_3 * pg.w;
+        keep = !(g0 * g0 + g1 * g1 + g2 * g2 > mr * mr * 1.00001f);
+      }
+    }
+    const uint32_t cand = __ballot_sync(FULL, keep);
+
+    // Classify every remaining node of the batch for this lane: prune, direct sum, accept or open.
     uint32_t dmask = 0, nwmask = 0, amask = 0, omask = 0;
     if ((b_mask >> lane) & 1u) {
-      for (uint32_t c = 0; c < b_count; ++c) {
-        const float4 G = sh.geo[c];
+      for (uint32_t rem = cand; rem; rem &= rem - 1) {
+        const uint32_t c = __ffs(rem) - 1;
+        const float4 G = bgeo[c];
         float t0 = __fsub_rn(G.x, x0), t1 = __fsub_rn(G.y, x1), t2 = __fsub_rn(G.z, x2);
         // every source y of the node lies in [centre - half, centre + half]
         const bool nowrap = fmaxf(fabsf(t0), fmaxf(fabsf(t1), fabsf(t2))) + G.w < w.guard;
         min_image3(t0, t1, t2, w);
         const float max_r = __fadd_rn(w.r_cut, __fmul_rn(SQRT_3, G.w));
         if (norm2(t0, t1, t2) > __fmul_rn(max_r, max_r)) continue;
-        if ((sh.link[c].w & 1u) == 0u) {
+        if ((blink[c].w & 1u) == 0u) {
           // children[0] == NO_CHILD: direct sum over the node's particles (tree.rs:286-298)
           dmask |= 1u << c;
           nwmask |= (uint32_t)nowrap << c;
           continue;
         }
-        const float4 M = sh.mass[c];
+        const float4 M = bmass[c];
         float s0 = __fsub_rn(M.x, x0), s1 = __fsub_rn(M.y, x1), s2 = __fsub_rn(M.z, x2);
         min_image3(s0, s1, s2, w);
         if (accept_node(G.w, w.theta, norm2(s0, s1, s2)))
@@ -420,7 +462,7 @@ __global__ void __launch_bounds__(WALK_THREADS) k_tree_walk(const uint4* __restr
         break;
       }
       if ((ouni >> lane) & 1u) {
-        const uint4 L = sh.link[lane];
+        const uint4 L = blink[lane];
         const int slot = sp + __popc(ouni & ((1u << lane) - 1u));
         sh.stack[slot] = make_uint2(L.z, opened_by);
         sh.count[slot] = (unsigned char)__popc(L.w & 0xFFu);
@@ -429,7 +471,7 @@ __global__ void __launch_bounds__(WALK_THREADS) k_tree_walk(const uint4* __restr
       __syncwarp();
     }
 
-    // Prefetch the next batch into registers; the loads complete during the work below.
+    // Start copying the next batch; the copies complete during the work below.
     const bool more = sp > 0;
     uint32_t nx_count = 0, nx_mask = 0;
     if (more) {
@@ -438,22 +480,22 @@ __global__ void __launch_bounds__(WALK_THREADS) k_tree_walk(const uint4* __restr
       nx_count = sh.count[sp];
       nx_mask = top.y;
       if ((uint32_t)lane < nx_count) {
-        pg = __ldg(geo + first + lane);
-        pm4 = __ldg(mass + first + lane);
-        pl = __ldg(link + first + lane);
+        cp_async16(&sh.geo[cur ^ 1][lane], geo + first + lane);
+        cp_async16(&sh.mass[cur ^ 1][lane], mass + first + lane);
+        cp_async16(&sh.link[cur ^ 1][lane], link + first + lane);
       }
     }
 
     // Accepted centres of mass (tree.rs:299-305).
     for (; amask; amask &= amask - 1) {
       const int c = __ffs(amask) - 1;
-      const float4 M = sh.mass[c];
+      const float4 M = bmass[c];
       float s0 = __fsub_rn(M.x, x0), s1 = __fsub_rn(M.y, x1), s2 = __fsub_rn(M.z, x2);
       min_image3(s0, s1, s2, w);
       const float f = pair_factor(norm2(s0, s1, s2), neg_k * M.w, w, far);
-      a0 = fmaf(-s0, f, a0);
-      a1 = fmaf(-s1, f, a1);
-      a2 = fmaf(-s2, f, a2);
+      A0.x = fmaf(-s0, f, A0.x);
+      A1.x = fmaf(-s1, f, A1.x);
+      A2.x = fmaf(-s2, f, A2.x);
       ++n_accepts;
     }
 
@@ -462,7 +504,7 @@ __global__ void __launch_bounds__(WALK_THREADS) k_tree_walk(const uint4* __restr
     if (dset) {
       uint32_t total = 0;
       for (uint32_t rem = dset; rem; rem &= rem - 1) {
-        const uint4 L = sh.link[__ffs(rem) - 1];
+        const uint4 L = blink[__ffs(rem) - 1];
         const uint32_t cnt = L.y - L.x;
         total += cnt;
         if ((dmask >> (__ffs(rem) - 1)) & 1u) n_cand += cnt;
@@ -475,7 +517,7 @@ __global__ void __launch_bounds__(WALK_THREADS) k_tree_walk(const uint4* __restr
         uint32_t live = 0, selfbit = 0, off = 0;
         for (uint32_t rem = dset; rem && off < base + 32u; rem &= rem - 1) {
           const int c = __ffs(rem) - 1;
-          const uint4 L = sh.link[c];
+          const uint4 L = blink[c];
           const uint32_t cnt = L.y - L.x;
           if (g >= off && g < off + cnt) {
             const float4 y = __ldg(x4 + L.x + (g - off));
@@ -511,10 +553,10 @@ __global__ void __launch_bounds__(WALK_THREADS) k_tree_walk(const uint4* __restr
     if (!more) break;
     b_count = nx_count;
     b_mask = nx_mask;
+    cur ^= 1;
   }
-  a0 = __fadd_rn(a0, __fadd_rn(A0.x, A0.y));
-  a1 = __fadd_rn(a1, __fadd_rn(A1.x, A1.y));
-  a2 = __fadd_rn(a2, __fadd_rn(A2.x, A2.y));
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+  const float a0 = __fadd_rn(A0.x, A0.y), a1 = __fadd_rn(A1.x, A1.y), a2 = __fadd_rn(A2.x, A2.y);
   if (valid) {
     if (accumulate) {
       acc3[3 * i] = __fadd_rn(acc3[3 * i], a0);
