@@ -6,7 +6,7 @@ touch the GPU; the first call loads the library and fails loudly when it is miss
 """
 from ._native import CpmError, Cosmology, exported_symbols, lib  # noqa: F401
 from .api import (Context, Fft3, ForceSplit, Mesh, PoissonSolver, Simulation, density_contrast,  # noqa: F401
-                  interpolate3, ln_a_schedule, octant_keys, short_range_factor, tree_accelerations,
+                  interpolate3, ln_a_schedule, octant_keys, power_spectrum, short_range_factor, tree_accelerations,
                   wavenumber, zeldovich)
 
 __version__ = "0.1.0"

@@ -206,6 +206,19 @@ def octant_keys(positions, box_size: float, levels: int = 21) -> tuple[np.ndarra
     return keys, perm
 
 
+def power_spectrum(positions, box_size: float, mesh_n: int, n_shells: int) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """Shell-averaged matter power spectrum of the particles' CIC density on an n^3 mesh: the
+    estimator of ics.rs:213-266 (V |delta_k|^2 / M^2 in shells round(|m|) = 1..n_shells).
+    Returns (k_mean, p_mean, counts)."""
+    x = f32c(positions).reshape(-1, 3)
+    k = np.zeros(n_shells, np.float64)
+    p = np.zeros(n_shells, np.float64)
+    cnt = np.zeros(n_shells, np.uint64)
+    c = _ctx(int(mesh_n), box_size)
+    c._check(nat.lib().cpm_power_spectrum(c.h, ptr(x), len(x), int(n_shells), ptr(k), ptr(p), ptr(cnt)))
+    return k, p, cnt
+
+
 def ln_a_schedule(a_start: float, a_end: float, steps: int) -> list[float]:
     """runner.rs:240 / integrator.rs:168: a_i = a0 (a_end / a0)^(i / steps) in f32, i = 1..steps."""
     a0 = np.float32(a_start)
@@ -323,6 +336,14 @@ class Simulation:
     def delta(self) -> Mesh:
         """integrator.rs:128-131: density contrast of the last force calculation."""
         return Mesh(self.mesh_n, self.box_size, self.state(want_delta=True)["delta"])
+
+    def power_spectrum(self, n_shells: int) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+        """power_spectrum() of the current particles, computed on the device."""
+        k = np.zeros(n_shells, np.float64)
+        p = np.zeros(n_shells, np.float64)
+        cnt = np.zeros(n_shells, np.uint64)
+        check(nat.lib().cpm_sim_power_spectrum(self.h, int(n_shells), ptr(k), ptr(p), ptr(cnt)), sim=True)
+        return k, p, cnt
 
     def phase_times(self, reset: bool = False) -> tuple[np.ndarray, int]:
         ms = np.zeros(8, np.float64)

@@ -4,6 +4,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "cpm_internal.cuh"
 #include "cpm_host.h"
@@ -50,7 +51,7 @@ struct cpm_ctx {
   TreeNodes tree;
   DevBuf x, x_sorted, keys, vals, acc, acc_sorted, out;
   DevBuf mesh_fx, mesh_a, mesh_b, mesh_c, mesh_d, spec;
-  DevBuf status, tree_counters;
+  DevBuf status, tree_counters, pk;
   uint64_t last_nodes = 0, last_pairs = 0, last_accepts = 0;
   uint32_t last_depth = 0;
 };
@@ -129,7 +130,7 @@ int cpm_ctx_destroy(cpm_ctx* c) {
   for (DevBuf* b : {&c->sort.keys_alt, &c->sort.vals_alt, &c->sort.block_hist, &c->sort.scan_tmp, &c->tree.geo,
                     &c->tree.mass, &c->tree.link, &c->tree.counters, &c->tree.prefix, &c->tree.scan_tmp, &c->tree.x4, &c->x,
                     &c->x_sorted, &c->keys, &c->vals, &c->acc, &c->acc_sorted, &c->out, &c->mesh_fx, &c->mesh_a,
-                    &c->mesh_b, &c->mesh_c, &c->mesh_d, &c->spec, &c->status, &c->tree_counters})
+                    &c->mesh_b, &c->mesh_c, &c->mesh_d, &c->spec, &c->status, &c->tree_counters, &c->pk})
     release(*b);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -146,6 +147,31 @@ static int upload_positions(cpm_ctx* c, const float* x3, size_t n) {
 static int mesh_cells(cpm_ctx* c, size_t* m) {
   const size_t n = (size_t)c->n_mesh;
   *m = n * n * n;
+  return CPM_OK;
+}
+
+// Uploads x3, sorts it by octant key (so that each CTA's particles are compact and the deposit's
+// shared-memory tile path is taken) and deposits `mass` per particle into c->mesh_fx.
+static int deposit_fixed_ctx(cpm_ctx* c, const float* x3, size_t n, float mass, int* shift_out) {
+  size_t m;
+  mesh_cells(c, &m);
+  int rc;
+  CPM_CU(c, ensure(c->mesh_fx, m * sizeof(unsigned long long)));
+  if (n) {
+    if ((rc = upload_positions(c, x3, n))) return rc;
+    CPM_CU(c, ensure(c->keys, n * sizeof(uint64_t)));
+    CPM_CU(c, ensure(c->vals, n * sizeof(uint32_t)));
+    CPM_CU(c, ensure(c->x_sorted, 3 * n * sizeof(float)));
+    launch_octant_keys(as<float>(c->x), n, c->box, KEY_LEVELS, as<uint64_t>(c->keys), as<uint32_t>(c->vals),
+                       as<DevStatus>(c->status), c->stream);
+    CPM_CU(c, radix_sort_pairs(as<uint64_t>(c->keys), as<uint32_t>(c->vals), n, 3 * KEY_LEVELS, c->sort, c->stream));
+    launch_permute3(as<float>(c->x), as<uint32_t>(c->vals), n, as<float>(c->x_sorted), c->stream);
+  }
+  const float h = c->box / (float)c->n_mesh;
+  const int shift = fixed_point_shift((double)std::fabs(mass) * (double)n + 1.0);
+  launch_deposit_fixed(as<float>(c->x_sorted), n, mass, c->n_mesh, h, shift, as<unsigned long long>(c->mesh_fx),
+                       c->stream);
+  *shift_out = shift;
   return CPM_OK;
 }
 
@@ -180,6 +206,34 @@ static int deposit_common(cpm_ctx* c, const float* x3, size_t n, float mass, int
   launch_fixed_to_f32(as<unsigned long long>(c->mesh_fx), m, shift, to_delta, mean, as<float>(c->mesh_a), c->stream);
   CPM_CU(c, cudaMemcpyAsync(out, c->mesh_a.p, m * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
   return sync_and_check(c);
+}
+
+int cpm_power_spectrum(cpm_ctx* c, const float* x3, size_t n, int n_shells, double* k_mean, double* p_mean,
+                       uint64_t* counts) {
+  if (!c) return set_error(nullptr, CPM_E_INVALID, "context is NULL");
+  if (!x3 || !k_mean || !p_mean || !counts) return set_error(&c->err, CPM_E_INVALID, "power_spectrum: null pointer");
+  if (n == 0) return set_error(&c->err, CPM_E_INVALID, "power_spectrum: no particles");
+  if (n_shells < 1 || n_shells > PK_MAX_SHELLS)
+    return set_error(&c->err, CPM_E_INVALID, "power_spectrum: n_shells must be in [1, 2048]");
+  if (!poisson_supported(c->n_mesh))
+    return set_error(&c->err, CPM_E_UNSUPPORTED, "power_spectrum: mesh size must be a power of two in [4, 512]");
+  int rc = reset_status(c);
+  if (rc) return rc;
+  int shift = 0;
+  if ((rc = deposit_fixed_ctx(c, x3, n, 1.0f, &shift))) return rc;
+  CPM_CU(c, fft_plan_init(c->plan, c->n_mesh));
+  CPM_CU(c, ensure(c->spec, half_spectrum_elems(c->n_mesh) * sizeof(float2)));
+  CPM_CU(c, ensure(c->pk, sizeof(PkSums)));
+  size_t m;
+  mesh_cells(c, &m);
+  launch_r2c3(c->plan, nullptr, as<unsigned long long>(c->mesh_fx), shift, (float)n / (float)m, as<float2>(c->spec),
+              c->stream);
+  launch_pk_bin(as<float2>(c->spec), c->n_mesh, n_shells, as<PkSums>(c->pk), c->stream);
+  std::vector<PkSums> host(1);
+  CPM_CU(c, cudaMemcpyAsync(host.data(), c->pk.p, sizeof(PkSums), cudaMemcpyDeviceToHost, c->stream));
+  if ((rc = sync_and_check(c))) return rc;
+  pk_finish(host[0], c->n_mesh, c->box, n_shells, k_mean, p_mean, counts);
+  return CPM_OK;
 }
 
 int cpm_mesh_deposit(cpm_ctx* c, const float* x3, size_t n, float mass, float* cells_out) {

@@ -175,6 +175,25 @@ struct PoissonParams {
 void launch_poisson(const FftPlan& p, const PoissonParams& pp, const float* delta, const unsigned long long* fx,
                     int fx_shift, float mean, float2* spec, float* gx, float* gy, float* gz, cudaStream_t s);
 
+// Forward R2C transform (same inputs as launch_poisson) into one padded half spectrum.
+void launch_r2c3(const FftPlan& p, const float* delta, const unsigned long long* fx, int fx_shift, float mean,
+                 float2* spec, cudaStream_t s);
+
+// ---------------------------------------------------------------------------------------------
+// Power spectrum — pk.cu
+// ---------------------------------------------------------------------------------------------
+constexpr int PK_MAX_SHELLS = 2048;
+struct PkSums {
+  double power[PK_MAX_SHELLS + 1];  // sum over modes of |F_k|^2, shell s at index s
+  double kabs[PK_MAX_SHELLS + 1];   // sum over modes of |m|
+  unsigned long long count[PK_MAX_SHELLS + 1];
+};
+// Accumulates the half spectrum of an n^3 real field into integer shells 1..n_shells of `sums`
+// (zeroed inside); modes with 0 < kz < n/2 stand for themselves and their Hermitian mirror.
+void launch_pk_bin(const float2* spec, int n, int n_shells, PkSums* sums, cudaStream_t s);
+// P(k) from the shell sums: k_mean = (2 pi / L) sum|m| / count, p_mean = L^3 sum|F|^2 / (M^2 count).
+void pk_finish(const PkSums& sums, int n, float box, int n_shells, double* k_mean, double* p_mean, uint64_t* counts);
+
 // ---------------------------------------------------------------------------------------------
 // Gather — gather.cu
 // ---------------------------------------------------------------------------------------------

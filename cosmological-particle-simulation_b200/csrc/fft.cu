@@ -661,6 +661,41 @@ static void poisson_n(const FftPlan& p, const PoissonParams& pp, const float* de
   }
 }
 
+// Forward R2C n^3 transform of delta (f32, or the u64 fixed-point mass mesh converted to
+// delta = c/mean - 1 on load) into the padded half spectrum: z, then y, then x lines.
+template <int N>
+static void r2c3_n(const FftPlan& p, const float* delta, const unsigned long long* fx, int fx_shift, float mean,
+                   float2* spec, cudaStream_t s) {
+  const float2* tw = static_cast<const float2*>(p.twiddle.p);
+  constexpr int M = N / 2, NH = N / 2 + 1, NHP = N / 2 + 2;
+  const long long n = N;
+  const int rows = N * N;
+  {
+    constexpr int T = threads_for<M>();
+    constexpr int NB = 4 * c_tile(M) + c_tile(M) <= SMEM_LIMIT ? 2 : 1;
+    const size_t smem = (2 * NB + 1) * c_tile(M);
+    launch_persistent(k_r2c_z<N, NB, T>, T, smem, (rows + TW - 1) / TW, s, delta, fx, std::ldexp(1.0f, -fx_shift),
+                      mean, spec, rows, tw);
+  }
+  cols_pass<N>(spec, 0, 1, ColGeo{n * NHP, NHP, NH, 0, N}, 0, tw, s);  // y lines, outer = x
+  cols_pass<N>(spec, 0, 1, ColGeo{NHP, n * NHP, NH, 0, N}, 0, tw, s);  // x lines, outer = y
+}
+
+void launch_r2c3(const FftPlan& p, const float* delta, const unsigned long long* fx, int fx_shift, float mean,
+                 float2* spec, cudaStream_t s) {
+  switch (p.n) {
+    case 4: r2c3_n<4>(p, delta, fx, fx_shift, mean, spec, s); break;
+    case 8: r2c3_n<8>(p, delta, fx, fx_shift, mean, spec, s); break;
+    case 16: r2c3_n<16>(p, delta, fx, fx_shift, mean, spec, s); break;
+    case 32: r2c3_n<32>(p, delta, fx, fx_shift, mean, spec, s); break;
+    case 64: r2c3_n<64>(p, delta, fx, fx_shift, mean, spec, s); break;
+    case 128: r2c3_n<128>(p, delta, fx, fx_shift, mean, spec, s); break;
+    case 256: r2c3_n<256>(p, delta, fx, fx_shift, mean, spec, s); break;
+    case 512: r2c3_n<512>(p, delta, fx, fx_shift, mean, spec, s); break;
+    default: break;
+  }
+}
+
 void launch_poisson(const FftPlan& p, const PoissonParams& pp, const float* delta, const unsigned long long* fx,
                     int fx_shift, float mean, float2* spec, float* gx, float* gy, float* gz, cudaStream_t s) {
   switch (p.n) {

@@ -32,7 +32,7 @@ struct cpm_sim {
   FftPlan plan;
   SortScratch sort;
   TreeNodes tree;
-  DevBuf x, p, acc, id, x2, p2, id2, keys, vals, fx, gx, gy, gz, spec, status, counters;
+  DevBuf x, p, acc, id, x2, p2, id2, keys, vals, fx, gx, gy, gz, spec, status, counters, pk;
   // Per-step phase events, recorded without host synchronisation into a ring of RING steps and
   // folded into phase_ms when the ring fills or cpm_sim_phase_times is called.
   static constexpr int RING = 64;
@@ -330,6 +330,26 @@ int cpm_sim_get_state(cpm_sim* s, float* x3, float* p3, float* acc3, float* delt
   return sim_check(s);
 }
 
+int cpm_sim_power_spectrum(cpm_sim* s, int n_shells, double* k_mean, double* p_mean, uint64_t* counts) {
+  if (!s) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_power_spectrum: sim is NULL");
+  if (!k_mean || !p_mean || !counts) return set_error(&s->err, CPM_E_INVALID, "cpm_sim_power_spectrum: null pointer");
+  if (n_shells < 1 || n_shells > PK_MAX_SHELLS)
+    return set_error(&s->err, CPM_E_INVALID, "cpm_sim_power_spectrum: n_shells must be in [1, 2048]");
+  const int mn = s->P.mesh_n;
+  // The deposit of the current positions (the mesh of the last force evaluation may predate a
+  // set_state); the next step deposits again before it uses the mesh.
+  launch_deposit_fixed(as<float>(s->x), s->n, 1.0f, mn, s->h, s->shift, as<unsigned long long>(s->fx), s->stream);
+  launch_r2c3(s->plan, nullptr, as<unsigned long long>(s->fx), s->shift, s->mean, as<float2>(s->spec), s->stream);
+  SIM_CU(s, ensure(s->pk, sizeof(PkSums)));
+  launch_pk_bin(as<float2>(s->spec), mn, n_shells, as<PkSums>(s->pk), s->stream);
+  std::vector<PkSums> host(1);
+  SIM_CU(s, cudaMemcpyAsync(host.data(), s->pk.p, sizeof(PkSums), cudaMemcpyDeviceToHost, s->stream));
+  int rc = sim_check(s);
+  if (rc) return rc;
+  pk_finish(host[0], mn, s->box, n_shells, k_mean, p_mean, counts);
+  return CPM_OK;
+}
+
 int cpm_sim_phase_times(cpm_sim* s, double* ms8, uint64_t* steps, int reset) {
   if (!s) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_phase_times: sim is NULL");
   int rc = flush_timing(s);
@@ -381,7 +401,7 @@ int cpm_sim_destroy(cpm_sim* s) {
   for (DevBuf* b : {&s->sort.keys_alt, &s->sort.vals_alt, &s->sort.block_hist, &s->sort.scan_tmp, &s->tree.geo,
                     &s->tree.mass, &s->tree.link, &s->tree.counters, &s->tree.prefix, &s->tree.scan_tmp, &s->tree.x4, &s->x, &s->p,
                     &s->acc, &s->id, &s->x2, &s->p2, &s->id2, &s->keys, &s->vals, &s->fx, &s->gx, &s->gy, &s->gz,
-                    &s->spec, &s->status, &s->counters})
+                    &s->spec, &s->status, &s->counters, &s->pk})
     release(*b);
   release(s->host_tmp);
   for (auto& row : s->ev)

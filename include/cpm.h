@@ -150,6 +150,17 @@ int cpm_tree_stats(cpm_ctx* ctx, uint64_t* nodes, uint64_t* leaf_pairs, uint64_t
 int cpm_ics_zeldovich(int n_side, float box_size, const cpm_cosmology* cosmo, float n_s, float sigma8, float a_init,
                       uint64_t seed, float* x3, float* p3);
 
+/* No counterpart in the reference, whose only power-spectrum estimator is inside the test
+ * ics.rs:213-266. The same estimator (P = V |delta_k|^2 / M^2 averaged over integer shells
+ * round(|m|), ics.rs:229-243, Nyquist modes included) applied to the CIC density of n particles
+ * x3 on the context's mesh (mesh.rs:29-69; delta = rho/mean - 1 as integrator.rs:117-126).
+ * Shell s = 1..n_shells (1 <= n_shells <= 2048) fills k_mean[s-1] (mean of 2 pi |m| / L over its
+ * modes), p_mean[s-1] (mean power) and counts[s-1] (modes; 0 leaves k_mean and p_mean 0). The
+ * context's mesh must be a power of two in [4, 512]. Sums are FP64; their last bits may vary from
+ * run to run (atomic summation order). */
+int cpm_power_spectrum(cpm_ctx* ctx, const float* x3, size_t n, int n_shells, double* k_mean, double* p_mean,
+                       uint64_t* counts);
+
 /* ------------------------------------------------------------------ device-resident simulation */
 /* Replaces `Simulation` (integrator.rs:34-186) under a `cuda` feature: state stays in HBM and
  * `step_to` runs one KDK step (kick, drift, deposit, FFT-Poisson, gather, tree build and walk,
@@ -194,6 +205,8 @@ int cpm_sim_step_to(cpm_sim* sim, float a1);
 int cpm_sim_step_host(cpm_sim* sim, float a1, float* x3, float* p3);
 /* Reads the state in the caller's particle order. Any pointer may be NULL. delta is n^3. */
 int cpm_sim_get_state(cpm_sim* sim, float* x3, float* p3, float* acc3, float* delta, float* a);
+/* cpm_power_spectrum of the simulation's current particles on its mesh, without copying them. */
+int cpm_sim_power_spectrum(cpm_sim* sim, int n_shells, double* k_mean, double* p_mean, uint64_t* counts);
 /* Overwrites positions and momenta (caller's order) and recomputes the acceleration at the current a. */
 int cpm_sim_set_state(cpm_sim* sim, const float* x3, const float* p3);
 /* Average device milliseconds per step of each phase since the last reset (needs CPM_SIM_TIMING):
