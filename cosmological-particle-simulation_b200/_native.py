@@ -101,6 +101,7 @@ def lib() -> C.CDLL:
         "cpm_tree_stats": (i, [vp, C.POINTER(u64), C.POINTER(u64), C.POINTER(u64), C.POINTER(u32)]),
         "cpm_ics_zeldovich": (i, [i, fl, C.POINTER(Cosmology), fl, fl, fl, u64, vp, vp]),
         "cpm_power_spectrum": (i, [vp, vp, sz, i, vp, vp, vp]),
+        "cpm_fft_supported": (i, [i]),
         "cpm_sim_power_spectrum": (i, [vp, i, vp, vp, vp]),
         "cpm_sim_create": (i, [C.POINTER(SimParams), vp, vp, fl, C.POINTER(vp)]),
         "cpm_sim_create_zeldovich": (i, [C.POINTER(SimParams), i, fl, fl, fl, u64, C.POINTER(vp)]),

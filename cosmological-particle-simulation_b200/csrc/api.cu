@@ -208,6 +208,8 @@ static int deposit_common(cpm_ctx* c, const float* x3, size_t n, float mass, int
   return sync_and_check(c);
 }
 
+int cpm_fft_supported(int n) { return fft_supported(n) ? 1 : 0; }
+
 int cpm_power_spectrum(cpm_ctx* c, const float* x3, size_t n, int n_shells, double* k_mean, double* p_mean,
                        uint64_t* counts) {
   if (!c) return set_error(nullptr, CPM_E_INVALID, "context is NULL");
@@ -216,7 +218,7 @@ int cpm_power_spectrum(cpm_ctx* c, const float* x3, size_t n, int n_shells, doub
   if (n_shells < 1 || n_shells > PK_MAX_SHELLS)
     return set_error(&c->err, CPM_E_INVALID, "power_spectrum: n_shells must be in [1, 2048]");
   if (!poisson_supported(c->n_mesh))
-    return set_error(&c->err, CPM_E_UNSUPPORTED, "power_spectrum: mesh size must be a power of two in [4, 512]");
+    return set_error(&c->err, CPM_E_UNSUPPORTED, std::string("power_spectrum: mesh size must be ") + fft_sizes_text());
   int rc = reset_status(c);
   if (rc) return rc;
   int shift = 0;
@@ -291,7 +293,7 @@ int cpm_fft3(cpm_ctx* c, cpm_cf32* data, int n, int inverse) {
   if (!data) return set_error(&c->err, CPM_E_INVALID, "fft3: data is NULL");
   if (n != c->n_mesh) return set_error(&c->err, CPM_E_MESH_MISMATCH, "fft3: n differs from the context's mesh size");
   if (!fft_supported(n))
-    return set_error(&c->err, CPM_E_UNSUPPORTED, "fft3: n = " + std::to_string(n) + " is not a power of two in [4, 1024]");
+    return set_error(&c->err, CPM_E_UNSUPPORTED, "fft3: n = " + std::to_string(n) + " is not one of " + fft_sizes_text());
   int rc = reset_status(c);
   if (rc) return rc;
   CPM_CU(c, fft_plan_init(c->plan, n));
@@ -316,7 +318,7 @@ int cpm_poisson_accel(cpm_ctx* c, const float* delta, int n, const cpm_cosmology
   if (!delta || !cosmo || !gx || !gy || !gz) return set_error(&c->err, CPM_E_INVALID, "poisson: null pointer");
   if (n != c->n_mesh) return set_error(&c->err, CPM_E_MESH_MISMATCH, "poisson: mesh size must match the solver");
   if (!poisson_supported(n))
-    return set_error(&c->err, CPM_E_UNSUPPORTED, "poisson: n = " + std::to_string(n) + " is not a power of two in [4, 512]");
+    return set_error(&c->err, CPM_E_UNSUPPORTED, "poisson: n = " + std::to_string(n) + " is not one of " + fft_sizes_text());
   if (!(a > 0.0f)) return set_error(&c->err, CPM_E_INVALID, "poisson: a must be > 0");
   int rc = reset_status(c);
   if (rc) return rc;

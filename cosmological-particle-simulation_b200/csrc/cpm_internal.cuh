@@ -146,9 +146,10 @@ void launch_fixed_to_f32(const unsigned long long* fx, size_t m, int shift, int 
 // ---------------------------------------------------------------------------------------------
 // FFT / Poisson — fft.cu
 // ---------------------------------------------------------------------------------------------
+// Mesh sizes with compiled transforms (powers of two 4..1024 and some 2^a 3^b 5^c sizes).
 bool fft_supported(int n);
-// Mesh sizes the fused Poisson pass supports (its two shared-memory tiles must fit one SM).
 bool poisson_supported(int n);
+const char* fft_sizes_text();  // the list of supported sizes, for error messages
 struct FftPlan {
   int n = 0;
   DevBuf twiddle;  // exp(-2 pi i m / n), m < n, float2 built from double

@@ -45,10 +45,12 @@ constexpr int TW = 16;       // lines per tile
 constexpr int TLD = TW + 1;  // shared-memory row pitch (elements)
 constexpr size_t SMEM_LIMIT = 227 * 1024;
 
-// Threads of a CTA that transforms TW lines of length L: one radix-8 butterfly each, 256..1024.
+// Threads of a CTA that transforms TW lines of length L: about one radix-8 butterfly each,
+// a multiple of 32 in 256..1024.
 template <int L>
 constexpr int threads_for() {
-  return TW * L / 8 < 256 ? 256 : (TW * L / 8 > 1024 ? 1024 : TW * L / 8);
+  constexpr int t = (TW * L / 8 + 31) / 32 * 32;
+  return t < 256 ? 256 : (t > 1024 ? 1024 : t);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -104,10 +106,42 @@ __device__ __forceinline__ void dft8(float2* v) {
   v[7] = csub(e3, t3);
 }
 
+template <bool INV>
+__device__ __forceinline__ void dft3(float2* v) {
+  // y1,2 = x0 - (x1 + x2)/2 -/+ i (sqrt(3)/2)(x1 - x2) (signs of i flipped for the inverse)
+  const float h = 0.86602540378443864676f;
+  const float2 t1 = cadd(v[1], v[2]), t2 = csub(v[1], v[2]);
+  const float2 m = make_float2(v[0].x - 0.5f * t1.x, v[0].y - 0.5f * t1.y);
+  const float2 r = rot90<INV>(make_float2(h * t2.x, h * t2.y));
+  v[0] = cadd(v[0], t1);
+  v[1] = cadd(m, r);
+  v[2] = csub(m, r);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft5(float2* v) {
+  // t1 = x1 + x4, t2 = x2 + x3, t3 = x1 - x4, t4 = x2 - x3;
+  // y1,4 = x0 + c1 t1 + c2 t2 -/+ i (s1 t3 + s2 t4), y2,3 = x0 + c2 t1 + c1 t2 -/+ i (s2 t3 - s1 t4)
+  const float c1 = 0.30901699437494742410f, c2 = -0.80901699437494742410f;
+  const float s1 = 0.95105651629515357212f, s2 = 0.58778525229247312917f;
+  const float2 t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]), t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
+  const float2 m1 = make_float2(v[0].x + c1 * t1.x + c2 * t2.x, v[0].y + c1 * t1.y + c2 * t2.y);
+  const float2 m2 = make_float2(v[0].x + c2 * t1.x + c1 * t2.x, v[0].y + c2 * t1.y + c1 * t2.y);
+  const float2 n1 = rot90<INV>(make_float2(s1 * t3.x + s2 * t4.x, s1 * t3.y + s2 * t4.y));
+  const float2 n2 = rot90<INV>(make_float2(s2 * t3.x - s1 * t4.x, s2 * t3.y - s1 * t4.y));
+  v[0] = cadd(v[0], cadd(t1, t2));
+  v[1] = cadd(m1, n1);
+  v[4] = csub(m1, n1);
+  v[2] = cadd(m2, n2);
+  v[3] = csub(m2, n2);
+}
+
 template <int R, bool INV>
 __device__ __forceinline__ void dft(float2* v) {
   if constexpr (R == 2) dft2<INV>(v);
+  else if constexpr (R == 3) dft3<INV>(v);
   else if constexpr (R == 4) dft4<INV>(v[0], v[1], v[2], v[3]);
+  else if constexpr (R == 5) dft5<INV>(v);
   else dft8<INV>(v);
 }
 
@@ -153,24 +187,33 @@ __device__ __forceinline__ void stockham_stage(float2* sm, const float2* __restr
   __syncthreads();
 }
 
-// Full length-N transform of the tile: radix-8 stages, then a final radix-4 or radix-2 stage.
+// Radix of the next Stockham stage for a remaining length L = 2^a 3^b 5^c: 8 while it divides,
+// then 4 or 2, then 3s, then 5s (powers of two: 8..8 then one 4 or 2).
+template <int L>
+constexpr int next_radix() {
+  return L % 8 == 0 ? 8 : (L % 4 == 0 ? 4 : (L % 2 == 0 ? 2 : (L % 3 == 0 ? 3 : 5)));
+}
+constexpr bool smooth235(int n) {
+  while (n % 2 == 0) n /= 2;
+  while (n % 3 == 0) n /= 3;
+  while (n % 5 == 0) n /= 5;
+  return n == 1;
+}
+
+template <int N, int NS, bool INV, int T, int TS>
+__device__ __forceinline__ void fft_stages(float2* sm, const float2* __restrict__ tw) {
+  if constexpr (NS < N) {
+    constexpr int R = next_radix<N / NS>();
+    stockham_stage<N, R, NS, INV, T, TS>(sm, tw);
+    fft_stages<N, NS * R, INV, T, TS>(sm, tw);
+  }
+}
+
+// Full length-N transform of the tile (N = 2^a 3^b 5^c).
 template <int N, bool INV, int T, int TS = 1>
 __device__ __forceinline__ void fft_lines(float2* sm, const float2* __restrict__ tw) {
-  static_assert((N & (N - 1)) == 0 && N >= 2 && N <= 1024, "power-of-two lengths 2..1024");
-  if constexpr (N == 2) {
-    stockham_stage<N, 2, 1, INV, T, TS>(sm, tw);
-  } else if constexpr (N == 4) {
-    stockham_stage<N, 4, 1, INV, T, TS>(sm, tw);
-  } else {
-    stockham_stage<N, 8, 1, INV, T, TS>(sm, tw);
-    if constexpr (N == 16) stockham_stage<N, 2, 8, INV, T, TS>(sm, tw);
-    if constexpr (N == 32) stockham_stage<N, 4, 8, INV, T, TS>(sm, tw);
-    if constexpr (N >= 64) stockham_stage<N, 8, 8, INV, T, TS>(sm, tw);
-    if constexpr (N == 128) stockham_stage<N, 2, 64, INV, T, TS>(sm, tw);
-    if constexpr (N == 256) stockham_stage<N, 4, 64, INV, T, TS>(sm, tw);
-    if constexpr (N >= 512) stockham_stage<N, 8, 64, INV, T, TS>(sm, tw);
-    if constexpr (N == 1024) stockham_stage<N, 2, 512, INV, T, TS>(sm, tw);
-  }
+  static_assert(N >= 2 && N <= 1024 && smooth235(N), "lengths 2..1024 with prime factors 2, 3, 5");
+  fft_stages<N, 1, INV, T, TS>(sm, tw);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -310,18 +353,18 @@ __global__ void __launch_bounds__(T) k_fft_rows(float2* data, int rows, const fl
       smem, N * TLD, (rows + TW - 1) / TW,
       [&](float2* buf, int tile) {
         const int row0 = tile * TW, valid = min(TW, rows - row0);
-        for (int q = threadIdx.x; q < N * TW; q += T) {
+        for (int q = threadIdx.x; q < row_span<N>(N); q += T) {
           const int t = row_t<N>(q), l = row_l<N>(q);
-          if (l < valid) cp_async8(buf + t * TLD + l, data + (size_t)(row0 + l) * N + t);
+          if (l < valid && t < N) cp_async8(buf + t * TLD + l, data + (size_t)(row0 + l) * N + t);
         }
       },
       [&](float2* cur, int tile) {
         const int row0 = tile * TW, valid = min(TW, rows - row0);
         fft_lines<N, INV, T>(cur, tw);
 #pragma unroll 4
-        for (int q = threadIdx.x; q < N * TW; q += T) {
+        for (int q = threadIdx.x; q < row_span<N>(N); q += T) {
           const int t = row_t<N>(q), l = row_l<N>(q);
-          if (l < valid) data[(size_t)(row0 + l) * N + t] = cur[t * TLD + l];
+          if (l < valid && t < N) data[(size_t)(row0 + l) * N + t] = cur[t * TLD + l];
         }
       });
 }
@@ -342,9 +385,9 @@ __global__ void __launch_bounds__(T) k_r2c_z(const float* __restrict__ delta,
       smem, 2 * M * TLD, (rows + TW - 1) / TW,
       [&](float2* buf, int tile) {
         const int row0 = tile * TW, valid = min(TW, rows - row0);
-        for (int q = threadIdx.x; q < M * TW; q += T) {
+        for (int q = threadIdx.x; q < row_span<M>(M); q += T) {
           const int m = row_t<M>(q), l = row_l<M>(q);
-          if (l >= valid) continue;
+          if (l >= valid || m >= M) continue;
           const size_t gi = (size_t)(row0 + l) * N + 2 * m;
           if (fx)
             cp_async16(buf + 2 * (m * TLD + l), fx + gi);
@@ -375,8 +418,9 @@ __global__ void __launch_bounds__(T) k_r2c_z(const float* __restrict__ delta,
         for (int q = threadIdx.x; q < row_span<M>(NH); q += T) {
           const int k = row_t<M>(q), l = row_l<M>(q);
           if (l >= valid || k >= NH) continue;
-          const float2 zk = cplx[(k & (M - 1)) * TLD + l];
-          const float2 zm = cplx[((M - k) & (M - 1)) * TLD + l];
+          // Z is M-periodic: Z[M] = Z[0] (k runs over 0..M)
+          const float2 zk = cplx[(k == M ? 0 : k) * TLD + l];
+          const float2 zm = cplx[(k == 0 ? 0 : M - k) * TLD + l];
           const float2 fe = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
           const float2 fo = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
           spec[(size_t)(row0 + l) * NHP + k] = cadd(fe, cmul(__ldg(tw + k), fo));
@@ -428,9 +472,9 @@ __global__ void __launch_bounds__(T) k_c2r_z(const float2* __restrict__ spec, lo
         __syncthreads();
         fft_lines<M, true, T, 2>(cur, tw);
 #pragma unroll 4
-        for (int q = threadIdx.x; q < M * TW; q += T) {
+        for (int q = threadIdx.x; q < row_span<M>(M); q += T) {
           const int m = row_t<M>(q), l = row_l<M>(q);
-          if (l < valid) {
+          if (l < valid && m < M) {
             const float2 v = cur[m * TLD + l];
             reinterpret_cast<float2*>(out + (size_t)(row0 + l) * N)[m] =
                 make_float2(__fmul_rn(v.x, scale), __fmul_rn(v.y, scale));
@@ -511,11 +555,63 @@ __global__ void __launch_bounds__(T) k_poisson_x(const float2* __restrict__ spec
       });
 }
 
+// Green's function and gradient of poisson.rs:52-74 applied elementwise to the half spectrum in
+// slot 0, writing -i k_a phi to slots 0..2 (the same f32 operations as k_poisson_x). Used where
+// the fused x pass does not fit in shared memory.
+__global__ void k_green_grad(float2* spec, long long comp, int n, PoissonParams pp, const float* __restrict__ deconv) {
+  const int nh = n / 2 + 1, nhp = n / 2 + 2;
+  const long long total = (long long)n * n * nh;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int kz = (int)(e % nh);
+    const long long line = e / nh;
+    const int iy = (int)(line % n), ix = (int)(line / n);
+    const long long gi = line * nhp + kz;
+    const float kx = wavenumber(ix, n, pp.two_pi_over_l), ky = wavenumber(iy, n, pp.two_pi_over_l);
+    const float kzv = wavenumber(kz, n, pp.two_pi_over_l);
+    float k2 = -0.0f;
+    k2 = __fadd_rn(k2, __fmul_rn(kx, kx));
+    k2 = __fadd_rn(k2, __fmul_rn(ky, ky));
+    k2 = __fadd_rn(k2, __fmul_rn(kzv, kzv));
+    float2 v = spec[gi];
+    if (k2 == 0.0f) {
+      v = make_float2(0.0f, 0.0f);
+    } else {
+      const float filter = expf(__fmul_rn(__fmul_rn(-k2, pp.r_split), pp.r_split));
+      float sc = __fmul_rn(__fdiv_rn(-pp.prefactor, k2), filter);
+      if (deconv) sc = __fmul_rn(sc, __fmul_rn(__fmul_rn(deconv[ix], deconv[iy]), deconv[kz]));
+      v = make_float2(__fmul_rn(v.x, sc), __fmul_rn(v.y, sc));
+    }
+    const float nk[3] = {-kx, -ky, -kzv};
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+      spec[a * comp + gi] = make_float2(__fsub_rn(__fmul_rn(v.x, 0.0f), __fmul_rn(v.y, nk[a])),
+                                        __fadd_rn(__fmul_rn(v.x, nk[a]), __fmul_rn(v.y, 0.0f)));
+  }
+}
+
 // ---------------------------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------------------------
-bool fft_supported(int n) { return n >= 4 && n <= 1024 && (n & (n - 1)) == 0; }
-bool poisson_supported(int n) { return fft_supported(n) && n <= 512; }
+// Mesh sizes with compiled transforms: powers of two 4..1024 and the 2^a 3^b 5^c sizes below.
+#define CPM_FFT_SIZES(X) \
+  X(4) X(8) X(16) X(32) X(48) X(64) X(80) X(96) X(128) X(160) X(192) X(256) X(320) X(384) X(512) X(1024)
+
+bool fft_supported(int n) {
+  switch (n) {
+#define CPM_CASE(N) case N:
+    CPM_FFT_SIZES(CPM_CASE)
+#undef CPM_CASE
+    return true;
+    default:
+      return false;
+  }
+}
+bool poisson_supported(int n) { return fft_supported(n); }
+
+const char* fft_sizes_text() {
+  return "4, 8, 16, 32, 48, 64, 80, 96, 128, 160, 192, 256, 320, 384, 512 or 1024";
+}
 
 size_t half_spectrum_elems(int n) { return (size_t)n * n * (size_t)(n / 2 + 2); }
 
@@ -609,55 +705,11 @@ static void fft3_c2c_n(float2* data, int inverse, const float2* tw, cudaStream_t
 void launch_fft3_c2c(const FftPlan& p, float2* data, int inverse, cudaStream_t s) {
   const float2* tw = static_cast<const float2*>(p.twiddle.p);
   switch (p.n) {
-    case 4: fft3_c2c_n<4>(data, inverse, tw, s); break;
-    case 8: fft3_c2c_n<8>(data, inverse, tw, s); break;
-    case 16: fft3_c2c_n<16>(data, inverse, tw, s); break;
-    case 32: fft3_c2c_n<32>(data, inverse, tw, s); break;
-    case 64: fft3_c2c_n<64>(data, inverse, tw, s); break;
-    case 128: fft3_c2c_n<128>(data, inverse, tw, s); break;
-    case 256: fft3_c2c_n<256>(data, inverse, tw, s); break;
-    case 512: fft3_c2c_n<512>(data, inverse, tw, s); break;
-    case 1024: fft3_c2c_n<1024>(data, inverse, tw, s); break;
+#define CPM_CASE(N) \
+  case N: fft3_c2c_n<N>(data, inverse, tw, s); break;
+    CPM_FFT_SIZES(CPM_CASE)
+#undef CPM_CASE
     default: break;
-  }
-}
-
-template <int N>
-static void poisson_n(const FftPlan& p, const PoissonParams& pp, const float* delta, const unsigned long long* fx,
-                      int fx_shift, float mean, float2* spec, float* gx, float* gy, float* gz, cudaStream_t s) {
-  const float2* tw = static_cast<const float2*>(p.twiddle.p);
-  const float* deconv = pp.deconvolve ? static_cast<const float*>(p.deconv.p) : nullptr;
-  constexpr int M = N / 2, NH = N / 2 + 1, NHP = N / 2 + 2;
-  const long long n = N;
-  const long long comp = n * n * NHP;  // elements per half spectrum
-  const int rows = N * N;
-  const int row_tiles = (rows + TW - 1) / TW;
-  // Slot 0 holds the forward spectrum; the x pass reads each tile of it before writing the
-  // same tile of slots 0..2, and tiles are disjoint, so the update in place is safe.
-  float2* s0 = spec;
-  {  // 1. z: R2C into slot 0 (staging buffers of 16-byte slots + one complex tile)
-    constexpr int T = threads_for<M>();
-    constexpr int NB = 4 * c_tile(M) + c_tile(M) <= SMEM_LIMIT ? 2 : 1;
-    const size_t smem = (2 * NB + 1) * c_tile(M);
-    launch_persistent(k_r2c_z<N, NB, T>, T, smem, row_tiles, s, delta, fx, std::ldexp(1.0f, -fx_shift), mean, s0,
-                      rows, tw);
-  }
-  // 2. y forward on slot 0: lines along y (stride NHP), columns along kz adjacent, outer = x
-  cols_pass<N>(s0, 0, 1, ColGeo{n * NHP, NHP, NH, 0, N}, 0, tw, s);
-  {  // 3. x forward + Green + gradient + x inverse -> slots 0..2; outer = y
-    constexpr int T = threads_for<N>();
-    constexpr int NBX = 3 * c_tile(N) <= SMEM_LIMIT ? 2 : 1;
-    const size_t smem = (NBX + 1) * c_tile(N);
-    ColGeo g{NHP, n * NHP, NH, (NH + TW - 1) / TW, N};
-    launch_persistent(k_poisson_x<N, NBX, T>, T, smem, g.outer * g.col_tiles, s, s0, spec, comp, g, pp, deconv, tw);
-  }
-  // 4. y inverse on the three component spectra
-  cols_pass<N>(spec, comp, 3, ColGeo{n * NHP, NHP, NH, 0, N}, 1, tw, s);
-  {  // 5. z: C2R with 1/n^3
-    constexpr int T = threads_for<M>();
-    constexpr int NB = 2 * c_tile(M + 1) <= SMEM_LIMIT ? 2 : 1;
-    const size_t smem = NB * c_tile(M + 1);
-    launch_persistent(k_c2r_z<N, NB, T>, T, smem, 3 * row_tiles, s, spec, comp, gx, gy, gz, pp.scale, rows, tw);
   }
 }
 
@@ -681,17 +733,63 @@ static void r2c3_n(const FftPlan& p, const float* delta, const unsigned long lon
   cols_pass<N>(spec, 0, 1, ColGeo{NHP, n * NHP, NH, 0, N}, 0, tw, s);  // x lines, outer = y
 }
 
+template <int N>
+static void poisson_n(const FftPlan& p, const PoissonParams& pp, const float* delta, const unsigned long long* fx,
+                      int fx_shift, float mean, float2* spec, float* gx, float* gy, float* gz, cudaStream_t s) {
+  const float2* tw = static_cast<const float2*>(p.twiddle.p);
+  const float* deconv = pp.deconvolve ? static_cast<const float*>(p.deconv.p) : nullptr;
+  constexpr int M = N / 2, NH = N / 2 + 1, NHP = N / 2 + 2;
+  const long long n = N;
+  const long long comp = n * n * NHP;  // elements per half spectrum
+  const int rows = N * N;
+  const int row_tiles = (rows + TW - 1) / TW;
+  if constexpr (2 * c_tile(N) > SMEM_LIMIT) {
+    // The fused x pass needs two N-point tiles: not on one SM at this size. Forward R2C, the
+    // Green's function and gradient elementwise, then inverse x and y passes on three spectra.
+    r2c3_n<N>(p, delta, fx, fx_shift, mean, spec, s);
+    const long long total = n * n * NH;
+    const int grid = (int)std::min<long long>((total + 255) / 256, 16LL * num_sms());
+    count_launch();
+    k_green_grad<<<grid, 256, 0, s>>>(spec, comp, N, pp, deconv);
+    cols_pass<N>(spec, comp, 3, ColGeo{NHP, n * NHP, NH, 0, N}, 1, tw, s);  // x lines, outer = y
+  } else {
+    // Slot 0 holds the forward spectrum; the x pass reads each tile of it before writing the
+    // same tile of slots 0..2, and tiles are disjoint, so the update in place is safe.
+    float2* s0 = spec;
+    {  // 1. z: R2C into slot 0 (staging buffers of 16-byte slots + one complex tile)
+      constexpr int T = threads_for<M>();
+      constexpr int NB = 4 * c_tile(M) + c_tile(M) <= SMEM_LIMIT ? 2 : 1;
+      const size_t smem = (2 * NB + 1) * c_tile(M);
+      launch_persistent(k_r2c_z<N, NB, T>, T, smem, row_tiles, s, delta, fx, std::ldexp(1.0f, -fx_shift), mean, s0,
+                        rows, tw);
+    }
+    // 2. y forward on slot 0: lines along y (stride NHP), columns along kz adjacent, outer = x
+    cols_pass<N>(s0, 0, 1, ColGeo{n * NHP, NHP, NH, 0, N}, 0, tw, s);
+    {  // 3. x forward + Green + gradient + x inverse -> slots 0..2; outer = y
+      constexpr int T = threads_for<N>();
+      constexpr int NBX = 3 * c_tile(N) <= SMEM_LIMIT ? 2 : 1;
+      const size_t smem = (NBX + 1) * c_tile(N);
+      ColGeo g{NHP, n * NHP, NH, (NH + TW - 1) / TW, N};
+      launch_persistent(k_poisson_x<N, NBX, T>, T, smem, g.outer * g.col_tiles, s, s0, spec, comp, g, pp, deconv, tw);
+    }
+  }
+  // 4. y inverse on the three component spectra
+  cols_pass<N>(spec, comp, 3, ColGeo{n * NHP, NHP, NH, 0, N}, 1, tw, s);
+  {  // 5. z: C2R with 1/n^3
+    constexpr int T = threads_for<M>();
+    constexpr int NB = 2 * c_tile(M + 1) <= SMEM_LIMIT ? 2 : 1;
+    const size_t smem = NB * c_tile(M + 1);
+    launch_persistent(k_c2r_z<N, NB, T>, T, smem, 3 * row_tiles, s, spec, comp, gx, gy, gz, pp.scale, rows, tw);
+  }
+}
+
 void launch_r2c3(const FftPlan& p, const float* delta, const unsigned long long* fx, int fx_shift, float mean,
                  float2* spec, cudaStream_t s) {
   switch (p.n) {
-    case 4: r2c3_n<4>(p, delta, fx, fx_shift, mean, spec, s); break;
-    case 8: r2c3_n<8>(p, delta, fx, fx_shift, mean, spec, s); break;
-    case 16: r2c3_n<16>(p, delta, fx, fx_shift, mean, spec, s); break;
-    case 32: r2c3_n<32>(p, delta, fx, fx_shift, mean, spec, s); break;
-    case 64: r2c3_n<64>(p, delta, fx, fx_shift, mean, spec, s); break;
-    case 128: r2c3_n<128>(p, delta, fx, fx_shift, mean, spec, s); break;
-    case 256: r2c3_n<256>(p, delta, fx, fx_shift, mean, spec, s); break;
-    case 512: r2c3_n<512>(p, delta, fx, fx_shift, mean, spec, s); break;
+#define CPM_CASE(N) \
+  case N: r2c3_n<N>(p, delta, fx, fx_shift, mean, spec, s); break;
+    CPM_FFT_SIZES(CPM_CASE)
+#undef CPM_CASE
     default: break;
   }
 }
@@ -699,14 +797,10 @@ void launch_r2c3(const FftPlan& p, const float* delta, const unsigned long long*
 void launch_poisson(const FftPlan& p, const PoissonParams& pp, const float* delta, const unsigned long long* fx,
                     int fx_shift, float mean, float2* spec, float* gx, float* gy, float* gz, cudaStream_t s) {
   switch (p.n) {
-    case 4: poisson_n<4>(p, pp, delta, fx, fx_shift, mean, spec, gx, gy, gz, s); break;
-    case 8: poisson_n<8>(p, pp, delta, fx, fx_shift, mean, spec, gx, gy, gz, s); break;
-    case 16: poisson_n<16>(p, pp, delta, fx, fx_shift, mean, spec, gx, gy, gz, s); break;
-    case 32: poisson_n<32>(p, pp, delta, fx, fx_shift, mean, spec, gx, gy, gz, s); break;
-    case 64: poisson_n<64>(p, pp, delta, fx, fx_shift, mean, spec, gx, gy, gz, s); break;
-    case 128: poisson_n<128>(p, pp, delta, fx, fx_shift, mean, spec, gx, gy, gz, s); break;
-    case 256: poisson_n<256>(p, pp, delta, fx, fx_shift, mean, spec, gx, gy, gz, s); break;
-    case 512: poisson_n<512>(p, pp, delta, fx, fx_shift, mean, spec, gx, gy, gz, s); break;
+#define CPM_CASE(N) \
+  case N: poisson_n<N>(p, pp, delta, fx, fx_shift, mean, spec, gx, gy, gz, s); break;
+    CPM_FFT_SIZES(CPM_CASE)
+#undef CPM_CASE
     default: break;
   }
 }

@@ -174,7 +174,7 @@ extern "C" int cpm_ics_zeldovich(int n_side, float box_size, const cpm_cosmology
   if (!cosmo || !x3 || !p3) return set_error(nullptr, CPM_E_INVALID, "cpm_ics_zeldovich: null pointer");
   if (!fft_supported(n_side))
     return set_error(nullptr, CPM_E_UNSUPPORTED,
-                     "cpm_ics_zeldovich: n = " + std::to_string(n_side) + " is not a power of two in [4, 1024]");
+                     "cpm_ics_zeldovich: n = " + std::to_string(n_side) + " is not one of " + fft_sizes_text());
   if (!(box_size > 0.0f) || !(a_init > 0.0f) || !(sigma8 > 0.0f))
     return set_error(nullptr, CPM_E_INVALID, "cpm_ics_zeldovich: box, a_init and sigma8 must be > 0");
   int rc = check_device_once(nullptr);

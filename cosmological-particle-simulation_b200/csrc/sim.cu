@@ -143,7 +143,7 @@ static int sim_new(const cpm_sim_params* params, float a0, cpm_sim** out) {
   if (!(P.box_size > 0.0f) || !(a0 > 0.0f)) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_create: box and a0 must be > 0");
   if (!poisson_supported(P.mesh_n))
     return set_error(nullptr, CPM_E_UNSUPPORTED,
-                     "cpm_sim_create: mesh_n = " + std::to_string(P.mesh_n) + " is not a power of two in [4, 512]");
+                     "cpm_sim_create: mesh_n = " + std::to_string(P.mesh_n) + " is not one of " + fft_sizes_text());
   int rc = check_device_once(nullptr);
   if (rc) return rc;
   cpm_sim* s = new cpm_sim();
@@ -212,7 +212,7 @@ int cpm_sim_create_zeldovich(const cpm_sim_params* params, int n_side, float n_s
   if (!params) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_create_zeldovich: params is NULL");
   if (!fft_supported(n_side) || (size_t)n_side * n_side * n_side != params->n_particles)
     return set_error(nullptr, CPM_E_INVALID,
-                     "cpm_sim_create_zeldovich: n_side must be a power of two in [4, 1024] with n_side^3 == n_particles");
+                     std::string("cpm_sim_create_zeldovich: n_side must be one of ") + fft_sizes_text() + " with n_side^3 == n_particles");
   if (!(sigma8 > 0.0f)) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_create_zeldovich: sigma8 must be > 0");
   cpm_sim* s = nullptr;
   int rc = sim_new(params, a0, &s);

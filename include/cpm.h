@@ -37,7 +37,7 @@ extern "C" {
 #define CPM_E_INVALID (-1)       /* null pointer, zero or negative size, bad enum value */
 #define CPM_E_MESH_MISMATCH (-2) /* mesh size differs from the context's (poisson.rs:35) */
 #define CPM_E_CAPACITY (-3)      /* more particles than the context or simulation holds */
-#define CPM_E_UNSUPPORTED (-4)   /* mesh size whose FFT length this build does not support */
+#define CPM_E_UNSUPPORTED (-4)   /* mesh size whose FFT length this build does not compile (cpm_fft_supported) */
 #define CPM_E_CUDA (-5)          /* a CUDA runtime call failed */
 #define CPM_E_NONFINITE (-6)     /* NaN or infinite input position */
 #define CPM_E_NOMEM (-7)         /* device allocation failed */
@@ -105,6 +105,12 @@ int cpm_mesh_interpolate(cpm_ctx* ctx, const float* cells, const float* x3, size
 int cpm_mesh_interpolate3(cpm_ctx* ctx, const float* gx, const float* gy, const float* gz, const float* x3,
                           size_t n, float* out3);
 
+/* No counterpart in the reference (rustfft takes any length). 1 when this build compiles the n-point
+ * transforms every FFT user here needs (cpm_fft3, cpm_poisson_accel, simulations, initial
+ * conditions, power spectra): n in {4, 8, 16, 32, 48, 64, 80, 96, 128, 160, 192, 256, 320, 384, 512,
+ * 1024}; else 0, and those calls return CPM_E_UNSUPPORTED. Host only. */
+int cpm_fft_supported(int n);
+
 /* fft.rs:28-33 `Fft3::forward` / `Fft3::inverse`: unnormalised in-place c2c transform of n^3
  * complex values (forward e^{-ikx}, inverse e^{+ikx}). n must equal the context's mesh size. */
 int cpm_fft3(cpm_ctx* ctx, cpm_cf32* data, int n, int inverse);
@@ -156,8 +162,8 @@ int cpm_ics_zeldovich(int n_side, float box_size, const cpm_cosmology* cosmo, fl
  * x3 on the context's mesh (mesh.rs:29-69; delta = rho/mean - 1 as integrator.rs:117-126).
  * Shell s = 1..n_shells (1 <= n_shells <= 2048) fills k_mean[s-1] (mean of 2 pi |m| / L over its
  * modes), p_mean[s-1] (mean power) and counts[s-1] (modes; 0 leaves k_mean and p_mean 0). The
- * context's mesh must be a power of two in [4, 512]. Sums are FP64; their last bits may vary from
- * run to run (atomic summation order). */
+ * context's mesh must be a supported FFT size (cpm_fft_supported). Sums are FP64; their last bits
+ * may vary from run to run (atomic summation order). */
 int cpm_power_spectrum(cpm_ctx* ctx, const float* x3, size_t n, int n_shells, double* k_mean, double* p_mean,
                        uint64_t* counts);
 

@@ -36,6 +36,13 @@ def test_version_string(native):
     assert native.lib().cpm_version().decode().startswith("cpm ")
 
 
+def test_fft_size_set(native):
+    """Sizes with compiled transforms: powers of two 4..1024 and the listed 2^a 3^b 5^c sizes."""
+    L = native.lib()
+    supported = {n for n in range(1, 2049) if L.cpm_fft_supported(n)}
+    assert supported == {4, 8, 16, 32, 48, 64, 80, 96, 128, 160, 192, 256, 320, 384, 512, 1024}
+
+
 def test_host_wavenumber_bit_exact(native, orc):
     for n in (4, 7, 16, 64, 512):
         for i in range(n):

@@ -109,7 +109,7 @@ def test_interpolate_reference_cases(cpm):
 
 # ------------------------------------------------------------------ FFT / Poisson
 
-@pytest.mark.parametrize("n", [4, 8, 16, 32, 64, 128])
+@pytest.mark.parametrize("n", [4, 8, 16, 32, 48, 64, 80, 96, 128, 160])
 @pytest.mark.parametrize("inverse", [False, True])
 def test_fft3_matches_oracle(cpm, orc, n, inverse):
     rng = np.random.default_rng(n)
@@ -134,7 +134,8 @@ def test_fft3_rejects_mesh_mismatch(cpm):
     del f
 
 
-@pytest.mark.parametrize("n,box,a,r_split", [(16, 1.0, 0.5, 0.0), (32, 64.0, 0.3, 1.25), (64, 64.0, 1.0, 1.25)])
+@pytest.mark.parametrize("n,box,a,r_split", [(16, 1.0, 0.5, 0.0), (32, 64.0, 0.3, 1.25), (64, 64.0, 1.0, 1.25),
+                                             (48, 50.0, 0.7, 1.25), (96, 100.0, 1.0, 1.25)])
 def test_poisson_matches_oracle(cpm, orc, n, box, a, r_split):
     x = orc.scattered_mesh(4 * n ** 3 // 8, box)
     delta = orc.density_contrast(n, box, x)
@@ -159,6 +160,23 @@ def test_plane_wave_force_matches_analytic(cpm):
     amp = c / k0
     assert np.max(np.abs(gx.cells - field(-(c / k0) * np.sin(k0 * xs)))) < 1e-5 * amp
     assert np.max(np.abs(gy.cells)) < 1e-5 * amp and np.max(np.abs(gz.cells)) < 1e-5 * amp
+
+
+def test_plane_wave_force_at_1024(cpm):
+    """poisson.rs:114-139 at n = 1024, where the Green's function runs as its own k-space pass (the
+    fused x pass needs more shared memory than one SM has): a wave along z of wavenumber 3."""
+    n, box, a, m = 1024, 512.0, 1.0, 3
+    cosmo = cpm.Cosmology.lcdm_default()
+    k0 = np.float32(2.0 * np.pi * m / box)
+    c = np.float32(np.float32(1.5) * np.float32(cosmo.omega_m)) / np.float32(a)
+    zs = (np.arange(n, dtype=np.float64) + 0.5) * (box / n)
+    delta = cpm.Mesh(n, box, np.broadcast_to(np.cos(k0 * zs).astype(np.float32), (n * n, n)).ravel().copy())
+    gx, gy, gz = cpm.PoissonSolver(n, box).acceleration(delta, cosmo, a, 0.0)
+    del delta
+    amp = c / k0
+    want = -(c / k0) * np.sin(k0 * zs)
+    assert np.max(np.abs(gx.cells)) < 1e-5 * amp and np.max(np.abs(gy.cells)) < 1e-5 * amp
+    assert np.max(np.abs(gz.cells.reshape(n * n, n) - want.astype(np.float32))) < 1e-5 * amp
 
 
 def test_poisson_mesh_mismatch_raises(cpm):

@@ -82,4 +82,4 @@ def test_power_spectrum_rejects_bad_arguments(cpm):
     with pytest.raises(cpm.CpmError):
         cpm.power_spectrum(np.zeros((0, 3), np.float32), 10.0, 16, 4)
     with pytest.raises(cpm.CpmError):
-        cpm.power_spectrum(x, 10.0, 1024, 4)  # mesh beyond the supported sizes
+        cpm.power_spectrum(x, 10.0, 100, 4)  # no compiled transform for n = 100

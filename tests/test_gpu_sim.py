@@ -59,6 +59,21 @@ def test_pm_step_matches_oracle_bit_for_bit_kick_drift(cpm, orc):
     assert rel_rms(g["acc"], r["acc"]) < 1e-5
 
 
+def test_pm_step_on_a_mixed_radix_mesh(cpm, orc):
+    """PM steps on a 48^3 mesh (radix 2 and 3) with 20^3 particles: force and positions as the oracle."""
+    c, x, p = _ics(orc, 20, 60.0, 0.02, 8)
+    cc = cpm.Cosmology(c.omega_r, c.omega_m, c.omega_l, c.h0)
+    gpu = cpm.Simulation(cc, 60.0, 48, x, p, 0.02, None)
+    ref = orc.Simulation(c, 60.0, 48, x, p, 0.02, None)
+    assert rel_rms(gpu.state()["acc"], ref.state()["acc"]) < 1e-5
+    for a1 in cpm.ln_a_schedule(0.02, 0.04, 2):
+        gpu.step_to(a1)
+        ref.step_to(a1)
+    g, r = gpu.state(), ref.state()
+    assert periodic_max_diff(g["x"], r["x"], 60.0) < 1e-5 * 60.0
+    assert rel_rms(g["acc"], r["acc"]) < 1e-5
+
+
 def test_treepm_accelerations_match_oracle(cpm, orc):
     """TreePM force at the ICs and after 2 steps: within 1e-5 relative RMS (config-1 cosmology)."""
     n, box, mesh = 16, 32.0, 32
@@ -124,7 +139,7 @@ def test_treepm_pair_force_matches_newton(cpm, orc):
     assert abs(acc[0, 0] - newton) / newton < 0.05 and abs(acc[1, 0] + newton) / newton < 0.05
 
 
-@pytest.mark.parametrize("n,box,seed", [(16, 64.0, 42), (32, 128.0, 7)])
+@pytest.mark.parametrize("n,box,seed", [(16, 64.0, 42), (32, 128.0, 7), (48, 96.0, 3)])
 def test_zeldovich_ics_match_oracle(cpm, orc, n, box, seed):
     """ics.rs:78-182 on the GPU vs the oracle: same Philox noise, same f32 scalars; FFT round-off only."""
     c = orc.cosmology(0.0, 0.3, 0.7, 70.0)
