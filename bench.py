@@ -160,13 +160,18 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
         # continue the schedule from a saved state (profiling of a given epoch, e.g. z = 0)
         st0 = np.load(args.load_state)
         a_saved = float(st0["a"])
-        sim = cpm.Simulation(cosmo, box, mesh, st0["x"], st0["p"], a_saved, split, flags=cpm._native.SIM_TIMING)
         full = schedule(wl["steps_total"], wl["steps_total"] + args.warmup + args.steps + 1)
         i0 = int(np.searchsorted(np.asarray(full, np.float32), np.float32(a_saved), side="right"))
         sched = full[i0:i0 + args.warmup + args.steps]
-    else:
-        sim = cpm.Simulation.from_zeldovich(cosmo, box, mesh, n_side, N_S, SIGMA8, A_INIT, wl["seed"] + rank, split,
-                                            flags=cpm._native.SIM_TIMING)
+
+    def make_sim(flags: int):
+        if args.load_state:
+            return cpm.Simulation(cosmo, box, mesh, st0["x"], st0["p"], a_saved, split, flags=flags)
+        return cpm.Simulation.from_zeldovich(cosmo, box, mesh, n_side, N_S, SIGMA8, A_INIT, wl["seed"] + rank, split,
+                                             flags=flags)
+
+    # The timed run replays the step's captured CUDA graphs (no per-phase events).
+    sim = make_sim(0)
     stream = torch.cuda.ExternalStream(sim.stream())
     for a1 in sched[:args.warmup]:
         sim.step_to(a1)
@@ -174,7 +179,6 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         st = sim.state()
         snapshots["start"] = (st["x"], st["p"], st["acc"], sched[args.warmup - 1] if args.warmup else A_INIT)
-    sim.phase_times(reset=True)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -196,8 +200,8 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
         ms = float(t.item())
     else:
         ms = ms_local
-    phases, nsteps = sim.phase_times()
     counters = sim.counters()
+    graphs = sim.graphs()
     if args.save_state and rank == 0:
         st = sim.state()
         np.savez(args.save_state, x=st["x"], p=st["p"], a=np.float32(st["a"]))
@@ -205,10 +209,23 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
         st = sim.state()
         snapshots["end"] = (st["x"], st["p"], st["acc"], sched[-1])
 
+    sim.close()
+
+    # Phase breakdown: the same window again with per-phase CUDA events (uncaptured steps).
+    phases, nsteps = np.zeros(8), 0
+    if not args.no_phases:
+        simp = make_sim(cpm._native.SIM_TIMING)
+        for a1 in sched[:args.warmup]:
+            simp.step_to(a1)
+        simp.phase_times(reset=True)
+        for a1 in sched[args.warmup:]:
+            simp.step_to(a1)
+        phases, nsteps = simp.phase_times()
+        simp.close()
+
     # End to end through the host-buffer C-ABI step, same schedule window, on a fresh simulation.
     e2e = None
     if not args.no_e2e:
-        sim.close()
         sim2 = cpm.Simulation.from_zeldovich(cosmo, box, mesh, n_side, N_S, SIGMA8, A_INIT, wl["seed"] + rank, split)
         for a1 in sched[:args.warmup]:
             sim2.step_to(a1)
@@ -239,8 +256,6 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
         e2e = {"value": n * world * len(e2e_steps) / (ems / 1e3), "unit": "particle-steps/s",
                "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": 24 * n, "steps": len(e2e_steps),
                "api": "cpm_sim_step_host (pinned host x, p in/out each step)"}
-    else:
-        sim.close()
 
     if rank != 0:
         return None
@@ -266,8 +281,10 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
                      "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
                      "peak_kind": peak_kind, "algorithmic_bytes_per_step": pm_b,
                      "traffic": traffic.get("pm_bytes_per_step") if traffic else None},
-        "phase_ms": {k: round(v, 4) for k, v in zip(phase_names, phases)},
+        "phase_ms": {k: round(float(v), 4) for k, v in zip(phase_names, phases)} if nsteps else None,
         "phase_steps": nsteps,
+        "phase_note": "per-phase CUDA events on a second run of the same window (uncaptured steps)",
+        "step_graphs": graphs,
         "tree": {"nodes_last_step": counters["nodes"], "leaf_pairs_last_step": counters["leaf_pairs"],
                  "node_accepts_last_step": counters["node_accepts"],
                  "candidates_last_step": counters["candidates"]},
@@ -367,6 +384,7 @@ def main() -> int:
     ap.add_argument("--e2e-steps", type=int, default=0, help="steps in the end-to-end run (0 = same as --steps)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-phases", action="store_true", help="skip the second, per-phase timed run")
     ap.add_argument("--cpu-walk-fraction", type=float, default=1.0 / 64.0)
     ap.add_argument("--ref-budget-s", type=float, default=120.0)
     ap.add_argument("--save-state", default="", help="write the state after the timed steps (npz: x, p, a)")

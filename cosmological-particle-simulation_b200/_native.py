@@ -114,6 +114,7 @@ def lib() -> C.CDLL:
         "cpm_sim_walk_candidates": (i, [vp, C.POINTER(u64)]),
         "cpm_walk_kernel_fit_error": (i, [fl, fl, i, C.POINTER(C.c_double)]),
         "cpm_sim_stream": (vp, [vp]),
+        "cpm_sim_graphs": (i, [vp]),
         "cpm_sim_destroy": (i, [vp]),
     }
     for name, (res, args) in sig.items():

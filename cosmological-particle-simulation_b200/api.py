@@ -359,6 +359,10 @@ class Simulation:
         return dict(nodes=nn.value, leaf_pairs=lp.value, node_accepts=na.value, launches_per_step=ln.value,
                     candidates=cand.value)
 
+    def graphs(self) -> int:
+        """Captured step graphs: 2 once both sorted-buffer parities replay a graph."""
+        return int(nat.lib().cpm_sim_graphs(self.h))
+
     def stream(self) -> int:
         return nat.lib().cpm_sim_stream(self.h) or 0
 

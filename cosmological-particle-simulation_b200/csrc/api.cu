@@ -132,6 +132,7 @@ int cpm_ctx_destroy(cpm_ctx* c) {
                     &c->x_sorted, &c->keys, &c->vals, &c->acc, &c->acc_sorted, &c->out, &c->mesh_fx, &c->mesh_a,
                     &c->mesh_b, &c->mesh_c, &c->mesh_d, &c->spec, &c->status, &c->tree_counters, &c->pk})
     release(*b);
+  tree_walk_free(c->tree);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return CPM_OK;

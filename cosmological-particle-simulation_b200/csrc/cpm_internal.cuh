@@ -169,6 +169,7 @@ struct PoissonParams {
   float r_split;
   float scale;      // 1 / n^3 (f32)
   int deconvolve;
+  const float* prefactor_dev = nullptr;  // when set, the prefactor is read from device memory
 };
 // Input: either f32 delta (delta != nullptr) or the u64 fixed-point mass mesh (fx != nullptr,
 // converted to delta = c/mean - 1 on load). Output: three f32 meshes. spec: 3 half spectra
@@ -216,6 +217,7 @@ struct TreeNodes {
   DevBuf scan_tmp;
   DevBuf x4;        // float4 copy of the sorted positions for the walk
   size_t capacity = 0;
+  void* walk_fit = nullptr;  // fitted pair-force coefficients of the last split (walk.cu)
 };
 struct TreeCounters {
   unsigned long long leaf_pairs;    // pairs within r_cut summed directly
@@ -229,17 +231,32 @@ cudaError_t tree_build(TreeNodes& t, const uint64_t* sorted_keys, const float* s
                        DevStatus* st, cudaStream_t s);
 // Walks the tree for every sorted particle; acc3 (sorted order) receives g_sr, or g + g_sr
 // when `accumulate` (the reference's g[c] += s[c], integrator.rs:154-158).
+// The coupling k is read from *k_dev when k_dev is set.
 void launch_tree_walk(const TreeNodes& t, const float* sorted_x3, size_t n, float box, const cpm_force_split& split,
-                      float k, float* acc3, int accumulate, TreeCounters* counters, DevStatus* st, cudaStream_t s);
+                      float k, float* acc3, int accumulate, TreeCounters* counters, DevStatus* st, cudaStream_t s,
+                      const float* k_dev = nullptr);
+// Releases the walk's per-tree state (the fitted pair-force coefficients).
+void tree_walk_free(TreeNodes& t);
 
 // ---------------------------------------------------------------------------------------------
 // Particle updates — kdk.cu
 // ---------------------------------------------------------------------------------------------
-// p += g * k (integrator.rs:301-307)
-void launch_kick(float* p3, const float* g3, size_t n, float k, cudaStream_t s);
-// Optional kick with k_prev, then kick with k1, then drift (integrator.rs:301-316).
+// The scalars of one simulation step, kept in device memory and read by its kernels, so that one
+// captured CUDA graph serves every step (a one-thread kernel writes them before each launch).
+struct StepScalars {
+  float k1;         // first half-kick factor, kick_factor(a0, a_mid)
+  float d;          // drift factor, drift_factor(a0, a1)
+  float k2;         // second half-kick factor, kick_factor(a_mid, a1)
+  float prefactor;  // Green's function prefactor 1.5 Omega_m / a1
+  float tree_k;     // short-range coupling K(a1)
+};
+void launch_set_step_scalars(StepScalars* dev, const StepScalars& v, cudaStream_t s);
+// p += g * k (integrator.rs:301-307); k is read from *k_dev when k_dev is set.
+void launch_kick(float* p3, const float* g3, size_t n, float k, cudaStream_t s, const float* k_dev = nullptr);
+// Optional kick with k_prev, then kick with k1, then drift (integrator.rs:301-316); k1 and d are
+// read from *sc when sc is set.
 void launch_kick_kick_drift(float* x3, float* p3, const float* g3, size_t n, float k_prev, int has_prev, float k1,
-                            float d, float box, cudaStream_t s);
+                            float d, float box, cudaStream_t s, const StepScalars* sc = nullptr);
 // Gather permutation: out[i] = in[perm[i]] for AoS triples and for u32 ids.
 void launch_permute3(const float* in3, const uint32_t* perm, size_t n, float* out3, cudaStream_t s);
 void launch_permute_u32(const uint32_t* in, const uint32_t* perm, size_t n, uint32_t* out, cudaStream_t s);

@@ -509,6 +509,7 @@ __global__ void __launch_bounds__(T) k_poisson_x(const float2* __restrict__ spec
         const int valid = min(TW, g.cols - ct * TW);
         const long long base = (long long)iy * g.outer_stride + (long long)ct * TW;
         const int z0 = ct * TW;
+        const float prefactor = pp.prefactor_dev ? *pp.prefactor_dev : pp.prefactor;
         fft_lines<N, false, T>(phi, tw);
         const float ky = wavenumber(iy, N, pp.two_pi_over_l);
         for (int q = threadIdx.x; q < N * TW; q += T) {
@@ -525,7 +526,7 @@ __global__ void __launch_bounds__(T) k_poisson_x(const float2* __restrict__ spec
           } else {
             // phi_k = delta_k * (-prefactor / k^2 * exp(-k^2 r_s^2)), k = 0 skipped (left zero)
             const float filter = expf(__fmul_rn(__fmul_rn(-k2, pp.r_split), pp.r_split));
-            float sc = __fmul_rn(__fdiv_rn(-pp.prefactor, k2), filter);
+            float sc = __fmul_rn(__fdiv_rn(-prefactor, k2), filter);
             if (deconv) sc = __fmul_rn(sc, __fmul_rn(__fmul_rn(deconv[t], deconv[iy]), deconv[z0 + l]));
             v = make_float2(__fmul_rn(v.x, sc), __fmul_rn(v.y, sc));
           }
@@ -561,6 +562,7 @@ __global__ void __launch_bounds__(T) k_poisson_x(const float2* __restrict__ spec
 __global__ void k_green_grad(float2* spec, long long comp, int n, PoissonParams pp, const float* __restrict__ deconv) {
   const int nh = n / 2 + 1, nhp = n / 2 + 2;
   const long long total = (long long)n * n * nh;
+  const float prefactor = pp.prefactor_dev ? *pp.prefactor_dev : pp.prefactor;
   for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
        e += (long long)gridDim.x * blockDim.x) {
     const int kz = (int)(e % nh);
@@ -578,7 +580,7 @@ __global__ void k_green_grad(float2* spec, long long comp, int n, PoissonParams 
       v = make_float2(0.0f, 0.0f);
     } else {
       const float filter = expf(__fmul_rn(__fmul_rn(-k2, pp.r_split), pp.r_split));
-      float sc = __fmul_rn(__fdiv_rn(-pp.prefactor, k2), filter);
+      float sc = __fmul_rn(__fdiv_rn(-prefactor, k2), filter);
       if (deconv) sc = __fmul_rn(sc, __fmul_rn(__fmul_rn(deconv[ix], deconv[iy]), deconv[kz]));
       v = make_float2(__fmul_rn(v.x, sc), __fmul_rn(v.y, sc));
     }

@@ -6,14 +6,21 @@
 
 namespace cpm {
 
-__global__ void k_kick(float* __restrict__ p3, const float* __restrict__ g3, size_t n3, float k) {
+__global__ void k_kick(float* __restrict__ p3, const float* __restrict__ g3, size_t n3, float k,
+                       const float* __restrict__ k_dev) {
+  if (k_dev) k = *k_dev;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += (size_t)gridDim.x * blockDim.x)
     p3[i] = __fadd_rn(p3[i], __fmul_rn(g3[i], k));
 }
 
 // Second half-kick of the previous step (when has_prev), first half-kick of this step, drift.
 __global__ void k_kick_kick_drift(float* __restrict__ x3, float* __restrict__ p3, const float* __restrict__ g3,
-                                  size_t n3, float k_prev, int has_prev, float k1, float d, float box) {
+                                  size_t n3, float k_prev, int has_prev, float k1, float d, float box,
+                                  const StepScalars* __restrict__ sc) {
+  if (sc) {
+    k1 = sc->k1;
+    d = sc->d;
+  }
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += (size_t)gridDim.x * blockDim.x) {
     const float g = g3[i];
     float p = p3[i];
@@ -66,17 +73,24 @@ static unsigned grid_for(size_t work) {
   return (unsigned)(b ? b : 1);
 }
 
-void launch_kick(float* p3, const float* g3, size_t n, float k, cudaStream_t s) {
+__global__ void k_set_step_scalars(StepScalars* dev, StepScalars v) { *dev = v; }
+
+void launch_set_step_scalars(StepScalars* dev, const StepScalars& v, cudaStream_t s) {
+  count_launch();
+  k_set_step_scalars<<<1, 1, 0, s>>>(dev, v);
+}
+
+void launch_kick(float* p3, const float* g3, size_t n, float k, cudaStream_t s, const float* k_dev) {
   if (n == 0) return;
   count_launch();
-  k_kick<<<grid_for(3 * n), 256, 0, s>>>(p3, g3, 3 * n, k);
+  k_kick<<<grid_for(3 * n), 256, 0, s>>>(p3, g3, 3 * n, k, k_dev);
 }
 
 void launch_kick_kick_drift(float* x3, float* p3, const float* g3, size_t n, float k_prev, int has_prev, float k1,
-                            float d, float box, cudaStream_t s) {
+                            float d, float box, cudaStream_t s, const StepScalars* sc) {
   if (n == 0) return;
   count_launch();
-  k_kick_kick_drift<<<grid_for(3 * n), 256, 0, s>>>(x3, p3, g3, 3 * n, k_prev, has_prev, k1, d, box);
+  k_kick_kick_drift<<<grid_for(3 * n), 256, 0, s>>>(x3, p3, g3, 3 * n, k_prev, has_prev, k1, d, box, sc);
 }
 
 void launch_permute3(const float* in3, const uint32_t* perm, size_t n, float* out3, cudaStream_t s) {

@@ -9,6 +9,14 @@
 //   kick(k2)                       (integrator.rs:183-184)
 // Particles are reordered every step; each particle's update is independent of its position in
 // the arrays, so the order only changes f32 summation order inside tree leaves.
+//
+// CUDA graphs. The step's scalars (kick and drift factors, the Green's function prefactor, the
+// tree coupling) live in a device block written by a one-thread kernel before each step, so the
+// kernel sequence of a step is the same every time except for the sorted-buffer swap, which
+// alternates. Each buffer parity gets one graph, captured from the first step of that parity
+// that follows an uncaptured (allocating) one and replayed for every later step of that parity.
+// CPM_SIM_NO_GRAPH launches every kernel directly, and so does CPM_SIM_TIMING, whose per-phase
+// event records are made on the stream between the kernels.
 #include <cstring>
 #include <string>
 #include <vector>
@@ -33,14 +41,21 @@ struct cpm_sim {
   SortScratch sort;
   TreeNodes tree;
   DevBuf x, p, acc, id, x2, p2, id2, keys, vals, fx, gx, gy, gz, spec, status, counters, pk;
-  // Per-step phase events, recorded without host synchronisation into a ring of RING steps and
-  // folded into phase_ms when the ring fills or cpm_sim_phase_times is called.
-  static constexpr int RING = 64;
-  cudaEvent_t ev[RING][N_PHASES] = {};
-  int ring_used = 0;
+  // Per-step phase events, one set per buffer parity. The set of parity q is read back when the
+  // next step of parity q is issued: the step in between is already queued, so the GPU does not
+  // wait for the host.
+  cudaEvent_t ev[2][N_PHASES] = {};
+  bool ev_pending[2] = {false, false};
+  int ev_set = -1;  // set the current step records into (-1: not inside a step)
   double phase_ms[N_PHASES] = {};
   uint64_t timed_steps = 0;
   uint32_t launches = 0;
+  int parity = 0;                     // flips with every force evaluation (the sorted buffers swap)
+  bool warm[2] = {false, false};      // an uncaptured step of this parity has run
+  bool no_graph[2] = {false, false};  // capture failed for this parity: launch directly
+  cudaGraphExec_t graph[2] = {};
+  uint32_t graph_launches[2] = {0, 0};
+  DevBuf stepv;     // StepScalars of the current step
   DevBuf host_tmp;  // caller-order staging of cpm_sim_step_host
 };
 
@@ -70,33 +85,45 @@ static int sim_check(cpm_sim* s) {
 }
 
 static void mark(cpm_sim* s, int phase) {
-  if ((s->P.flags & CPM_SIM_TIMING) && s->ring_used < cpm_sim::RING)
-    cudaEventRecord(s->ev[s->ring_used][phase], s->stream);
+  if ((s->P.flags & CPM_SIM_TIMING) && s->ev_set >= 0) cudaEventRecord(s->ev[s->ev_set][phase], s->stream);
 }
 
-// Folds the recorded steps into phase_ms. Phases: 0 kick+drift, 1 keys+sort+reorder, 2 deposit,
-// 3 FFT-Poisson, 4 gather, 5 tree build, 6 walk + second kick, 7 whole step.
-static int flush_timing(cpm_sim* s) {
-  if (s->ring_used == 0) return CPM_OK;
-  SIM_CU(s, cudaEventSynchronize(s->ev[s->ring_used - 1][7]));
-  for (int r = 0; r < s->ring_used; ++r) {
-    float ms;
-    for (int ph = 0; ph < 6; ++ph) {
-      cudaEventElapsedTime(&ms, s->ev[r][ph], s->ev[r][ph + 1]);
-      s->phase_ms[ph] += ms;
-    }
-    cudaEventElapsedTime(&ms, s->ev[r][6], s->ev[r][7]);
-    s->phase_ms[6] += ms;
-    cudaEventElapsedTime(&ms, s->ev[r][0], s->ev[r][7]);
-    s->phase_ms[7] += ms;
+// Folds the recorded step of event set q into phase_ms. Phases: 0 kick+drift, 1 keys+sort+reorder,
+// 2 deposit, 3 FFT-Poisson, 4 gather, 5 tree build, 6 walk + second kick, 7 whole step.
+static int flush_set(cpm_sim* s, int q) {
+  if (!s->ev_pending[q]) return CPM_OK;
+  SIM_CU(s, cudaEventSynchronize(s->ev[q][7]));
+  float ms;
+  for (int ph = 0; ph < 6; ++ph) {
+    SIM_CU(s, cudaEventElapsedTime(&ms, s->ev[q][ph], s->ev[q][ph + 1]));
+    s->phase_ms[ph] += ms;
   }
-  s->timed_steps += (uint64_t)s->ring_used;
-  s->ring_used = 0;
+  SIM_CU(s, cudaEventElapsedTime(&ms, s->ev[q][6], s->ev[q][7]));
+  s->phase_ms[6] += ms;
+  SIM_CU(s, cudaEventElapsedTime(&ms, s->ev[q][0], s->ev[q][7]));
+  s->phase_ms[7] += ms;
+  s->timed_steps += 1;
+  s->ev_pending[q] = false;
   return CPM_OK;
 }
 
-// Sort into key order, then the force: deposit, FFT-Poisson, gather, tree. Phases 1..6.
-static int sim_accelerations(cpm_sim* s, float a) {
+static int flush_timing(cpm_sim* s) {
+  int rc = flush_set(s, s->parity ^ 1);
+  if (!rc) rc = flush_set(s, s->parity);
+  return rc;
+}
+
+// The swap of the sorted buffers that ends a key sort.
+static void swap_sorted(cpm_sim* s) {
+  std::swap(s->x, s->x2);
+  std::swap(s->p, s->p2);
+  std::swap(s->id, s->id2);
+  s->parity ^= 1;
+}
+
+// Sort into key order, then the force: deposit, FFT-Poisson, gather, tree. Phases 1..6. With
+// `dev`, the Poisson prefactor and the tree coupling are read from the device step block.
+static int sim_accelerations(cpm_sim* s, float a, const StepScalars* dev = nullptr) {
   const size_t n = s->n;
   const int mn = s->P.mesh_n;
   mark(s, 1);
@@ -106,15 +133,14 @@ static int sim_accelerations(cpm_sim* s, float a) {
   launch_permute3(as<float>(s->x), as<uint32_t>(s->vals), n, as<float>(s->x2), s->stream);
   launch_permute3(as<float>(s->p), as<uint32_t>(s->vals), n, as<float>(s->p2), s->stream);
   launch_permute_u32(as<uint32_t>(s->id), as<uint32_t>(s->vals), n, as<uint32_t>(s->id2), s->stream);
-  std::swap(s->x, s->x2);
-  std::swap(s->p, s->p2);
-  std::swap(s->id, s->id2);
+  swap_sorted(s);
   mark(s, 2);
   launch_deposit_fixed(as<float>(s->x), n, 1.0f, mn, s->h, s->shift, as<unsigned long long>(s->fx), s->stream);
   mark(s, 3);
   const float r_split = s->P.use_tree ? s->P.split.r_split : 0.0f;
-  const PoissonParams pp =
+  PoissonParams pp =
       make_poisson_params(mn, s->box, s->P.cosmo.omega_m, a, r_split, (s->P.flags & CPM_SIM_DECONVOLVE) ? 1 : 0);
+  if (dev) pp.prefactor_dev = &dev->prefactor;
   launch_poisson(s->plan, pp, nullptr, as<unsigned long long>(s->fx), s->shift, s->mean, as<float2>(s->spec),
                  as<float>(s->gx), as<float>(s->gy), as<float>(s->gz), s->stream);
   mark(s, 4);
@@ -128,7 +154,8 @@ static int sim_accelerations(cpm_sim* s, float a) {
     SIM_CU(s, cudaMemsetAsync(s->counters.p, 0, sizeof(TreeCounters), s->stream));
     const float k = tree_coupling(s->P.cosmo.omega_m, s->box, a, n);
     launch_tree_walk(s->tree, as<float>(s->x), n, s->box, s->P.split, k, as<float>(s->acc), 1,
-                     as<TreeCounters>(s->counters), as<DevStatus>(s->status), s->stream);
+                     as<TreeCounters>(s->counters), as<DevStatus>(s->status), s->stream,
+                     dev ? &dev->tree_k : nullptr);
   } else {
     mark(s, 6);
   }
@@ -176,6 +203,7 @@ static int sim_new(const cpm_sim_params* params, float a0, cpm_sim** out) {
   ok = ok && ensure(s->spec, 3 * half * sizeof(float2)) == cudaSuccess;
   ok = ok && ensure(s->status, sizeof(DevStatus)) == cudaSuccess;
   ok = ok && ensure(s->counters, sizeof(TreeCounters)) == cudaSuccess;
+  ok = ok && ensure(s->stepv, sizeof(StepScalars)) == cudaSuccess;
   ok = ok && fft_plan_init(s->plan, P.mesh_n) == cudaSuccess;
   if (!ok) {
     s->err = "cpm_sim_create: device allocation failed";
@@ -257,28 +285,79 @@ int cpm_sim_set_state(cpm_sim* s, const float* x3, const float* p3) {
   return sim_check(s);
 }
 
+// One KDK step with the scalars in the device block: phases 0..7.
+static int step_body(cpm_sim* s, float a1) {
+  const StepScalars* dev = as<StepScalars>(s->stepv);
+  mark(s, 0);
+  launch_kick_kick_drift(as<float>(s->x), as<float>(s->p), as<float>(s->acc), s->n, 0.0f, 0, 0.0f, 0.0f, s->box,
+                         s->stream, dev);
+  int rc = sim_accelerations(s, a1, dev);
+  if (rc) return rc;
+  launch_kick(as<float>(s->p), as<float>(s->acc), s->n, 0.0f, s->stream, &dev->k2);
+  mark(s, 7);
+  return CPM_OK;
+}
+
+// Captures step_body into the graph of parity q and launches it. On a capture failure the
+// host-side buffer swap is undone and the step runs uncaptured (and parity q stays uncaptured).
+static int step_captured(cpm_sim* s, int q, float a1) {
+  const unsigned long long l0 = launch_count();
+  cudaError_t e = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal);
+  int rc = e == cudaSuccess ? step_body(s, a1) : CPM_E_CUDA;
+  cudaGraph_t g = nullptr;
+  if (e == cudaSuccess) e = cudaStreamEndCapture(s->stream, &g);
+  if (rc == CPM_OK && e == cudaSuccess && g) e = cudaGraphInstantiate(&s->graph[q], g, 0);
+  if (g) cudaGraphDestroy(g);
+  if (rc != CPM_OK || e != cudaSuccess || !s->graph[q]) {
+    cudaGetLastError();
+    if (s->graph[q]) cudaGraphExecDestroy(s->graph[q]);
+    s->graph[q] = nullptr;
+    s->no_graph[q] = true;
+    if (s->parity != q) swap_sorted(s);
+    return step_body(s, a1);
+  }
+  s->graph_launches[q] = (uint32_t)(launch_count() - l0);
+  SIM_CU(s, cudaGraphLaunch(s->graph[q], s->stream));
+  return CPM_OK;
+}
+
 int cpm_sim_step_to(cpm_sim* s, float a1) {
   if (!s) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_step_to: sim is NULL");
   if (!(a1 > 0.0f) || !std::isfinite(a1)) return set_error(&s->err, CPM_E_INVALID, "cpm_sim_step_to: a1 must be > 0");
   const cpm_cosmology& c = s->P.cosmo;
   const float a0 = s->a;
   const float am = midpoint(c, a0, a1);
-  const float k1 = kick_factor(c, a0, am);
-  const float d = drift_factor(c, a0, a1);
-  const float k2 = kick_factor(c, am, a1);
-  if ((s->P.flags & CPM_SIM_TIMING) && s->ring_used == cpm_sim::RING) {
-    int rc = flush_timing(s);
-    if (rc) return rc;
-  }
+  StepScalars sc;
+  sc.k1 = kick_factor(c, a0, am);
+  sc.d = drift_factor(c, a0, a1);
+  sc.k2 = kick_factor(c, am, a1);
+  sc.prefactor = make_poisson_params(s->P.mesh_n, s->box, c.omega_m, a1, 0.0f, 0).prefactor;
+  sc.tree_k = tree_coupling(c.omega_m, s->box, a1, s->n);
+  const int q = s->parity;
+  int rc;
+  if ((s->P.flags & CPM_SIM_TIMING) && (rc = flush_set(s, q))) return rc;
+  launch_set_step_scalars(as<StepScalars>(s->stepv), sc, s->stream);
   const unsigned long long l0 = launch_count();
-  mark(s, 0);
-  launch_kick_kick_drift(as<float>(s->x), as<float>(s->p), as<float>(s->acc), s->n, 0.0f, 0, k1, d, s->box, s->stream);
-  int rc = sim_accelerations(s, a1);
+  s->ev_set = q;
+  const bool graphs =
+      !(s->P.flags & (CPM_SIM_NO_GRAPH | CPM_SIM_TIMING)) && s->warm[q] && !s->no_graph[q];
+  if (graphs && s->graph[q]) {
+    const cudaError_t e = cudaGraphLaunch(s->graph[q], s->stream);
+    if (e == cudaSuccess) swap_sorted(s);  // the host side of the replayed sort
+    rc = e == cudaSuccess ? CPM_OK
+                          : set_error(&s->err, CPM_E_CUDA, std::string("cudaGraphLaunch: ") + cudaGetErrorString(e));
+    s->launches = 1 + s->graph_launches[q];
+  } else if (graphs) {
+    rc = step_captured(s, q, a1);
+    s->launches = 1 + (s->graph[q] ? s->graph_launches[q] : (uint32_t)(launch_count() - l0));
+  } else {
+    rc = step_body(s, a1);
+    s->warm[q] = true;
+    s->launches = 1 + (uint32_t)(launch_count() - l0);
+  }
+  s->ev_set = -1;
   if (rc) return rc;
-  launch_kick(as<float>(s->p), as<float>(s->acc), s->n, k2, s->stream);
-  mark(s, 7);
-  s->launches = (uint32_t)(launch_count() - l0);
-  if (s->P.flags & CPM_SIM_TIMING) s->ring_used += 1;
+  if (s->P.flags & CPM_SIM_TIMING) s->ev_pending[q] = true;
   s->a = a1;
   return CPM_OK;
 }
@@ -394,6 +473,8 @@ int cpm_sim_counters(cpm_sim* s, uint64_t* nodes, uint64_t* leaf_pairs, uint64_t
 
 void* cpm_sim_stream(cpm_sim* s) { return s ? (void*)s->stream : nullptr; }
 
+int cpm_sim_graphs(cpm_sim* s) { return s ? (s->graph[0] ? 1 : 0) + (s->graph[1] ? 1 : 0) : 0; }
+
 int cpm_sim_destroy(cpm_sim* s) {
   if (!s) return CPM_OK;
   if (s->stream) cudaStreamSynchronize(s->stream);
@@ -403,7 +484,11 @@ int cpm_sim_destroy(cpm_sim* s) {
                     &s->acc, &s->id, &s->x2, &s->p2, &s->id2, &s->keys, &s->vals, &s->fx, &s->gx, &s->gy, &s->gz,
                     &s->spec, &s->status, &s->counters, &s->pk})
     release(*b);
+  tree_walk_free(s->tree);
   release(s->host_tmp);
+  release(s->stepv);
+  for (cudaGraphExec_t& g : s->graph)
+    if (g) cudaGraphExecDestroy(g);
   for (auto& row : s->ev)
     for (auto& e : row)
       if (e) cudaEventDestroy(e);

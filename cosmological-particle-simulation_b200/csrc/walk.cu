@@ -63,7 +63,7 @@ struct PairConst2 {
   float2 c0[FIT_DEG + 1];
   float2 neg_log2e;   // -log2(e)
   float2 eps2;        // softening^2
-  float2 neg_k;       // -K m
+  float2 neg_m;       // -m (the coupling K multiplies the sum at the end)
 };
 
 struct WalkParams {
@@ -225,7 +225,7 @@ __device__ __forceinline__ float2 pair_factor2(float2 r2, const WalkParams& w, c
   }
   const float2 q = __fadd2_rn(r2, c.eps2);
   const float2 rs = make_float2(rsqrt_approx(q.x), rsqrt_approx(q.y));
-  return __fmul2_rn(__fmul2_rn(c.neg_k, S), __fmul2_rn(__fmul2_rn(rs, rs), rs));
+  return __fmul2_rn(__fmul2_rn(c.neg_m, S), __fmul2_rn(__fmul2_rn(rs, rs), rs));
 }
 
 // tree.rs:253-261: d = x - L round(x / L), x = a - b, exact. |x| < 0.49 L gives a zero quotient
@@ -346,7 +346,7 @@ __global__ void __launch_bounds__(WALK_THREADS) k_tree_walk(const uint4* __restr
                                                             const float4* __restrict__ x4, size_t n, WalkParams w,
                                                             const float* __restrict__ far, float* __restrict__ acc3,
                                                             int accumulate, unsigned long long* counters,
-                                                            DevStatus* st) {
+                                                            DevStatus* st, const float* __restrict__ k_dev) {
   __shared__ WalkShared shared[WALK_WARPS];
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -358,7 +358,6 @@ __global__ void __launch_bounds__(WALK_THREADS) k_tree_walk(const uint4* __restr
   const float4 xi = valid ? __ldg(x4 + i) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   const float x0 = xi.x, x1 = xi.y, x2 = xi.z;
   const uint32_t self = (uint32_t)i;
-  const float neg_k = -w.k;
 
   // Bounding box of the warp's particles (centre cg, half extent hg), for a conservative
   // warp-level prune test: a node farther than r_cut + sqrt(3) half from the whole box is pruned
@@ -492,7 +491,7 @@ __global__ void __launch_bounds__(WALK_THREADS) k_tree_walk(const uint4* __restr
       const float4 M = bmass[c];
       float s0 = __fsub_rn(M.x, x0), s1 = __fsub_rn(M.y, x1), s2 = __fsub_rn(M.z, x2);
       min_image3(s0, s1, s2, w);
-      const float f = pair_factor(norm2(s0, s1, s2), neg_k * M.w, w, far);
+      const float f = pair_factor(norm2(s0, s1, s2), -M.w, w, far);
       A0.x = fmaf(-s0, f, A0.x);
       A1.x = fmaf(-s1, f, A1.x);
       A2.x = fmaf(-s2, f, A2.x);
@@ -556,7 +555,9 @@ __global__ void __launch_bounds__(WALK_THREADS) k_tree_walk(const uint4* __restr
     cur ^= 1;
   }
   asm volatile("cp.async.wait_all;\n" ::: "memory");
-  const float a0 = __fadd_rn(A0.x, A0.y), a1 = __fadd_rn(A1.x, A1.y), a2 = __fadd_rn(A2.x, A2.y);
+  // tree.rs:61-66 multiplies every pair by the coupling K; here the unit-coupling sum is scaled once
+  const float kk = k_dev ? *k_dev : w.k;
+  const float a0 = kk * (A0.x + A0.y), a1 = kk * (A1.x + A1.y), a2 = kk * (A2.x + A2.y);
   if (valid) {
     if (accumulate) {
       acc3[3 * i] = __fadd_rn(acc3[3 * i], a0);
@@ -592,6 +593,9 @@ __global__ void k_pack4(const float* __restrict__ x3, size_t n, float4* __restri
 
 // ------------------------------------------------------------------ host launch
 
+// Fitted pair-force coefficients of one tree's last split (refitted when the split changes; a
+// simulation's split is fixed, so its first step uploads them and later steps, captured graphs
+// included, only read them).
 struct FitCache {
   float r_split = -1.0f, r_cut = -1.0f;
   SFit fit{};
@@ -599,15 +603,22 @@ struct FitCache {
   DevBuf far_dev;
 };
 
-static FitCache& fit_cache() {
-  static thread_local FitCache c;
-  return c;
+void tree_walk_free(TreeNodes& t) {
+  FitCache* fc = static_cast<FitCache*>(t.walk_fit);
+  if (fc) {
+    release(fc->far_dev);
+    delete fc;
+  }
+  t.walk_fit = nullptr;
 }
 
 void launch_tree_walk(const TreeNodes& t, const float* sorted_x3, size_t n, float box, const cpm_force_split& split,
-                      float k, float* acc3, int accumulate, TreeCounters* counters, DevStatus* st, cudaStream_t s) {
+                      float k, float* acc3, int accumulate, TreeCounters* counters, DevStatus* st, cudaStream_t s,
+                      const float* k_dev) {
   if (n == 0) return;
-  FitCache& fc = fit_cache();
+  TreeNodes& tm = const_cast<TreeNodes&>(t);
+  if (!tm.walk_fit) tm.walk_fit = new FitCache();
+  FitCache& fc = *static_cast<FitCache*>(tm.walk_fit);
   if (fc.r_split != split.r_split || fc.r_cut != split.r_cut || !fc.far_dev.p) {
     fc.fit = make_fit(split.r_split, split.r_cut, fc.far);
     if (ensure(fc.far_dev, fc.far.size() * sizeof(float)) != cudaSuccess) return;
@@ -615,7 +626,6 @@ void launch_tree_walk(const TreeNodes& t, const float* sorted_x3, size_t n, floa
     fc.r_split = split.r_split;
     fc.r_cut = split.r_cut;
   }
-  TreeNodes& tm = const_cast<TreeNodes&>(t);
   if (ensure(tm.x4, n * sizeof(float4)) != cudaSuccess) return;
   const unsigned pb = (unsigned)std::min<size_t>((n + 255) / 256, 148 * 16);
   count_launch();
@@ -639,14 +649,14 @@ void launch_tree_walk(const TreeNodes& t, const float* sorted_x3, size_t n, floa
   for (int j = 0; j <= FIT_DEG; ++j) w.p2.c0[j] = dup(fc.fit.c0[j]);
   w.p2.neg_log2e = dup(-1.44269504f);
   w.p2.eps2 = dup(w.eps2);
-  w.p2.neg_k = dup(-k);
+  w.p2.neg_m = dup(-1.0f);
   const size_t groups = (n + 31) / 32;
   const unsigned blocks = (unsigned)((groups + WALK_WARPS - 1) / WALK_WARPS);
   count_launch();
   k_tree_walk<<<blocks, WALK_THREADS, 0, s>>>(static_cast<const uint4*>(t.link.p), static_cast<const float4*>(t.geo.p),
                                               static_cast<const float4*>(t.mass.p), as<float4>(tm.x4), n, w,
                                               static_cast<const float*>(fc.far_dev.p), acc3, accumulate,
-                                              reinterpret_cast<unsigned long long*>(counters), st);
+                                              reinterpret_cast<unsigned long long*>(counters), st, k_dev);
 }
 
 }  // namespace cpm

@@ -170,7 +170,7 @@ int cpm_power_spectrum(cpm_ctx* ctx, const float* x3, size_t n, int n_shells, do
 /* ------------------------------------------------------------------ device-resident simulation */
 /* Replaces `Simulation` (integrator.rs:34-186) under a `cuda` feature: state stays in HBM and
  * `step_to` runs one KDK step (kick, drift, deposit, FFT-Poisson, gather, tree build and walk,
- * kick) as one CUDA graph. */
+ * kick) as one CUDA graph (see CPM_SIM_NO_GRAPH). */
 typedef struct {
   cpm_cosmology cosmo;
   float box_size;
@@ -186,9 +186,13 @@ typedef struct {
 #define CPM_SIM_FIXED_POINT 0x1u
 /* Divide the PM Green's function by the CIC window squared (the reference does not). */
 #define CPM_SIM_DECONVOLVE 0x2u
-/* Record per-phase CUDA-event timings for cpm_sim_phase_times(). */
+/* Record per-phase CUDA-event timings for cpm_sim_phase_times(). The step then runs uncaptured
+ * (as under CPM_SIM_NO_GRAPH), with the event records between its kernels. */
 #define CPM_SIM_TIMING 0x4u
-/* Run the step without CUDA-graph capture (each kernel launched directly). */
+/* Run the step without CUDA-graph capture (each kernel launched directly). By default the first
+ * two steps run uncaptured (they allocate the sort and tree buffers) and each later step replays
+ * one of two captured graphs (the sorted particle buffers alternate between them); CPM_SIM_TIMING
+ * also runs every step uncaptured. */
 #define CPM_SIM_NO_GRAPH 0x8u
 
 /* integrator.rs:54-79 `Simulation::new`: uploads x3, p3 (AoS [n][3]) and computes the initial
@@ -211,6 +215,10 @@ int cpm_sim_step_to(cpm_sim* sim, float a1);
 int cpm_sim_step_host(cpm_sim* sim, float a1, float* x3, float* p3);
 /* Reads the state in the caller's particle order. Any pointer may be NULL. delta is n^3. */
 int cpm_sim_get_state(cpm_sim* sim, float* x3, float* p3, float* acc3, float* delta, float* a);
+/* Number of captured step graphs (0 before the third step, under CPM_SIM_NO_GRAPH or
+ * CPM_SIM_TIMING, or when capture failed and the steps run uncaptured; 2 once both buffer
+ * parities are captured). */
+int cpm_sim_graphs(cpm_sim* sim);
 /* cpm_power_spectrum of the simulation's current particles on its mesh, without copying them. */
 int cpm_sim_power_spectrum(cpm_sim* sim, int n_shells, double* k_mean, double* p_mean, uint64_t* counts);
 /* Overwrites positions and momenta (caller's order) and recomputes the acceleration at the current a. */

@@ -176,14 +176,34 @@ def test_step_host_equals_step_to(cpm):
     assert np.array_equal(sa["x"], xh) and np.array_equal(sa["p"], ph)
 
 
+def test_graph_replay_equals_direct_launches(cpm):
+    """Steps replayed from the captured CUDA graphs give bit-identical states to steps launched
+    kernel by kernel (CPM_SIM_NO_GRAPH); both parities get a graph after four steps."""
+    cc = cpm.Cosmology(0.0, 0.3, 0.7, 70.0)
+    split = cpm.ForceSplit.with_(32.0, 32, 16, 1.0 / 30.0, 0.5)
+    g = cpm.Simulation.from_zeldovich(cc, 32.0, 32, 16, 0.96, 0.8, 0.02, 4, split)
+    d = cpm.Simulation.from_zeldovich(cc, 32.0, 32, 16, 0.96, 0.8, 0.02, 4, split, flags=cpm._native.SIM_NO_GRAPH)
+    for i, a1 in enumerate(cpm.ln_a_schedule(0.02, 0.5, 8)):
+        g.step_to(a1)
+        d.step_to(a1)
+        if i == 1:
+            assert g.graphs() == 0  # the first step of each parity runs uncaptured
+    assert g.graphs() == 2 and d.graphs() == 0
+    sg, sd = g.state(), d.state()
+    for key in ("x", "p", "acc"):
+        assert np.array_equal(sg[key], sd[key]), key
+    assert g.counters()["leaf_pairs"] == d.counters()["leaf_pairs"]
+
+
 def test_phase_timing_and_counters(cpm):
     cc = cpm.Cosmology(0.0, 0.3, 0.7, 70.0)
     split = cpm.ForceSplit.with_(32.0, 32, 16, 1.0 / 30.0, 0.5)
     s = cpm.Simulation.from_zeldovich(cc, 32.0, 32, 16, 0.96, 0.8, 0.02, 9, split, flags=cpm._native.SIM_TIMING)
-    for a1 in cpm.ln_a_schedule(0.02, 0.3, 6)[:4]:
+    for a1 in cpm.ln_a_schedule(0.02, 0.3, 6):
         s.step_to(a1)
     ms, steps = s.phase_times()
-    assert steps == 4 and np.all(ms >= 0) and ms[7] > 0
+    assert s.graphs() == 0  # phase timing records events between kernels: no capture
+    assert steps == 6 and np.all(ms >= 0) and ms[7] > 0
     assert abs(ms[:7].sum() - ms[7]) < 0.05 * ms[7] + 1e-3
     c = s.counters()
     assert c["nodes"] > 0 and c["leaf_pairs"] > 0 and c["launches_per_step"] > 10
