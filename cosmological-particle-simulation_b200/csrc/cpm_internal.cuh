@@ -257,6 +257,13 @@ void launch_kick(float* p3, const float* g3, size_t n, float k, cudaStream_t s, 
 // read from *sc when sc is set.
 void launch_kick_kick_drift(float* x3, float* p3, const float* g3, size_t n, float k_prev, int has_prev, float k1,
                             float d, float box, cudaStream_t s, const StepScalars* sc = nullptr);
+// Fixed-point positions x = q L / 2^32 (q uint32 per component). The first half-kick as
+// launch_kick_kick_drift, then the drift q += round(p d 2^32 / L) (FP64 product, wrapping modulo
+// 2^32, so the periodic wrap is exact for displacements below L/2), and x3 = f32 of the new q.
+void launch_kick_drift_fixed(uint32_t* q3, float* x3, float* p3, const float* g3, size_t n, float box,
+                             cudaStream_t s, const StepScalars* sc);
+// q3 = round(x3 2^32 / L) modulo 2^32, and x3 rewritten as the f32 of q3.
+void launch_to_fixed(float* x3, uint32_t* q3, size_t n, float box, cudaStream_t s);
 // Gather permutation: out[i] = in[perm[i]] for AoS triples and for u32 ids.
 void launch_permute3(const float* in3, const uint32_t* perm, size_t n, float* out3, cudaStream_t s);
 void launch_permute_u32(const uint32_t* in, const uint32_t* perm, size_t n, uint32_t* out, cudaStream_t s);

@@ -31,6 +31,33 @@ __global__ void k_kick_kick_drift(float* __restrict__ x3, float* __restrict__ p3
   }
 }
 
+__device__ __forceinline__ float fixed_to_x(uint32_t q, double unit) { return (float)((double)q * unit); }
+
+__global__ void k_kick_drift_fixed(uint32_t* __restrict__ q3, float* __restrict__ x3, float* __restrict__ p3,
+                                   const float* __restrict__ g3, size_t n3, float box,
+                                   const StepScalars* __restrict__ sc) {
+  const float k1 = sc->k1, d = sc->d;
+  const double per_length = 4294967296.0 / (double)box, unit = (double)box / 4294967296.0;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += (size_t)gridDim.x * blockDim.x) {
+    const float p = __fadd_rn(p3[i], __fmul_rn(g3[i], k1));
+    p3[i] = p;
+    const long long dq = __double2ll_rn((double)p * (double)d * per_length);
+    const uint32_t q = q3[i] + (uint32_t)(unsigned long long)dq;  // modulo 2^32: the periodic wrap
+    q3[i] = q;
+    x3[i] = fixed_to_x(q, unit);
+  }
+}
+
+__global__ void k_to_fixed(float* __restrict__ x3, uint32_t* __restrict__ q3, size_t n3, float box) {
+  const double per_length = 4294967296.0 / (double)box, unit = (double)box / 4294967296.0;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += (size_t)gridDim.x * blockDim.x) {
+    const long long qq = __double2ll_rn((double)x3[i] * per_length);
+    const uint32_t q = (uint32_t)(unsigned long long)qq;
+    q3[i] = q;
+    x3[i] = fixed_to_x(q, unit);
+  }
+}
+
 __global__ void k_permute3(const float* __restrict__ in3, const uint32_t* __restrict__ perm, size_t n,
                            float* __restrict__ out3) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -91,6 +118,19 @@ void launch_kick_kick_drift(float* x3, float* p3, const float* g3, size_t n, flo
   if (n == 0) return;
   count_launch();
   k_kick_kick_drift<<<grid_for(3 * n), 256, 0, s>>>(x3, p3, g3, 3 * n, k_prev, has_prev, k1, d, box, sc);
+}
+
+void launch_kick_drift_fixed(uint32_t* q3, float* x3, float* p3, const float* g3, size_t n, float box,
+                             cudaStream_t s, const StepScalars* sc) {
+  if (n == 0) return;
+  count_launch();
+  k_kick_drift_fixed<<<grid_for(3 * n), 256, 0, s>>>(q3, x3, p3, g3, 3 * n, box, sc);
+}
+
+void launch_to_fixed(float* x3, uint32_t* q3, size_t n, float box, cudaStream_t s) {
+  if (n == 0) return;
+  count_launch();
+  k_to_fixed<<<grid_for(3 * n), 256, 0, s>>>(x3, q3, 3 * n, box);
 }
 
 void launch_permute3(const float* in3, const uint32_t* perm, size_t n, float* out3, cudaStream_t s) {

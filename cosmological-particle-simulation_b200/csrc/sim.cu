@@ -17,6 +17,11 @@
 // that follows an uncaptured (allocating) one and replayed for every later step of that parity.
 // CPM_SIM_NO_GRAPH launches every kernel directly, and so does CPM_SIM_TIMING, whose per-phase
 // event records are made on the stream between the kernels.
+//
+// CPM_SIM_FIXED_POINT keeps the master positions as uint32 fixed point q (x = q L / 2^32) in key
+// order beside x: the drift adds round(p d 2^32 / L) to q, so the periodic wrap is exact and the
+// resolution is L / 2^32 everywhere in the box; x (f32, what every force kernel reads) is
+// rewritten from q after each drift. Positions given by the caller are rounded to the grid.
 #include <cstring>
 #include <string>
 #include <vector>
@@ -56,6 +61,7 @@ struct cpm_sim {
   cudaGraphExec_t graph[2] = {};
   uint32_t graph_launches[2] = {0, 0};
   DevBuf stepv;     // StepScalars of the current step
+  DevBuf q, q2;     // fixed-point positions (CPM_SIM_FIXED_POINT) and their sort scratch
   DevBuf host_tmp;  // caller-order staging of cpm_sim_step_host
 };
 
@@ -118,8 +124,11 @@ static void swap_sorted(cpm_sim* s) {
   std::swap(s->x, s->x2);
   std::swap(s->p, s->p2);
   std::swap(s->id, s->id2);
+  std::swap(s->q, s->q2);
   s->parity ^= 1;
 }
+
+static bool fixed_point(const cpm_sim* s) { return (s->P.flags & CPM_SIM_FIXED_POINT) != 0; }
 
 // Sort into key order, then the force: deposit, FFT-Poisson, gather, tree. Phases 1..6. With
 // `dev`, the Poisson prefactor and the tree coupling are read from the device step block.
@@ -133,6 +142,8 @@ static int sim_accelerations(cpm_sim* s, float a, const StepScalars* dev = nullp
   launch_permute3(as<float>(s->x), as<uint32_t>(s->vals), n, as<float>(s->x2), s->stream);
   launch_permute3(as<float>(s->p), as<uint32_t>(s->vals), n, as<float>(s->p2), s->stream);
   launch_permute_u32(as<uint32_t>(s->id), as<uint32_t>(s->vals), n, as<uint32_t>(s->id2), s->stream);
+  if (fixed_point(s))  // the 32-bit words of q move like those of x
+    launch_permute3(as<float>(s->q), as<uint32_t>(s->vals), n, as<float>(s->q2), s->stream);
   swap_sorted(s);
   mark(s, 2);
   launch_deposit_fixed(as<float>(s->x), n, 1.0f, mn, s->h, s->shift, as<unsigned long long>(s->fx), s->stream);
@@ -204,6 +215,8 @@ static int sim_new(const cpm_sim_params* params, float a0, cpm_sim** out) {
   ok = ok && ensure(s->status, sizeof(DevStatus)) == cudaSuccess;
   ok = ok && ensure(s->counters, sizeof(TreeCounters)) == cudaSuccess;
   ok = ok && ensure(s->stepv, sizeof(StepScalars)) == cudaSuccess;
+  if (P.flags & CPM_SIM_FIXED_POINT)
+    for (DevBuf* b : {&s->q, &s->q2}) ok = ok && ensure(*b, 3 * n * sizeof(uint32_t)) == cudaSuccess;
   ok = ok && fft_plan_init(s->plan, P.mesh_n) == cudaSuccess;
   if (!ok) {
     s->err = "cpm_sim_create: device allocation failed";
@@ -260,6 +273,7 @@ int cpm_sim_create_zeldovich(const cpm_sim_params* params, int n_side, float n_s
     return e == cudaErrorMemoryAllocation ? CPM_E_NOMEM : CPM_E_CUDA;
   }
   launch_iota(as<uint32_t>(s->id), s->n, s->stream);
+  if (fixed_point(s)) launch_to_fixed(as<float>(s->x), as<uint32_t>(s->q), s->n, s->box, s->stream);
   rc = sim_accelerations(s, s->a);
   if (rc == CPM_OK) rc = sim_check(s);
   if (rc) {
@@ -280,6 +294,7 @@ int cpm_sim_set_state(cpm_sim* s, const float* x3, const float* p3) {
   for (size_t i = 0; i < n; ++i) iota[i] = (uint32_t)i;
   SIM_CU(s, cudaMemcpyAsync(s->id.p, iota.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
   launch_check_finite(as<float>(s->x), n, as<DevStatus>(s->status), s->stream);
+  if (fixed_point(s)) launch_to_fixed(as<float>(s->x), as<uint32_t>(s->q), n, s->box, s->stream);
   int rc = sim_accelerations(s, s->a);
   if (rc) return rc;
   return sim_check(s);
@@ -289,8 +304,12 @@ int cpm_sim_set_state(cpm_sim* s, const float* x3, const float* p3) {
 static int step_body(cpm_sim* s, float a1) {
   const StepScalars* dev = as<StepScalars>(s->stepv);
   mark(s, 0);
-  launch_kick_kick_drift(as<float>(s->x), as<float>(s->p), as<float>(s->acc), s->n, 0.0f, 0, 0.0f, 0.0f, s->box,
-                         s->stream, dev);
+  if (fixed_point(s))
+    launch_kick_drift_fixed(as<uint32_t>(s->q), as<float>(s->x), as<float>(s->p), as<float>(s->acc), s->n, s->box,
+                            s->stream, dev);
+  else
+    launch_kick_kick_drift(as<float>(s->x), as<float>(s->p), as<float>(s->acc), s->n, 0.0f, 0, 0.0f, 0.0f, s->box,
+                           s->stream, dev);
   int rc = sim_accelerations(s, a1, dev);
   if (rc) return rc;
   launch_kick(as<float>(s->p), as<float>(s->acc), s->n, 0.0f, s->stream, &dev->k2);
@@ -382,6 +401,7 @@ static int download_caller_order(cpm_sim* s, const float* src3, float* host3) {
 int cpm_sim_step_host(cpm_sim* s, float a1, float* x3, float* p3) {
   if (!s || !x3 || !p3) return set_error(s ? &s->err : nullptr, CPM_E_INVALID, "cpm_sim_step_host: null pointer");
   int rc = upload_caller_order(s, x3, as<float>(s->x));
+  if (!rc && fixed_point(s)) launch_to_fixed(as<float>(s->x), as<uint32_t>(s->q), s->n, s->box, s->stream);
   if (!rc) rc = upload_caller_order(s, p3, as<float>(s->p));
   if (!rc) rc = cpm_sim_step_to(s, a1);
   if (!rc) rc = download_caller_order(s, as<float>(s->x), x3);
@@ -482,7 +502,7 @@ int cpm_sim_destroy(cpm_sim* s) {
   for (DevBuf* b : {&s->sort.keys_alt, &s->sort.vals_alt, &s->sort.block_hist, &s->sort.scan_tmp, &s->tree.geo,
                     &s->tree.mass, &s->tree.link, &s->tree.counters, &s->tree.prefix, &s->tree.scan_tmp, &s->tree.x4, &s->x, &s->p,
                     &s->acc, &s->id, &s->x2, &s->p2, &s->id2, &s->keys, &s->vals, &s->fx, &s->gx, &s->gy, &s->gz,
-                    &s->spec, &s->status, &s->counters, &s->pk})
+                    &s->spec, &s->status, &s->counters, &s->pk, &s->q, &s->q2})
     release(*b);
   tree_walk_free(s->tree);
   release(s->host_tmp);

@@ -181,8 +181,11 @@ typedef struct {
   uint32_t flags;         /* CPM_SIM_* below */
 } cpm_sim_params;
 
-/* Positions as uint32 fixed point (x = q L / 2^32) so the periodic wrap of the drift is exact.
- * Precision mode; the default f32 mode is the reference's arithmetic. */
+/* Positions as uint32 fixed point (x = q L / 2^32): the drift adds round(p d 2^32 / L) (FP64
+ * product) modulo 2^32, so the periodic wrap is exact and the resolution is L / 2^32 anywhere in
+ * the box (displacements per step must stay below L/2). Positions given by the caller are rounded
+ * to that grid; the force kernels read the f32 value of q. Precision mode; the default f32 mode is
+ * the reference's arithmetic (integrator.rs:309-316). */
 #define CPM_SIM_FIXED_POINT 0x1u
 /* Divide the PM Green's function by the CIC window squared (the reference does not). */
 #define CPM_SIM_DECONVOLVE 0x2u

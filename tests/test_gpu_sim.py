@@ -195,6 +195,48 @@ def test_graph_replay_equals_direct_launches(cpm):
     assert g.counters()["leaf_pairs"] == d.counters()["leaf_pairs"]
 
 
+def test_fixed_point_mode_tracks_f32_mode(cpm):
+    """CPM_SIM_FIXED_POINT (uint32 positions) follows the f32 trajectory from the same ICs."""
+    cc = cpm.Cosmology(0.0, 0.3, 0.7, 70.0)
+    split = cpm.ForceSplit.with_(32.0, 32, 16, 1.0 / 30.0, 0.5)
+    f = cpm.Simulation.from_zeldovich(cc, 32.0, 32, 16, 0.96, 0.8, 0.02, 5, split)
+    q = cpm.Simulation.from_zeldovich(cc, 32.0, 32, 16, 0.96, 0.8, 0.02, 5, split, flags=cpm._native.SIM_FIXED_POINT)
+    for a1 in cpm.ln_a_schedule(0.02, 0.3, 6):
+        f.step_to(a1)
+        q.step_to(a1)
+    sf, sq = f.state(), q.state()
+    assert periodic_max_diff(sq["x"], sf["x"], 32.0) < 1e-4 * 32.0
+    assert rel_rms(sq["p"], sf["p"]) < 1e-3
+    assert sq["x"].min() >= 0.0 and sq["x"].max() <= 32.0
+
+
+def test_fixed_point_drift_wraps_exactly(cpm, orc):
+    """A force-free lattice streaming across the periodic boundary several times ends where the
+    summed drift factors put it, to f32 resolution (the uint32 wrap loses nothing)."""
+    box = 32.0
+    c = orc.cosmology(0.0, 0.3, 0.7, 70.0)
+    cc = cpm.Cosmology(c.omega_r, c.omega_m, c.omega_l, c.h0)
+    g = np.array([4.0, 20.0], np.float32)
+    x0 = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3).astype(np.float32)
+    sched = cpm.ln_a_schedule(0.5, 1.0, 5)
+    a_prev, dsum = 0.5, 0.0
+    for a1 in sched:
+        dsum += orc.drift_factor(c, a_prev, a1)
+        a_prev = a1
+    v = np.float32(3.3 * box / dsum)  # 3.3 box lengths along x over the run
+    p0 = np.zeros_like(x0)
+    p0[:, 0] = v
+    split = cpm.ForceSplit.with_(box, 32, 2, 1.0 / 30.0, 0.5)
+    sim = cpm.Simulation(cc, box, 32, x0, p0, 0.5, split, flags=cpm._native.SIM_FIXED_POINT)
+    for a1 in sched:
+        sim.step_to(a1)
+    st = sim.state()
+    assert np.max(np.abs(st["p"] - p0)) < 1e-5 * v  # the lattice feels no net force
+    want = np.mod(x0[:, 0].astype(np.float64) + float(v) * dsum, box)
+    assert periodic_max_diff(st["x"][:, 0], want, box) < 2e-5 * box
+    assert np.max(np.abs(st["x"][:, 1:] - x0[:, 1:])) < 1e-5
+
+
 def test_phase_timing_and_counters(cpm):
     cc = cpm.Cosmology(0.0, 0.3, 0.7, 70.0)
     split = cpm.ForceSplit.with_(32.0, 32, 16, 1.0 / 30.0, 0.5)
