@@ -115,6 +115,8 @@ def lib() -> C.CDLL:
         "cpm_walk_kernel_fit_error": (i, [fl, fl, i, C.POINTER(C.c_double)]),
         "cpm_sim_stream": (vp, [vp]),
         "cpm_sim_graphs": (i, [vp]),
+        "cpm_sim_snapshot": (i, [vp, vp, vp, vp, vp, C.POINTER(i), C.POINTER(fl)]),
+        "cpm_density_grid": (i, [vp, vp, i, vp, C.POINTER(i)]),
         "cpm_sim_destroy": (i, [vp]),
     }
     for name, (res, args) in sig.items():

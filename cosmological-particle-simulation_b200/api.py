@@ -219,6 +219,17 @@ def power_spectrum(positions, box_size: float, mesh_n: int, n_shells: int) -> tu
     return k, p, cnt
 
 
+def density_grid(delta: "Mesh") -> np.ndarray:
+    """frame.rs:30-55 `downsample_grid`: the (m, m, m) texture, index [z, y, x], of 1 + block means."""
+    n = delta.n
+    gm = n // max(1, -(-n // 128))
+    out = np.empty(gm ** 3, np.float32)
+    side = C.c_int()
+    c = _ctx(n, delta.box_size)
+    c._check(nat.lib().cpm_density_grid(c.h, ptr(f32c(delta.cells)), int(n), ptr(out), C.byref(side)))
+    return out.reshape(side.value, side.value, side.value)
+
+
 def ln_a_schedule(a_start: float, a_end: float, steps: int) -> list[float]:
     """runner.rs:240 / integrator.rs:168: a_i = a0 (a_end / a0)^(i / steps) in f32, i = 1..steps."""
     a0 = np.float32(a_start)
@@ -358,6 +369,24 @@ class Simulation:
         check(nat.lib().cpm_sim_walk_candidates(self.h, C.byref(cand)), sim=True)
         return dict(nodes=nn.value, leaf_pairs=lp.value, node_accepts=na.value, launches_per_step=ln.value,
                     candidates=cand.value)
+
+    def snapshot(self, want_grid: bool = False) -> dict:
+        """runner.rs:263-284 `snapshot`: redshift, positions, speeds, densities, rsd shifts, the
+        optional density grid and the max speed, with the reductions done on the device."""
+        n = self.n
+        speeds = np.empty(n, np.float32)
+        dens = np.empty(n, np.float32)
+        rsd = np.empty((n, 3), np.float32)
+        gside = C.c_int()
+        gm = self.mesh_n // max(1, -(-self.mesh_n // 128))
+        grid = np.empty(gm ** 3, np.float32) if want_grid else None
+        vmax = C.c_float()
+        check(nat.lib().cpm_sim_snapshot(self.h, ptr(speeds), ptr(dens), ptr(rsd), ptr(grid), C.byref(gside),
+                                         C.byref(vmax)), sim=True)
+        st = self.state()
+        return dict(redshift=np.float32(1.0) / np.float32(st["a"]) - np.float32(1.0), positions=st["x"], speeds=speeds, densities=dens,
+                    rsd=rsd, grid=grid.reshape(gside.value, gside.value, gside.value) if want_grid else None,
+                    max_speed=vmax.value)
 
     def graphs(self) -> int:
         """Captured step graphs: 2 once both sorted-buffer parities replay a graph."""

@@ -211,6 +211,25 @@ static int deposit_common(cpm_ctx* c, const float* x3, size_t n, float mass, int
 
 int cpm_fft_supported(int n) { return fft_supported(n) ? 1 : 0; }
 
+int cpm_density_grid(cpm_ctx* c, const float* delta, int n, float* grid, int* grid_n) {
+  if (!c) return set_error(nullptr, CPM_E_INVALID, "context is NULL");
+  if (!delta || !grid) return set_error(&c->err, CPM_E_INVALID, "density_grid: null pointer");
+  if (n != c->n_mesh) return set_error(&c->err, CPM_E_MESH_MISMATCH, "density_grid: n differs from the context's mesh");
+  int rc = reset_status(c);
+  if (rc) return rc;
+  const size_t m3 = (size_t)n * n * n;
+  const int gm = density_grid_side(n);
+  const size_t gm3 = (size_t)gm * gm * gm;
+  CPM_CU(c, ensure(c->mesh_a, m3 * sizeof(float)));
+  CPM_CU(c, ensure(c->mesh_b, gm3 * sizeof(float)));
+  CPM_CU(c, cudaMemcpyAsync(c->mesh_a.p, delta, m3 * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  launch_downsample_grid(as<float>(c->mesh_a), n, as<float>(c->mesh_b), c->stream);
+  CPM_CU(c, cudaMemcpyAsync(grid, c->mesh_b.p, gm3 * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  if ((rc = sync_and_check(c))) return rc;
+  if (grid_n) *grid_n = gm;
+  return CPM_OK;
+}
+
 int cpm_power_spectrum(cpm_ctx* c, const float* x3, size_t n, int n_shells, double* k_mean, double* p_mean,
                        uint64_t* counts) {
   if (!c) return set_error(nullptr, CPM_E_INVALID, "context is NULL");

@@ -275,6 +275,20 @@ void launch_check_finite(const float* x3, size_t n, DevStatus* st, cudaStream_t 
 void launch_iota(uint32_t* id, size_t n, cudaStream_t s);
 
 // ---------------------------------------------------------------------------------------------
+// Viewer snapshot — snapshot.cu (runner.rs:263-284, frame.rs)
+// ---------------------------------------------------------------------------------------------
+constexpr int DENSITY_GRID_MAX = 128;  // frame.rs:27 MAX_GRID
+// Side m = n / ceil(n / 128) of the downsampled density grid of an n^3 mesh.
+int density_grid_side(int n);
+// Key-order p3 and interpolated delta in, caller-order outputs through id (any may be null);
+// max_speed_bits (zeroed by the caller) receives the bits of the largest speed.
+void launch_snapshot_particles(const float* p3, const float* dens_in, const uint32_t* id, size_t n, float a,
+                               float rsd_scale, float* speeds, float* dens, float* rsd3, unsigned int* max_speed_bits,
+                               cudaStream_t s);
+// frame.rs:30-55: 1 + block means of delta, x fastest, density_grid_side(n)^3 values.
+void launch_downsample_grid(const float* delta, int n, float* out, cudaStream_t s);
+
+// ---------------------------------------------------------------------------------------------
 // Initial conditions — ics.cu
 // ---------------------------------------------------------------------------------------------
 // Zel'dovich positions and momenta (AoS f32, lattice order (ix*n + iy)*n + iz) into device memory.

@@ -62,6 +62,7 @@ struct cpm_sim {
   uint32_t graph_launches[2] = {0, 0};
   DevBuf stepv;     // StepScalars of the current step
   DevBuf q, q2;     // fixed-point positions (CPM_SIM_FIXED_POINT) and their sort scratch
+  DevBuf snap;      // device outputs of cpm_sim_snapshot
   DevBuf host_tmp;  // caller-order staging of cpm_sim_step_host
 };
 
@@ -449,6 +450,42 @@ int cpm_sim_power_spectrum(cpm_sim* s, int n_shells, double* k_mean, double* p_m
   return CPM_OK;
 }
 
+int cpm_sim_snapshot(cpm_sim* s, float* speeds, float* densities, float* rsd3, float* grid, int* grid_n,
+                     float* max_speed) {
+  if (!s) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_snapshot: sim is NULL");
+  const size_t n = s->n;
+  const int mn = s->P.mesh_n;
+  const size_t m3 = (size_t)mn * mn * mn;
+  const int gm = density_grid_side(mn);
+  const size_t gm3 = (size_t)gm * gm * gm;
+  SIM_CU(s, ensure(s->snap, (5 * n + gm3 + 1) * sizeof(float)));
+  float* base = as<float>(s->snap);
+  float *d_speeds = base, *d_dens = base + n, *d_rsd = base + 2 * n, *d_grid = base + 5 * n;
+  unsigned int* d_max = reinterpret_cast<unsigned int*>(base + 5 * n + gm3);
+  if (densities || grid)  // delta of the last force evaluation (integrator.rs:117-126)
+    launch_fixed_to_f32(as<unsigned long long>(s->fx), m3, s->shift, 1, s->mean, as<float>(s->gx), s->stream);
+  if (densities) launch_interpolate(as<float>(s->gx), as<float>(s->x), n, mn, s->h, as<float>(s->x2), s->stream);
+  SIM_CU(s, cudaMemsetAsync(d_max, 0, sizeof(unsigned int), s->stream));
+  const float a = s->a;
+  const float e = cosmo_e(s->P.cosmo, a);
+  const float rsd_scale = 1.0f / (a * a * e);  // frame.rs:66
+  launch_snapshot_particles(as<float>(s->p), densities ? as<float>(s->x2) : nullptr, as<uint32_t>(s->id), n, a,
+                            rsd_scale, speeds ? d_speeds : nullptr, densities ? d_dens : nullptr,
+                            rsd3 ? d_rsd : nullptr, d_max, s->stream);
+  if (grid) launch_downsample_grid(as<float>(s->gx), mn, d_grid, s->stream);
+  if (speeds) SIM_CU(s, cudaMemcpyAsync(speeds, d_speeds, n * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+  if (densities) SIM_CU(s, cudaMemcpyAsync(densities, d_dens, n * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+  if (rsd3) SIM_CU(s, cudaMemcpyAsync(rsd3, d_rsd, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+  if (grid) SIM_CU(s, cudaMemcpyAsync(grid, d_grid, gm3 * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+  unsigned int bits = 0;
+  SIM_CU(s, cudaMemcpyAsync(&bits, d_max, sizeof(bits), cudaMemcpyDeviceToHost, s->stream));
+  const int rc = sim_check(s);
+  if (rc) return rc;
+  if (grid_n) *grid_n = gm;
+  if (max_speed) std::memcpy(max_speed, &bits, sizeof(float));
+  return CPM_OK;
+}
+
 int cpm_sim_phase_times(cpm_sim* s, double* ms8, uint64_t* steps, int reset) {
   if (!s) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_phase_times: sim is NULL");
   int rc = flush_timing(s);
@@ -502,7 +539,7 @@ int cpm_sim_destroy(cpm_sim* s) {
   for (DevBuf* b : {&s->sort.keys_alt, &s->sort.vals_alt, &s->sort.block_hist, &s->sort.scan_tmp, &s->tree.geo,
                     &s->tree.mass, &s->tree.link, &s->tree.counters, &s->tree.prefix, &s->tree.scan_tmp, &s->tree.x4, &s->x, &s->p,
                     &s->acc, &s->id, &s->x2, &s->p2, &s->id2, &s->keys, &s->vals, &s->fx, &s->gx, &s->gy, &s->gz,
-                    &s->spec, &s->status, &s->counters, &s->pk, &s->q, &s->q2})
+                    &s->spec, &s->status, &s->counters, &s->pk, &s->q, &s->q2, &s->snap})
     release(*b);
   tree_walk_free(s->tree);
   release(s->host_tmp);

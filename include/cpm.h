@@ -167,6 +167,13 @@ int cpm_ics_zeldovich(int n_side, float box_size, const cpm_cosmology* cosmo, fl
 int cpm_power_spectrum(cpm_ctx* ctx, const float* x3, size_t n, int n_shells, double* k_mean, double* p_mean,
                        uint64_t* counts);
 
+/* frame.rs:30-55 `downsample_grid(delta)`: the viewer's gas texture, 1 + delta averaged over f^3
+ * blocks with f = ceil(n / 128) (frame.rs:27 MAX_GRID), side m = n / f (grid_n), ordered x fastest
+ * then y then z (the mesh is z fastest, so this transposes). delta is the context's n^3 mesh
+ * (CPM_E_MESH_MISMATCH otherwise); grid holds m^3 floats; grid_n may be NULL. Bit-identical to the
+ * reference's f32 sums. */
+int cpm_density_grid(cpm_ctx* ctx, const float* delta, int n, float* grid, int* grid_n);
+
 /* ------------------------------------------------------------------ device-resident simulation */
 /* Replaces `Simulation` (integrator.rs:34-186) under a `cuda` feature: state stays in HBM and
  * `step_to` runs one KDK step (kick, drift, deposit, FFT-Poisson, gather, tree build and walk,
@@ -222,6 +229,15 @@ int cpm_sim_get_state(cpm_sim* sim, float* x3, float* p3, float* acc3, float* de
  * CPM_SIM_TIMING, or when capture failed and the steps run uncaptured; 2 once both buffer
  * parities are captured). */
 int cpm_sim_graphs(cpm_sim* sim);
+/* runner.rs:263-284 `snapshot(&sim, want_grid)` and the max speed of runner.rs:244-247, computed on
+ * the device (no particle copy to the host beyond the outputs asked for). In the caller's particle
+ * order: speeds[n] = |p| / a (frame.rs:9-10); densities[n] = max(1 + delta(x), 0), delta the mesh
+ * of the last force evaluation interpolated by CIC (mesh.rs:72-77); rsd3[n][3] = p / (a^2 E(a))
+ * (frame.rs:62-69); grid = downsample_grid(delta) as cpm_density_grid (grid_n receives its side);
+ * max_speed = the largest speed. Any pointer may be NULL. Bit-identical to the reference's f32
+ * arithmetic for equal state. */
+int cpm_sim_snapshot(cpm_sim* sim, float* speeds, float* densities, float* rsd3, float* grid, int* grid_n,
+                     float* max_speed);
 /* cpm_power_spectrum of the simulation's current particles on its mesh, without copying them. */
 int cpm_sim_power_spectrum(cpm_sim* sim, int n_shells, double* k_mean, double* p_mean, uint64_t* counts);
 /* Overwrites positions and momenta (caller's order) and recomputes the acceleration at the current a. */
