@@ -213,6 +213,7 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
 
     # Phase breakdown: the same window again with per-phase CUDA events (uncaptured steps).
     phases, nsteps = np.zeros(8), 0
+    walk = None
     if not args.no_phases:
         simp = make_sim(cpm._native.SIM_TIMING)
         for a1 in sched[:args.warmup]:
@@ -220,7 +221,16 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
         simp.phase_times(reset=True)
         for a1 in sched[args.warmup:]:
             simp.step_to(a1)
-        phases, nsteps = simp.phase_times()
+        phases, nsteps = simp.phase_times(reset=True)
+        # one more step from the end state (the most clustered): interactions per second of the walk
+        simp.step_to(float(np.float32(sched[-1] * sched[-1] / sched[-2])))
+        ph1, _ = simp.phase_times()
+        c1 = simp.counters()
+        inter = c1["leaf_pairs"] + c1["node_accepts"]
+        walk = {"interactions": inter, "leaf_pairs": c1["leaf_pairs"], "node_accepts": c1["node_accepts"],
+                "candidates": c1["candidates"], "walk_ms": round(float(ph1[6]), 4),
+                "interactions_per_s": inter / (float(ph1[6]) / 1e3) if ph1[6] > 0 else None,
+                "note": "one step after the timed window (a beyond the last timed a), walk + second kick timed"}
         simp.close()
 
     # End to end through the host-buffer C-ABI step, same schedule window, on a fresh simulation.
@@ -288,6 +298,7 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
         "tree": {"nodes_last_step": counters["nodes"], "leaf_pairs_last_step": counters["leaf_pairs"],
                  "node_accepts_last_step": counters["node_accepts"],
                  "candidates_last_step": counters["candidates"]},
+        "tree_walk_end_state": walk,
         "gpu_launches": counters["launches_per_step"] * args.steps,
         "launches_per_step": counters["launches_per_step"],
         "clocks": clk,
