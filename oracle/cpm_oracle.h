@@ -131,6 +131,13 @@ void orc_zeldovich(int n, float box, const orc_cosmology* c, const orc_pspec* ps
 void orc_power_spectrum(const float* x3, size_t np, float box, int n, int n_shells, double* k_mean,
                         double* p_mean, uint64_t* counts);
 
+/* FP64 build (cpm_oracle_f64.cpp): PM (poisson.rs:33-88) plus, when split is given, the short-range
+ * tree force (tree.rs:171-323, coupling k_tree) in double precision at n_sample sampled particles
+ * (indices into x3); acc3 is [n_sample][3]. The precision-study reference for f32 results. */
+void orc64_accelerations(const float* x3, size_t n, double box, int mesh_n, double omega_m, double a,
+                         const orc_split* split, double k_tree, const uint32_t* sample, size_t n_sample,
+                         double* acc3);
+
 int orc_num_threads(void);
 
 #ifdef __cplusplus

@@ -103,6 +103,8 @@ def lib() -> C.CDLL:
         "orc_zeldovich": (None, [i, fl, C.POINTER(Cosmology), C.POINTER(PSpec), fl, C.c_uint64, f32p, f32p]),
         "orc_power_spectrum": (None, [f32p, sz, fl, i, i, f64p, f64p, u64p]),
         "orc_num_threads": (i, []),
+        "orc64_accelerations": (None, [f32p, sz, C.c_double, i, C.c_double, C.c_double, C.c_void_p, C.c_double,
+                                       u32p, sz, f64p]),
         "orc_step_sample": (None, [C.POINTER(Cosmology), fl, i, f32p, f32p, f32p, sz, fl, fl, C.c_void_p, u32p, sz,
                                    i, f64p]),
     }
@@ -410,6 +412,25 @@ def power_spectrum(x, box: float, n: int, n_shells: int):
     c = np.empty(n_shells, np.uint64)
     lib().orc_power_spectrum(x, len(x), box, n, n_shells, k, p, c)
     return k, p, c
+
+
+def tree_coupling64(omega_m: float, box: float, a: float, n: int) -> float:
+    """integrator.rs:150-152 in double: K = (3/2) Omega_m L^3 / (4 pi a N)."""
+    return 1.5 * omega_m * box ** 3 / (4.0 * np.pi * a * n)
+
+
+def accelerations_f64(x, box: float, mesh_n: int, omega_m: float, a: float, split: Split | None,
+                      sample) -> np.ndarray:
+    """FP64 build: PM + short-range tree force (coupling tree_coupling64) at the sampled particles,
+    everything in double precision; returns (len(sample), 3) float64."""
+    x = _f32(x)
+    sample = np.ascontiguousarray(sample, np.uint32)
+    out = np.empty((len(sample), 3), np.float64)
+    k = tree_coupling64(omega_m, box, a, len(x))
+    sp = C.cast(C.pointer(split), C.c_void_p) if split is not None else None
+    lib().orc64_accelerations(x, len(x), float(box), int(mesh_n), float(omega_m), float(a), sp, k, sample,
+                              len(sample), out)
+    return out
 
 
 def num_threads() -> int:
