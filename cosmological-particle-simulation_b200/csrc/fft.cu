@@ -726,7 +726,7 @@ static void r2c3_n(const FftPlan& p, const float* delta, const unsigned long lon
   const int rows = N * N;
   {
     constexpr int T = threads_for<M>();
-    constexpr int NB = 4 * c_tile(M) + c_tile(M) <= SMEM_LIMIT ? 2 : 1;
+    constexpr int NB = 2 * (4 * c_tile(M) + c_tile(M)) <= SMEM_LIMIT ? 2 : 1;  // two CTAs per SM
     const size_t smem = (2 * NB + 1) * c_tile(M);
     launch_persistent(k_r2c_z<N, NB, T>, T, smem, (rows + TW - 1) / TW, s, delta, fx, std::ldexp(1.0f, -fx_shift),
                       mean, spec, rows, tw);
@@ -760,7 +760,7 @@ static void poisson_n(const FftPlan& p, const PoissonParams& pp, const float* de
     float2* s0 = spec;
     {  // 1. z: R2C into slot 0 (staging buffers of 16-byte slots + one complex tile)
       constexpr int T = threads_for<M>();
-      constexpr int NB = 4 * c_tile(M) + c_tile(M) <= SMEM_LIMIT ? 2 : 1;
+      constexpr int NB = 2 * (4 * c_tile(M) + c_tile(M)) <= SMEM_LIMIT ? 2 : 1;  // two CTAs per SM
       const size_t smem = (2 * NB + 1) * c_tile(M);
       launch_persistent(k_r2c_z<N, NB, T>, T, smem, row_tiles, s, delta, fx, std::ldexp(1.0f, -fx_shift), mean, s0,
                         rows, tw);

@@ -198,17 +198,32 @@ __global__ void __launch_bounds__(RS_THREADS) k_radix_hist(const uint64_t* __res
   for (int t = threadIdx.x; t < RS_BINS; t += RS_THREADS) block_hist[(size_t)t * nblocks + blockIdx.x] = h[t];
 }
 
+// Dynamic shared memory of k_radix_scatter: per-warp digit counts, the block's digit starts and
+// global bases, and the tile reordered by digit.
+constexpr size_t RS_SCATTER_SMEM =
+    sizeof(uint32_t) * (RS_WARPS * RS_BINS + 2 * RS_BINS) + (sizeof(uint64_t) + sizeof(uint32_t)) * RS_TILE;
+
+// One stable pass: the tile is ranked by digit (per warp with __match_any_sync, warps in order),
+// reordered in shared memory, and each digit's run is written out contiguously, so consecutive
+// threads store consecutive addresses.
 __global__ void __launch_bounds__(RS_THREADS) k_radix_scatter(const uint64_t* __restrict__ kin,
                                                               const uint32_t* __restrict__ vin,
                                                               uint64_t* __restrict__ kout,
                                                               uint32_t* __restrict__ vout, size_t n, int shift,
                                                               const uint32_t* __restrict__ offsets, int nblocks) {
-  __shared__ uint32_t wc[RS_WARPS][RS_BINS];
+  extern __shared__ __align__(16) unsigned char rs_smem[];
+  uint64_t* sk = reinterpret_cast<uint64_t*>(rs_smem);                       // [RS_TILE]
+  uint32_t* sv = reinterpret_cast<uint32_t*>(sk + RS_TILE);                  // [RS_TILE]
+  uint32_t(*wc)[RS_BINS] = reinterpret_cast<uint32_t(*)[RS_BINS]>(sv + RS_TILE);  // [RS_WARPS][RS_BINS]
+  uint32_t* dstart = &wc[RS_WARPS][0];                                       // [RS_BINS]
+  uint32_t* gbase = dstart + RS_BINS;                                        // [RS_BINS]
+  __shared__ uint32_t warp_tot[RS_WARPS];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int t = threadIdx.x; t < RS_WARPS * RS_BINS; t += RS_THREADS) (&wc[0][0])[t] = 0;
   __syncthreads();
   const unsigned lt_mask = (1u << lane) - 1u;
-  const size_t wbase = (size_t)blockIdx.x * RS_TILE + (size_t)warp * 32 * RS_ITEMS;
+  const size_t tile0 = (size_t)blockIdx.x * RS_TILE;
+  const size_t wbase = tile0 + (size_t)warp * 32 * RS_ITEMS;
   uint64_t k[RS_ITEMS];
   uint32_t v[RS_ITEMS];
   uint32_t rank[RS_ITEMS];
@@ -230,14 +245,31 @@ __global__ void __launch_bounds__(RS_THREADS) k_radix_scatter(const uint64_t* __
     __syncwarp();
   }
   __syncthreads();
-  for (int t = threadIdx.x; t < RS_BINS; t += RS_THREADS) {
-    uint32_t run = offsets[(size_t)t * nblocks + blockIdx.x];
+  // Thread t = digit t: its block total, then the exclusive scan over digits (block-local starts).
+  static_assert(RS_THREADS == RS_BINS, "one thread per digit");
+  const int t = threadIdx.x;
+  uint32_t tot = 0;
 #pragma unroll
-    for (int w = 0; w < RS_WARPS; ++w) {
-      const uint32_t c = wc[w][t];
-      wc[w][t] = run;
-      run += c;
-    }
+  for (int w = 0; w < RS_WARPS; ++w) tot += wc[w][t];
+  uint32_t incl = tot;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) warp_tot[warp] = incl;
+  __syncthreads();
+  uint32_t before = 0;
+  for (int w = 0; w < warp; ++w) before += warp_tot[w];
+  const uint32_t start = before + incl - tot;
+  dstart[t] = start;
+  gbase[t] = offsets[(size_t)t * nblocks + blockIdx.x] - start;
+  uint32_t run = start;
+#pragma unroll
+  for (int w = 0; w < RS_WARPS; ++w) {
+    const uint32_t c = wc[w][t];
+    wc[w][t] = run;
+    run += c;
   }
   __syncthreads();
 #pragma unroll
@@ -245,10 +277,18 @@ __global__ void __launch_bounds__(RS_THREADS) k_radix_scatter(const uint64_t* __
     const size_t i = wbase + (size_t)j * 32 + lane;
     if (i < n) {
       const uint32_t d = (uint32_t)((k[j] >> shift) & (RS_BINS - 1));
-      const uint32_t pos = wc[warp][d] + rank[j];
-      kout[pos] = k[j];
-      vout[pos] = v[j];
+      const uint32_t lp = wc[warp][d] + rank[j];
+      sk[lp] = k[j];
+      sv[lp] = v[j];
     }
+  }
+  __syncthreads();
+  const uint32_t count = (uint32_t)min((size_t)RS_TILE, n - tile0);
+  for (uint32_t q = threadIdx.x; q < count; q += RS_THREADS) {
+    const uint64_t key = sk[q];
+    const uint32_t pos = gbase[(uint32_t)((key >> shift) & (RS_BINS - 1))] + q;
+    kout[pos] = key;
+    vout[pos] = sv[q];
   }
 }
 
@@ -266,13 +306,20 @@ cudaError_t radix_sort_pairs(uint64_t* keys, uint32_t* vals, size_t n, int bits,
   uint32_t* vb = as<uint32_t>(sc.vals_alt);
   uint32_t* hist = as<uint32_t>(sc.block_hist);
   const int passes = (bits + 7) / 8;
+  static bool smem_set = false;  // the attribute is per function; set before the first launch
+  if (!smem_set) {
+    if ((e = cudaFuncSetAttribute(k_radix_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)RS_SCATTER_SMEM)) != cudaSuccess)
+      return e;
+    smem_set = true;
+  }
   for (int p = 0; p < passes; ++p) {
     const int shift = 8 * p;
     count_launch();
     k_radix_hist<<<nblocks, RS_THREADS, 0, s>>>(ka, n, shift, hist, nblocks);
     if ((e = exclusive_scan_u32(hist, hist, (size_t)RS_BINS * nblocks, sc.scan_tmp, s)) != cudaSuccess) return e;
     count_launch();
-    k_radix_scatter<<<nblocks, RS_THREADS, 0, s>>>(ka, va, kb, vb, n, shift, hist, nblocks);
+    k_radix_scatter<<<nblocks, RS_THREADS, RS_SCATTER_SMEM, s>>>(ka, va, kb, vb, n, shift, hist, nblocks);
     std::swap(ka, kb);
     std::swap(va, vb);
   }

@@ -10,6 +10,7 @@
 //   Simulation    integrator.rs:34-186 new, step_to, positions/momenta, delta
 #pragma once
 
+#include <algorithm>
 #include <array>
 #include <complex>
 #include <cstddef>
@@ -179,6 +180,49 @@ class Simulation {  // integrator.rs:34-186
     Mesh m(mesh_n_, box_);
     check(cpm_sim_get_state(sim_.get(), nullptr, nullptr, nullptr, m.cells.data(), nullptr));
     return m;
+  }
+
+  // runner.rs:263-284 `snapshot`, reduced on the device (frame.rs:1-70): speeds |p|/a,
+  // densities max(1 + delta(x), 0), rsd shifts p / (a^2 E), the density grid when asked, max speed.
+  struct Frame {
+    Real redshift;
+    std::vector<Real> speeds, densities;
+    std::vector<Vec3> rsd;
+    std::size_t grid_n = 0;
+    std::vector<Real> grid;  // grid_n^3, x fastest
+    Real max_speed;
+  };
+  Frame snapshot(bool want_grid) const {
+    Frame f;
+    const std::size_t n = positions.size();
+    f.redshift = 1.0f / a - 1.0f;
+    f.speeds.resize(n);
+    f.densities.resize(n);
+    f.rsd.resize(n);
+    if (want_grid) {
+      const std::size_t fac = std::max<std::size_t>(1, (mesh_n_ + 127) / 128);
+      const std::size_t m = mesh_n_ / fac;
+      f.grid.resize(m * m * m);
+    }
+    int gn = 0;
+    check(cpm_sim_snapshot(sim_.get(), f.speeds.data(), f.densities.data(), f.rsd[0].data(),
+                           want_grid ? f.grid.data() : nullptr, &gn, &f.max_speed));
+    f.grid_n = want_grid ? (std::size_t)gn : 0;
+    return f;
+  }
+
+  // Shell-averaged P(k) of the current particles (the estimator of ics.rs:213-266), on the device.
+  struct PowerSpectrum {
+    std::vector<double> k_mean, p_mean;
+    std::vector<std::uint64_t> counts;
+  };
+  PowerSpectrum power_spectrum(int n_shells) const {
+    PowerSpectrum ps;
+    ps.k_mean.resize(n_shells);
+    ps.p_mean.resize(n_shells);
+    ps.counts.resize(n_shells);
+    check(cpm_sim_power_spectrum(sim_.get(), n_shells, ps.k_mean.data(), ps.p_mean.data(), ps.counts.data()));
+    return ps;
   }
 
   std::vector<Vec3> positions;

@@ -73,6 +73,12 @@ int main() {
     sim.step_to(1.0004f);
     const Real after = sim.positions[1][0] - sim.positions[0][0];
     CHECK("pair_attracts", after < before && after > 0.0f && sim.a == 1.0004f);
+    // runner.rs:263-284 snapshot on the device: both particles move, the grid is 64^3 of 1 + delta
+    const auto frame = sim.snapshot(true);
+    CHECK("snapshot", frame.speeds.size() == 2 && frame.speeds[0] > 0.0f && frame.max_speed >= frame.speeds[1] &&
+                          frame.grid_n == 64 && frame.grid.size() == 64u * 64u * 64u && frame.densities[0] >= 0.0f);
+    const auto ps = sim.power_spectrum(8);
+    CHECK("power_spectrum", ps.counts.size() == 8 && ps.counts[0] > 0 && ps.p_mean[0] > 0.0);
   }
   std::printf("all ok\n");
   return 0;
