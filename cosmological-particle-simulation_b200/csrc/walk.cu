@@ -283,7 +283,8 @@ __device__ __forceinline__ uint32_t bit_span(uint32_t lo, uint32_t len) {
 // Direct-sum phase 1 for one chunk: bit t set when source t lies within r_cut of the lane's
 // particle (tree.rs:286-298); the caller keeps the bits of the sources it sums directly. The
 // difference and its squared norm round exactly like the reference's separate f32 operations;
-// without periodic images two sources are tested per instruction (f32x2).
+// without periodic images the differences and squares of two sources are formed per instruction
+// (f32x2, each element rounded like the scalar operation) and the sums are scalar.
 template <bool WRAP>
 __device__ __forceinline__ uint32_t chunk_candidates(const WalkShared& sh, int cnt, float x0, float x1, float x2,
                                                      const WalkParams& w) {
@@ -295,8 +296,11 @@ __device__ __forceinline__ uint32_t chunk_candidates(const WalkShared& sh, int c
       const float2 d0 = __fadd2_rn(X0, *reinterpret_cast<const float2*>(sh.nx + t));
       const float2 d1 = __fadd2_rn(X1, *reinterpret_cast<const float2*>(sh.ny + t));
       const float2 d2 = __fadd2_rn(X2, *reinterpret_cast<const float2*>(sh.nz + t));
-      const float2 r2 = __fadd2_rn(__fadd2_rn(__fmul2_rn(d0, d0), __fmul2_rn(d1, d1)), __fmul2_rn(d2, d2));
-      pm |= ((uint32_t)!(r2.x > w.cut2) | ((uint32_t)!(r2.y > w.cut2) << 1)) << t;
+      // The squares are packed, the sums scalar: a packed multiply feeding a packed add can be
+      // contracted into one FMA, which would round differently from the reference's f32 ops.
+      const float2 q0 = __fmul2_rn(d0, d0), q1 = __fmul2_rn(d1, d1), q2 = __fmul2_rn(d2, d2);
+      const float r2a = __fadd_rn(__fadd_rn(q0.x, q1.x), q2.x), r2b = __fadd_rn(__fadd_rn(q0.y, q1.y), q2.y);
+      pm |= ((uint32_t)!(r2a > w.cut2) | ((uint32_t)!(r2b > w.cut2) << 1)) << t;
     }
   } else {
     for (int t = 0; t < cnt; ++t) {

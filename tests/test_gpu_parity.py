@@ -237,6 +237,19 @@ def test_tree_interaction_counts_match_oracle(cpm, orc):
     assert stats["nodes"] == len(orc.tree_build(x, 10.0)["count"])
 
 
+@pytest.mark.parametrize("n,box,r_cut", [(300_000, 40.0, 1.2), (200_000, 20.0, 0.9)])
+def test_cutoff_decisions_exact_at_scale(cpm, orc, n, box, r_cut):
+    """theta = 0 accepts no node, so the pair count depends only on the node centres (bit-exact)
+    and the reference's f32 cutoff test r^2 > r_cut^2: the count must equal the oracle's exactly,
+    over ~1e8 candidate pairs, many of them within an ulp of the cutoff."""
+    x = orc.scattered_tree(n, box, 17)
+    stats = {}
+    cpm.tree_accelerations(x, box, cpm.ForceSplit(0.5, r_cut, 0.05, 0.0), 1.0, stats=stats)
+    lp, na, _ = orc.tree_walk_stats(x, box, orc.Split(0.5, r_cut, 0.05, 0.0))
+    assert na == 0 and stats["node_accepts"] == 0
+    assert stats["leaf_pairs"] == lp
+
+
 def test_periodic_pair_interacts_across_the_boundary(cpm):
     """tree.rs:420-430 on the GPU."""
     acc = cpm.tree_accelerations(np.array([[0.1, 5.0, 5.0], [9.9, 5.0, 5.0]], np.float32), 10.0,
