@@ -72,6 +72,7 @@ struct WalkParams {
   float r_cut;
   float cut2;   // r_cut * r_cut
   float theta;
+  float theta2;  // theta * theta (f32), for the squared form of the opening test
   float inv_two_rs;
   float eps2;   // softening^2
   float k;      // Newtonian coupling
@@ -249,14 +250,15 @@ __device__ __forceinline__ float norm2(float a, float b, float c) {
   return __fadd_rn(__fadd_rn(__fmul_rn(a, a), __fmul_rn(b, b)), __fmul_rn(c, c));
 }
 
-// The reference's opening test `2 half < theta * sqrt(r2)` (tree.rs:297) with IEEE sqrt, evaluated
-// with rsqrtf and settled exactly only when the two sides are within a few ulps.
-__device__ __forceinline__ bool accept_node(float half, float theta, float r2) {
-  const float lhs = __fmul_rn(2.0f, half);
-  const float ra = r2 > 0.0f ? r2 * rsqrtf(r2) : 0.0f;
-  const float rhs_a = theta * ra;
-  if (fabsf(rhs_a - lhs) > 1e-6f * lhs) return lhs < rhs_a;
-  return lhs < __fmul_rn(theta, sqrtf(r2));
+// The reference's opening test `2 half < theta * sqrt(r2)` (tree.rs:297), from per-node
+// constants: lhs = 2 half, L2 = lhs^2, tol = 1e-5 L2. theta^2 r2 and
+// L2 carry at most ~7e-7 relative rounding against the exact squares of both sides, so outside
+// the 1e-5 band the squared comparison decides like the reference's; inside it the reference's
+// expression is evaluated (IEEE square root).
+__device__ __forceinline__ bool accept_node_sq(float r2, const float4& pre, const WalkParams& w) {
+  const float diff = __fsub_rn(__fmul_rn(w.theta2, r2), pre.y);
+  if (fabsf(diff) > pre.z) return diff > 0.0f;
+  return pre.w < __fmul_rn(w.theta, __fsqrt_rn(r2));
 }
 
 // Per-warp shared state of the walk.
@@ -266,6 +268,8 @@ struct WalkShared {
   float4 geo[2][8];                // the current and the next batch: centre, half
   float4 mass[2][8];               //                                 centre of mass, count
   uint4 link[2][8];                //                                 start, end, first child, child mask
+  float4 pre[8];                   // per node of the current batch: prune radius^2, (2 half)^2,
+                                   // 1e-5 (2 half)^2, 2 half
   float nx[32], ny[32], nz[32];    // a chunk of direct-sum sources, negated: -x, -y, -z
   float4 box_c, box_h;             // the warp's bounding box: centre, half extent (+ tolerance)
 };
@@ -408,44 +412,75 @@ __global__ void __launch_bounds__(WALK_THREADS) k_tree_walk(const uint4* __restr
     // image (|centre - x| < 0.49 L on every axis for the whole box), so that the lanes' own
     // distances are the raw differences; it keeps a node unless even the box's nearest point is
     // beyond r_cut + sqrt(3) half by a relative margin of 1e-5.
-    bool keep = false;
+    bool keep = false, far_edge = false, direct = false;
     if ((uint32_t)lane < b_count) {
       const float4 bc = sh.box_c, bh = sh.box_h, pg = bgeo[lane];
       const float e0 = fabsf(pg.x - bc.x), e1 = fabsf(pg.y - bc.y), e2 = fabsf(pg.z - bc.z);
+      const float mr = __fadd_rn(w.r_cut, __fmul_rn(SQRT_3, pg.w));
+      const float lhs = __fmul_rn(2.0f, pg.w), l2 = __fmul_rn(lhs, lhs);
+      sh.pre[lane] = make_float4(__fmul_rn(mr, mr), l2, 1e-5f * l2, lhs);
+      direct = (blink[lane].w & 1u) == 0u;
       keep = true;
-      if (fmaxf(e0 + bh.x, fmaxf(e1 + bh.y, e2 + bh.z)) < w.guard) {
+      const float emax = fmaxf(e0 + bh.x, fmaxf(e1 + bh.y, e2 + bh.z));
+      if (emax < w.guard) {
         const float g0 = fmaxf(e0 - bh.x, 0.0f), g1 = fmaxf(e1 - bh.y, 0.0f), g2 = fmaxf(e2 - bh.z, 0.0f);
-        const float mr = w.r_cut + SQRT_3 * pg.w;
         keep = !(g0 * g0 + g1 * g1 + g2 * g2 > mr * mr * 1.00001f);
       }
+      // No lane needs a periodic image for this node: every difference between a lane's
+      // particle and the node's centre, centre of mass or particles (all inside the cube) is
+      // below 0.49 L on every axis.
+      far_edge = emax + pg.w < w.guard;
     }
     const uint32_t cand = __ballot_sync(FULL, keep);
+    const uint32_t nwall = __ballot_sync(FULL, far_edge);
+    const uint32_t dbits = __ballot_sync(FULL, direct);
+    __syncwarp();
 
     // Classify every remaining node of the batch for this lane: prune, direct sum, accept or open.
     uint32_t dmask = 0, nwmask = 0, amask = 0, omask = 0;
     if ((b_mask >> lane) & 1u) {
-      for (uint32_t rem = cand; rem; rem &= rem - 1) {
-        const uint32_t c = __ffs(rem) - 1;
-        const float4 G = bgeo[c];
-        float t0 = __fsub_rn(G.x, x0), t1 = __fsub_rn(G.y, x1), t2 = __fsub_rn(G.z, x2);
-        // every source y of the node lies in [centre - half, centre + half]
-        const bool nowrap = fmaxf(fabsf(t0), fmaxf(fabsf(t1), fabsf(t2))) + G.w < w.guard;
-        min_image3(t0, t1, t2, w);
-        const float max_r = __fadd_rn(w.r_cut, __fmul_rn(SQRT_3, G.w));
-        if (norm2(t0, t1, t2) > __fmul_rn(max_r, max_r)) continue;
-        if ((blink[c].w & 1u) == 0u) {
-          // children[0] == NO_CHILD: direct sum over the node's particles (tree.rs:286-298)
-          dmask |= 1u << c;
-          nwmask |= (uint32_t)nowrap << c;
-          continue;
+      if ((cand & ~nwall) == 0u) {
+        // No node of the batch involves a periodic image: raw differences.
+        for (uint32_t rem = cand; rem; rem &= rem - 1) {
+          const uint32_t c = __ffs(rem) - 1;
+          const float4 G = bgeo[c], P = sh.pre[c];
+          const float t0 = __fsub_rn(G.x, x0), t1 = __fsub_rn(G.y, x1), t2 = __fsub_rn(G.z, x2);
+          if (norm2(t0, t1, t2) > P.x) continue;
+          if ((dbits >> c) & 1u) {
+            dmask |= 1u << c;
+            continue;
+          }
+          const float4 M = bmass[c];
+          const float s0 = __fsub_rn(M.x, x0), s1 = __fsub_rn(M.y, x1), s2 = __fsub_rn(M.z, x2);
+          if (accept_node_sq(norm2(s0, s1, s2), P, w))
+            amask |= 1u << c;
+          else
+            omask |= 1u << c;
         }
-        const float4 M = bmass[c];
-        float s0 = __fsub_rn(M.x, x0), s1 = __fsub_rn(M.y, x1), s2 = __fsub_rn(M.z, x2);
-        min_image3(s0, s1, s2, w);
-        if (accept_node(G.w, w.theta, norm2(s0, s1, s2)))
-          amask |= 1u << c;
-        else
-          omask |= 1u << c;
+        nwmask = dmask;
+      } else {
+        for (uint32_t rem = cand; rem; rem &= rem - 1) {
+          const uint32_t c = __ffs(rem) - 1;
+          const float4 G = bgeo[c], P = sh.pre[c];
+          float t0 = __fsub_rn(G.x, x0), t1 = __fsub_rn(G.y, x1), t2 = __fsub_rn(G.z, x2);
+          // every source y of the node lies in [centre - half, centre + half]
+          const bool nowrap = fmaxf(fabsf(t0), fmaxf(fabsf(t1), fabsf(t2))) + G.w < w.guard;
+          min_image3(t0, t1, t2, w);
+          if (norm2(t0, t1, t2) > P.x) continue;
+          if ((dbits >> c) & 1u) {
+            // children[0] == NO_CHILD: direct sum over the node's particles (tree.rs:286-298)
+            dmask |= 1u << c;
+            nwmask |= (uint32_t)nowrap << c;
+            continue;
+          }
+          const float4 M = bmass[c];
+          float s0 = __fsub_rn(M.x, x0), s1 = __fsub_rn(M.y, x1), s2 = __fsub_rn(M.z, x2);
+          min_image3(s0, s1, s2, w);
+          if (accept_node_sq(norm2(s0, s1, s2), P, w))
+            amask |= 1u << c;
+          else
+            omask |= 1u << c;
+        }
       }
     }
 
@@ -641,6 +676,7 @@ void launch_tree_walk(const TreeNodes& t, const float* sorted_x3, size_t n, floa
   w.r_cut = split.r_cut;
   w.cut2 = split.r_cut * split.r_cut;
   w.theta = split.theta;
+  w.theta2 = split.theta * split.theta;
   w.inv_two_rs = (float)(1.0 / (2.0 * (double)split.r_split));
   w.eps2 = split.softening * split.softening;
   w.k = k;
