@@ -64,6 +64,13 @@ struct cpm_sim {
   DevBuf q, q2;     // fixed-point positions (CPM_SIM_FIXED_POINT) and their sort scratch
   DevBuf snap;      // device outputs of cpm_sim_snapshot
   DevBuf host_tmp;  // caller-order staging of cpm_sim_step_host
+  // cpm_sim_step_host copies the new positions out on a second stream while the forces are
+  // computed: they are final once the step has sorted them.
+  DevBuf host_tmp_x;
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_sorted = nullptr;
+  float* x_out = nullptr;      // caller-order destination of this step's positions, or null
+  bool direct_step = false;    // run the next step uncaptured
 };
 
 #define SIM_CU(s, call)                                                                                      \
@@ -146,6 +153,13 @@ static int sim_accelerations(cpm_sim* s, float a, const StepScalars* dev = nullp
   if (fixed_point(s))  // the 32-bit words of q move like those of x
     launch_permute3(as<float>(s->q), as<uint32_t>(s->vals), n, as<float>(s->q2), s->stream);
   swap_sorted(s);
+  if (s->x_out) {
+    SIM_CU(s, cudaEventRecord(s->ev_sorted, s->stream));
+    SIM_CU(s, cudaStreamWaitEvent(s->side, s->ev_sorted, 0));
+    launch_scatter3(as<float>(s->x), as<uint32_t>(s->id), n, as<float>(s->host_tmp_x), s->side);
+    SIM_CU(s, cudaMemcpyAsync(s->x_out, s->host_tmp_x.p, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, s->side));
+    s->x_out = nullptr;
+  }
   mark(s, 2);
   launch_deposit_fixed(as<float>(s->x), n, 1.0f, mn, s->h, s->shift, as<unsigned long long>(s->fx), s->stream);
   mark(s, 3);
@@ -360,7 +374,7 @@ int cpm_sim_step_to(cpm_sim* s, float a1) {
   const unsigned long long l0 = launch_count();
   s->ev_set = q;
   const bool graphs =
-      !(s->P.flags & (CPM_SIM_NO_GRAPH | CPM_SIM_TIMING)) && s->warm[q] && !s->no_graph[q];
+      !(s->P.flags & (CPM_SIM_NO_GRAPH | CPM_SIM_TIMING)) && !s->direct_step && s->warm[q] && !s->no_graph[q];
   if (graphs && s->graph[q]) {
     const cudaError_t e = cudaGraphLaunch(s->graph[q], s->stream);
     if (e == cudaSuccess) swap_sorted(s);  // the host side of the replayed sort
@@ -399,15 +413,32 @@ static int download_caller_order(cpm_sim* s, const float* src3, float* host3) {
   return CPM_OK;
 }
 
+// The step runs uncaptured so that the positions' copy to the host can start on the second
+// stream right after the sort and overlap the force computation; the momenta follow at the end.
 int cpm_sim_step_host(cpm_sim* s, float a1, float* x3, float* p3) {
   if (!s || !x3 || !p3) return set_error(s ? &s->err : nullptr, CPM_E_INVALID, "cpm_sim_step_host: null pointer");
+  if (!s->side) {
+    SIM_CU(s, cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking));
+    SIM_CU(s, cudaEventCreateWithFlags(&s->ev_sorted, cudaEventDisableTiming));
+  }
+  SIM_CU(s, ensure(s->host_tmp_x, 3 * s->n * sizeof(float)));
   int rc = upload_caller_order(s, x3, as<float>(s->x));
   if (!rc && fixed_point(s)) launch_to_fixed(as<float>(s->x), as<uint32_t>(s->q), s->n, s->box, s->stream);
   if (!rc) rc = upload_caller_order(s, p3, as<float>(s->p));
-  if (!rc) rc = cpm_sim_step_to(s, a1);
-  if (!rc) rc = download_caller_order(s, as<float>(s->x), x3);
+  if (!rc) {
+    s->x_out = x3;
+    s->direct_step = true;
+    rc = cpm_sim_step_to(s, a1);
+    s->direct_step = false;
+    if (s->x_out) {  // the step ended before its sort
+      s->x_out = nullptr;
+      if (!rc) rc = download_caller_order(s, as<float>(s->x), x3);
+    }
+  }
   if (!rc) rc = download_caller_order(s, as<float>(s->p), p3);
+  const cudaError_t e = cudaStreamSynchronize(s->side);
   if (rc) return rc;
+  if (e != cudaSuccess) return set_error(&s->err, CPM_E_CUDA, std::string("position copy: ") + cudaGetErrorString(e));
   return sim_check(s);
 }
 
@@ -535,6 +566,7 @@ int cpm_sim_graphs(cpm_sim* s) { return s ? (s->graph[0] ? 1 : 0) + (s->graph[1]
 int cpm_sim_destroy(cpm_sim* s) {
   if (!s) return CPM_OK;
   if (s->stream) cudaStreamSynchronize(s->stream);
+  if (s->side) cudaStreamSynchronize(s->side);
   fft_plan_free(s->plan);
   for (DevBuf* b : {&s->sort.keys_alt, &s->sort.vals_alt, &s->sort.block_hist, &s->sort.scan_tmp, &s->tree.geo,
                     &s->tree.mass, &s->tree.link, &s->tree.counters, &s->tree.prefix, &s->tree.scan_tmp, &s->tree.x4, &s->x, &s->p,
@@ -543,6 +575,7 @@ int cpm_sim_destroy(cpm_sim* s) {
     release(*b);
   tree_walk_free(s->tree);
   release(s->host_tmp);
+  release(s->host_tmp_x);
   release(s->stepv);
   for (cudaGraphExec_t& g : s->graph)
     if (g) cudaGraphExecDestroy(g);
@@ -550,6 +583,8 @@ int cpm_sim_destroy(cpm_sim* s) {
     for (auto& e : row)
       if (e) cudaEventDestroy(e);
   if (s->stream) cudaStreamDestroy(s->stream);
+  if (s->side) cudaStreamDestroy(s->side);
+  if (s->ev_sorted) cudaEventDestroy(s->ev_sorted);
   delete s;
   return CPM_OK;
 }

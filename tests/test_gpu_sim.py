@@ -162,18 +162,26 @@ def test_sim_from_device_ics_equals_host_ics(cpm, orc):
 
 
 def test_step_host_equals_step_to(cpm):
-    """cpm_sim_step_host (host-owned state) gives bit-identical results to the resident step."""
+    """cpm_sim_step_host (host-owned state; positions copied out on a second stream while the
+    forces run) gives bit-identical results to the resident step, graph-replayed steps included,
+    and resident steps may follow host steps."""
     cc = cpm.Cosmology(0.0, 0.3, 0.7, 70.0)
     split = cpm.ForceSplit.with_(32.0, 32, 16, 1.0 / 30.0, 0.5)
     a = cpm.Simulation.from_zeldovich(cc, 32.0, 32, 16, 0.96, 0.8, 0.02, 9, split)
     b = cpm.Simulation.from_zeldovich(cc, 32.0, 32, 16, 0.96, 0.8, 0.02, 9, split)
     st = b.state()
     xh, ph = st["x"].copy(), st["p"].copy()
-    for a1 in cpm.ln_a_schedule(0.02, 0.3, 6)[:3]:
+    sched = cpm.ln_a_schedule(0.02, 0.3, 8)
+    for a1 in sched[:6]:
         a.step_to(a1)
         b.step_host(a1, xh, ph)
-    sa = a.state()
-    assert np.array_equal(sa["x"], xh) and np.array_equal(sa["p"], ph)
+        sa = a.state()
+        assert np.array_equal(sa["x"], xh) and np.array_equal(sa["p"], ph)
+    for a1 in sched[6:]:
+        a.step_to(a1)
+        b.step_to(a1)
+    sa, sb = a.state(), b.state()
+    assert np.array_equal(sa["x"], sb["x"]) and np.array_equal(sa["p"], sb["p"])
 
 
 def test_graph_replay_equals_direct_launches(cpm):
