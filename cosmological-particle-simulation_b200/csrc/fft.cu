@@ -29,9 +29,10 @@
 //   2. y pass: forward c2c along y;
 //   3. x pass: forward c2c along x, the Green's function of poisson.rs:52-74 in the reference's f32
 //      operation order (optionally divided by the CIC window squared), then two inverse x
-//      transforms: of -i k_x phi (x component) and of phi, which gives the y and z components after
-//      multiplying by -i k_y and -i k_z (constant along an x line) — three half spectra written;
-//   4. y pass: inverse c2c along y of the three spectra;
+//      transforms: of -i k_x phi (x component) and of phi — two half spectra written;
+//   4. y pass: inverse c2c along y of the x component; and, reading the x-transformed phi once,
+//      of -i k_y phi and -i k_z phi (k_y and k_z are constant along an x line, so the factors
+//      commute with the x transform), written as the y and z components;
 //   5. z pass: C2R of each row, scaled by 1/n^3 (poisson.rs:77-87), into three f32 meshes.
 #include <algorithm>
 #include <cmath>
@@ -487,7 +488,7 @@ __global__ void __launch_bounds__(T) k_c2r_z(const float2* __restrict__ spec, lo
 // c2c along x, the Green's function of poisson.rs:52-74, then
 //   x component: inverse x transform of -i k_x phi;
 //   y, z components: -i k_y and -i k_z times the inverse x transform of phi (k_y, k_z constant
-//   along the line, so the factor commutes with the transform).
+//   along the line, so the factor commutes with the transform), applied by k_grad_yz.
 // The gradient factor is the reference's (phi * (0 - i k_a), poisson.rs:70); for y and z it
 // multiplies the transformed phi instead, which differs only in round-off.
 // Shared memory: NBUF input tiles, then one work tile for -i k_x phi.
@@ -539,20 +540,49 @@ __global__ void __launch_bounds__(T) k_poisson_x(const float2* __restrict__ spec
         __syncthreads();
         fft_lines<N, true, T>(gxb, tw);
         fft_lines<N, true, T>(phi, tw);
-        const float nky = -ky;
-#pragma unroll 2
+        // -i k_x phi to slot 0; the x-transformed phi to slot 1, from which the y pass forms the
+        // y and z components (k_y and k_z are constant along an x line)
+        store_cols<N, T>(gxb, spec_out, base, g.elem_stride, valid);
+        store_cols<N, T>(phi, spec_out + comp_stride, base, g.elem_stride, valid);
+      });
+}
+
+// Inverse y pass of the y and z gradient components: reads the x-transformed potential of slot 1
+// once, forms -i k_y phi and -i k_z phi (the f32 operations of k_green_grad) and writes their
+// inverse y transforms to slots 1 and 2; tile -> (x, column tile), lines along y.
+template <int N, int NBUF, int T>
+__global__ void __launch_bounds__(T) k_grad_yz(float2* spec, long long comp_stride, ColGeo g, PoissonParams pp,
+                                               const float2* __restrict__ tw) {
+  extern __shared__ float2 smem[];
+  float2* gzb = smem + NBUF * N * TLD;
+  float2* phi_slot = spec + comp_stride;
+  pipeline<NBUF>(
+      smem, N * TLD, g.outer * g.col_tiles,
+      [&](float2* buf, int tile) {
+        const int o = tile / g.col_tiles, ct = tile % g.col_tiles;
+        const long long base = (long long)o * g.outer_stride + (long long)ct * TW;
+        async_load_cols<N, T>(buf, phi_slot, base, g.elem_stride, min(TW, g.cols - ct * TW));
+      },
+      [&](float2* cur, int tile) {
+        const int o = tile / g.col_tiles, ct = tile % g.col_tiles;
+        const int valid = min(TW, g.cols - ct * TW);
+        const long long base = (long long)o * g.outer_stride + (long long)ct * TW;
+        const int z0 = ct * TW;
         for (int q = threadIdx.x; q < N * TW; q += T) {
           const int l = q % TW, t = q / TW;
-          if (l >= valid) continue;
-          const long long gi = base + l + (long long)t * g.elem_stride;
-          spec_out[gi] = gxb[t * TLD + l];
-          const float2 p = phi[t * TLD + l];
+          const float2 p = cur[t * TLD + l];
+          const float nky = -wavenumber(t, N, pp.two_pi_over_l);
           const float nkz = -wavenumber(z0 + l, N, pp.two_pi_over_l);
-          spec_out[comp_stride + gi] = make_float2(__fsub_rn(__fmul_rn(p.x, 0.0f), __fmul_rn(p.y, nky)),
-                                                   __fadd_rn(__fmul_rn(p.x, nky), __fmul_rn(p.y, 0.0f)));
-          spec_out[2 * comp_stride + gi] = make_float2(__fsub_rn(__fmul_rn(p.x, 0.0f), __fmul_rn(p.y, nkz)),
-                                                       __fadd_rn(__fmul_rn(p.x, nkz), __fmul_rn(p.y, 0.0f)));
+          cur[t * TLD + l] = make_float2(__fsub_rn(__fmul_rn(p.x, 0.0f), __fmul_rn(p.y, nky)),
+                                         __fadd_rn(__fmul_rn(p.x, nky), __fmul_rn(p.y, 0.0f)));
+          gzb[t * TLD + l] = make_float2(__fsub_rn(__fmul_rn(p.x, 0.0f), __fmul_rn(p.y, nkz)),
+                                         __fadd_rn(__fmul_rn(p.x, nkz), __fmul_rn(p.y, 0.0f)));
         }
+        __syncthreads();
+        fft_lines<N, true, T>(cur, tw);
+        fft_lines<N, true, T>(gzb, tw);
+        store_cols<N, T>(cur, phi_slot, base, g.elem_stride, valid);
+        store_cols<N, T>(gzb, spec + 2 * comp_stride, base, g.elem_stride, valid);
       });
 }
 
@@ -767,16 +797,27 @@ static void poisson_n(const FftPlan& p, const PoissonParams& pp, const float* de
     }
     // 2. y forward on slot 0: lines along y (stride NHP), columns along kz adjacent, outer = x
     cols_pass<N>(s0, 0, 1, ColGeo{n * NHP, NHP, NH, 0, N}, 0, tw, s);
-    {  // 3. x forward + Green + gradient + x inverse -> slots 0..2; outer = y
+    {  // 3. x forward + Green + gradient + x inverse -> slots 0 (-i k_x phi) and 1 (phi); outer = y
       constexpr int T = threads_for<N>();
       constexpr int NBX = 3 * c_tile(N) <= SMEM_LIMIT ? 2 : 1;
       const size_t smem = (NBX + 1) * c_tile(N);
       ColGeo g{NHP, n * NHP, NH, (NH + TW - 1) / TW, N};
       launch_persistent(k_poisson_x<N, NBX, T>, T, smem, g.outer * g.col_tiles, s, s0, spec, comp, g, pp, deconv, tw);
     }
+    // 4. y inverse: slot 0 (x component), then slots 1, 2 (y, z components) from the potential
+    cols_pass<N>(spec, comp, 1, ColGeo{n * NHP, NHP, NH, 0, N}, 1, tw, s);
+    {
+      constexpr int T = threads_for<N>();
+      constexpr int NBY = 3 * c_tile(N) <= SMEM_LIMIT ? 2 : 1;
+      const size_t smem = (NBY + 1) * c_tile(N);
+      ColGeo g{n * NHP, NHP, NH, (NH + TW - 1) / TW, N};
+      launch_persistent(k_grad_yz<N, NBY, T>, T, smem, g.outer * g.col_tiles, s, spec, comp, g, pp, tw);
+    }
   }
-  // 4. y inverse on the three component spectra
-  cols_pass<N>(spec, comp, 3, ColGeo{n * NHP, NHP, NH, 0, N}, 1, tw, s);
+  if constexpr (2 * c_tile(N) > SMEM_LIMIT) {
+    // 4. y inverse on the three component spectra
+    cols_pass<N>(spec, comp, 3, ColGeo{n * NHP, NHP, NH, 0, N}, 1, tw, s);
+  }
   {  // 5. z: C2R with 1/n^3
     constexpr int T = threads_for<M>();
     constexpr int NB = 2 * c_tile(M + 1) <= SMEM_LIMIT ? 2 : 1;
