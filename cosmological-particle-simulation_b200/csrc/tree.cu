@@ -4,7 +4,8 @@
 // tree.rs:186-250), so every node of the reference's tree is a contiguous range of the sorted
 // array: the particles whose first d digits equal the node's prefix. One kernel per level splits
 // each node of that level that holds more than LEAF_SIZE particles: the 8 octant sub-ranges are
-// found by binary search on digit d+1 (sorted within the node), and the non-empty ones become
+// found on digit d+1 (sorted within the node: a thread per node on wide levels,
+// a warp per node on levels with few nodes), and the non-empty ones become
 // children, allocated contiguously in octant order. Node centres are built with the reference's
 // f32 arithmetic (centre +- half/2), so they are bit-identical. A node deeper than the 21 key
 // digits that still holds more than LEAF_SIZE particles stays a leaf (the reference would keep
@@ -31,6 +32,36 @@ constexpr int CNT_WORDS = 64;
 
 __device__ __forceinline__ uint32_t digit_at(uint64_t key, int shift) { return (uint32_t)(key >> shift) & 7u; }
 
+// First index in [lo, hi) whose digit at `shift` is >= o, or hi if none (digits non-decreasing in
+// the range), found by the whole warp: each round probes 32 evenly spaced keys and keeps the
+// interval between the last probe below o and the first at or above it, so a range of c keys
+// takes about log32(c) rounds of one load per lane.
+__device__ __forceinline__ uint32_t warp_lower_bound(const uint64_t* __restrict__ keys, uint32_t lo, uint32_t hi,
+                                                     uint32_t o, int shift, int lane) {
+  const unsigned FULL = 0xffffffffu;
+  while (hi - lo >= 32u) {
+    const uint32_t p = lo + (uint32_t)(((uint64_t)(hi - lo) * (uint32_t)lane) >> 5);  // p_0 = lo
+    const uint32_t ge = __ballot_sync(FULL, digit_at(__ldg(keys + p), shift) >= o);
+    if (ge & 1u) return lo;
+    const int j = ge ? __ffs(ge) - 1 : 32;  // first probe at or above o (32: none)
+    const uint32_t plo = __shfl_sync(FULL, p, j - 1);
+    const uint32_t phi = j < 32 ? __shfl_sync(FULL, p, j & 31) : hi;
+    lo = plo + 1u;
+    hi = phi;
+  }
+  const uint32_t p = lo + (uint32_t)lane;
+  const uint32_t ge = __ballot_sync(FULL, p >= hi || digit_at(__ldg(keys + p), shift) >= o);
+  return lo + (uint32_t)(__ffs(ge) - 1);  // lane hi - lo (< 32) always votes
+}
+
+__global__ void k_tree_root(uint4* link, float4* geo, uint32_t* counters, uint32_t n, float half0) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    link[0] = make_uint4(0u, n, 0u, 0u);
+    geo[0] = make_float4(half0, half0, half0, half0);
+  }
+  if (blockIdx.x == 0 && threadIdx.x < CNT_WORDS) counters[threadIdx.x] = threadIdx.x == 0 ? 1u : 0u;
+}
+
 // first index in [lo, hi) whose digit is >= o (digits non-decreasing in the range)
 __device__ __forceinline__ uint32_t lower_bound_digit(const uint64_t* __restrict__ keys, uint32_t lo, uint32_t hi,
                                                       uint32_t o, int shift) {
@@ -44,17 +75,19 @@ __device__ __forceinline__ uint32_t lower_bound_digit(const uint64_t* __restrict
   return lo;
 }
 
-__global__ void k_tree_root(uint4* link, float4* geo, uint32_t* counters, uint32_t n, float half0) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) {
-    link[0] = make_uint4(0u, n, 0u, 0u);
-    geo[0] = make_float4(half0, half0, half0, half0);
-  }
-  if (blockIdx.x == 0 && threadIdx.x < CNT_WORDS) counters[threadIdx.x] = threadIdx.x == 0 ? 1u : 0u;
-}
+// Splits the nodes of level d. A level with more nodes than the grid has warps takes one node
+// per thread: the 8 octant sub-ranges by binary search on digit d+1. A smaller level (the top
+// levels, and the sparse deep levels of clustered states), where a thread's searches would be
+// a long chain of dependent loads with little else in flight, takes one node per warp: nodes of
+// up to SMALL_NODE particles count the digits of all their keys (coalesced loads, a ballot per
+// octant), larger ones search the 7 boundaries with warp_lower_bound.
+constexpr uint32_t SMALL_NODE = 256;
 
 __global__ void __launch_bounds__(BUILD_THREADS) k_tree_level(int d, const uint64_t* __restrict__ keys, uint4* link,
                                                               float4* geo, uint32_t* counters, uint32_t capacity,
                                                               DevStatus* st) {
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
   uint32_t lb = 0;
   for (int j = 0; j < d; ++j) lb += counters[j];
   const uint32_t cnt = counters[d];
@@ -62,52 +95,120 @@ __global__ void __launch_bounds__(BUILD_THREADS) k_tree_level(int d, const uint6
   // After a capacity failure the counters overshoot; never touch nodes past the arrays.
   const uint32_t level_end = min(next_base, capacity);
   const int shift = 3 * (KEY_LEVELS - 1 - d);
-  for (uint32_t node = lb + blockIdx.x * BUILD_THREADS + threadIdx.x; node < level_end;
-       node += gridDim.x * BUILD_THREADS) {
+  const uint32_t warps = gridDim.x * (BUILD_THREADS / 32);
+  if (cnt > warps) {
+    for (uint32_t node = lb + blockIdx.x * BUILD_THREADS + threadIdx.x; node < level_end;
+         node += gridDim.x * BUILD_THREADS) {
+      const uint4 L = link[node];
+      const uint32_t s = L.x, e = L.y, c = e - s;
+      if (c <= (uint32_t)LEAF_SIZE || d >= MAX_DEPTH) {
+        link[node] = make_uint4(s, e, 0u, (uint32_t)d << 8);
+        continue;
+      }
+      if (d >= KEY_LEVELS) {
+        atomicAdd(&counters[CNT_DEPTH_LIMIT], 1u);
+        link[node] = make_uint4(s, e, 0u, (uint32_t)d << 8);
+        continue;
+      }
+      uint32_t b[9];
+      b[0] = s;
+      b[8] = e;
+      uint32_t lo = s;
+#pragma unroll
+      for (uint32_t o = 1; o < 8; ++o) {
+        lo = lower_bound_digit(keys, lo, e, o, shift);
+        b[o] = lo;
+      }
+      uint32_t mask = 0;
+#pragma unroll
+      for (int o = 0; o < 8; ++o)
+        if (b[o + 1] > b[o]) mask |= 1u << o;
+      const uint32_t nch = (uint32_t)__popc(mask);
+      const uint32_t first = next_base + atomicAdd(&counters[d + 1], nch);
+      if (first + nch > capacity) {
+        dev_fail(st, DEV_NODE_CAPACITY, (int)(first + nch));
+        link[node] = make_uint4(s, e, 0u, (uint32_t)d << 8);
+        continue;
+      }
+      const float4 G = geo[node];
+      const float q = G.w * 0.5f;  // half / 2.0
+      uint32_t r = 0;
+#pragma unroll
+      for (int o = 0; o < 8; ++o) {
+        if (!(mask & (1u << o))) continue;
+        const uint32_t child = first + r++;
+        link[child] = make_uint4(b[o], b[o + 1], 0u, 0u);
+        geo[child] = make_float4(__fadd_rn(G.x, (o & 1) ? q : -q), __fadd_rn(G.y, (o & 2) ? q : -q),
+                                 __fadd_rn(G.z, (o & 4) ? q : -q), q);
+      }
+      link[node] = make_uint4(s, e, first, mask | ((uint32_t)d << 8));
+      atomicMax(&counters[CNT_MAX_DEPTH], (uint32_t)(d + 1));
+    }
+    return;
+  }
+  for (uint32_t node = lb + blockIdx.x * (BUILD_THREADS / 32) + (threadIdx.x >> 5); node < level_end;
+       node += warps) {
     const uint4 L = link[node];
     const uint32_t s = L.x, e = L.y, c = e - s;
     if (c <= (uint32_t)LEAF_SIZE || d >= MAX_DEPTH) {
-      link[node] = make_uint4(s, e, 0u, (uint32_t)d << 8);
+      if (lane == 0) link[node] = make_uint4(s, e, 0u, (uint32_t)d << 8);
       continue;
     }
     if (d >= KEY_LEVELS) {
-      atomicAdd(&counters[CNT_DEPTH_LIMIT], 1u);
-      link[node] = make_uint4(s, e, 0u, (uint32_t)d << 8);
+      if (lane == 0) {
+        atomicAdd(&counters[CNT_DEPTH_LIMIT], 1u);
+        link[node] = make_uint4(s, e, 0u, (uint32_t)d << 8);
+      }
       continue;
     }
-    uint32_t b[9];
-    b[0] = s;
-    b[8] = e;
-    uint32_t lo = s;
+    uint32_t bo = s;  // lane o (1..7): first index whose digit is >= o
+    if (c <= SMALL_NODE) {
+      uint32_t below = 0;  // lane o: keys with digit < o
+      for (uint32_t i0 = s; i0 < e; i0 += 32) {
+        const uint32_t i = i0 + (uint32_t)lane;
+        const uint32_t dg = i < e ? digit_at(__ldg(keys + i), shift) : 8u;
 #pragma unroll
-    for (uint32_t o = 1; o < 8; ++o) {
-      lo = lower_bound_digit(keys, lo, e, o, shift);
-      b[o] = lo;
+        for (uint32_t o = 1; o < 8; ++o) {
+          const uint32_t bal = __ballot_sync(FULL, dg < o);
+          if ((uint32_t)lane == o) below += (uint32_t)__popc(bal);
+        }
+      }
+      bo = s + below;
+    } else {
+      uint32_t lo = s;
+      for (uint32_t o = 1; o < 8; ++o) {
+        lo = warp_lower_bound(keys, lo, e, o, shift, lane);
+        if ((uint32_t)lane == o) bo = lo;
+      }
     }
-    uint32_t mask = 0;
-#pragma unroll
-    for (int o = 0; o < 8; ++o)
-      if (b[o + 1] > b[o]) mask |= 1u << o;
+    // Lane o < 8: octant o's range [olo, ohi) (b[0] = s, b[8] = e).
+    const uint32_t nb = __shfl_sync(FULL, bo, (lane + 1) & 31);
+    const uint32_t olo = lane == 0 ? s : bo, ohi = lane == 7 ? e : nb;
+    const uint32_t mask = __ballot_sync(FULL, lane < 8 && ohi > olo);
     const uint32_t nch = (uint32_t)__popc(mask);
-    const uint32_t first = next_base + atomicAdd(&counters[d + 1], nch);
+    uint32_t first = 0;
+    if (lane == 0) first = next_base + atomicAdd(&counters[d + 1], nch);
+    first = __shfl_sync(FULL, first, 0);
     if (first + nch > capacity) {
-      dev_fail(st, DEV_NODE_CAPACITY, (int)(first + nch));
-      link[node] = make_uint4(s, e, 0u, (uint32_t)d << 8);
+      if (lane == 0) {
+        dev_fail(st, DEV_NODE_CAPACITY, (int)(first + nch));
+        link[node] = make_uint4(s, e, 0u, (uint32_t)d << 8);
+      }
       continue;
     }
-    const float4 G = geo[node];
-    const float q = G.w * 0.5f;  // half / 2.0
-    uint32_t r = 0;
-#pragma unroll
-    for (int o = 0; o < 8; ++o) {
-      if (!(mask & (1u << o))) continue;
-      const uint32_t child = first + r++;
-      link[child] = make_uint4(b[o], b[o + 1], 0u, 0u);
+    if (lane < 8 && ((mask >> lane) & 1u)) {
+      const float4 G = geo[node];
+      const float q = G.w * 0.5f;  // half / 2.0
+      const int o = lane;
+      const uint32_t child = first + (uint32_t)__popc(mask & ((1u << o) - 1u));
+      link[child] = make_uint4(olo, ohi, 0u, 0u);
       geo[child] = make_float4(__fadd_rn(G.x, (o & 1) ? q : -q), __fadd_rn(G.y, (o & 2) ? q : -q),
                                __fadd_rn(G.z, (o & 4) ? q : -q), q);
     }
-    link[node] = make_uint4(s, e, first, mask | ((uint32_t)d << 8));
-    atomicMax(&counters[CNT_MAX_DEPTH], (uint32_t)(d + 1));
+    if (lane == 0) {
+      link[node] = make_uint4(s, e, first, mask | ((uint32_t)d << 8));
+      atomicMax(&counters[CNT_MAX_DEPTH], (uint32_t)(d + 1));
+    }
   }
 }
 
