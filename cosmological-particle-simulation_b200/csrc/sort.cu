@@ -1,6 +1,6 @@
 // sort.cu — octant keys of the tree descent, stable LSD radix sort of (u64 key, u32 value)
 // pairs, and exclusive scans. HBM-bound integer work: coalesced tiles, per-warp ranking with
-// __match_any_sync, no tensor cores.
+// ballots, no tensor cores.
 #include <algorithm>
 #include <atomic>
 
@@ -171,13 +171,26 @@ cudaError_t exclusive_scan_u32(const uint32_t* in, uint32_t* out, size_t n, DevB
 // ---------------------------------------------------------------------------------------------
 // LSD radix sort, 8-bit digits. Per pass: block histograms (digit-major), exclusive scan of the
 // histograms, then a stable scatter. Within a block each warp ranks a contiguous sub-tile in
-// warp-striped rounds with __match_any_sync, so equal digits keep their input order.
+// warp-striped rounds (lanes with equal digits found by ballots), so equal digits keep their
+// input order.
 // ---------------------------------------------------------------------------------------------
 constexpr int RS_THREADS = 256;
 constexpr int RS_ITEMS = 16;
 constexpr int RS_TILE = RS_THREADS * RS_ITEMS;
 constexpr int RS_WARPS = RS_THREADS / 32;
 constexpr int RS_BINS = 256;
+
+// The lanes whose 9-bit value d equals this lane's (a digit, or 0x100 | lane for a lane without
+// an element): one ballot per bit, the same mask as __match_any_sync.
+__device__ __forceinline__ uint32_t match_digit(uint32_t d) {
+  uint32_t peers = 0xffffffffu;
+#pragma unroll
+  for (int b = 0; b < 9; ++b) {
+    const uint32_t bal = __ballot_sync(0xffffffffu, (d >> b) & 1u);
+    peers &= ((d >> b) & 1u) ? bal : ~bal;
+  }
+  return peers;
+}
 
 __global__ void __launch_bounds__(RS_THREADS) k_radix_hist(const uint64_t* __restrict__ keys, size_t n, int shift,
                                                            uint32_t* __restrict__ block_hist, int nblocks) {
@@ -191,7 +204,7 @@ __global__ void __launch_bounds__(RS_THREADS) k_radix_hist(const uint64_t* __res
     const size_t i = base + (size_t)j * RS_THREADS + threadIdx.x;
     const bool valid = i < n;
     const uint32_t d = valid ? (uint32_t)((keys[i] >> shift) & (RS_BINS - 1)) : (0x100u | (uint32_t)lane);
-    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    const uint32_t peers = match_digit(d);
     if (valid && (__ffs(peers) - 1) == lane) atomicAdd(&h[d], (uint32_t)__popc(peers));
   }
   __syncthreads();
@@ -203,7 +216,7 @@ __global__ void __launch_bounds__(RS_THREADS) k_radix_hist(const uint64_t* __res
 constexpr size_t RS_SCATTER_SMEM =
     sizeof(uint32_t) * (RS_WARPS * RS_BINS + 2 * RS_BINS) + (sizeof(uint64_t) + sizeof(uint32_t)) * RS_TILE;
 
-// One stable pass: the tile is ranked by digit (per warp with __match_any_sync, warps in order),
+// One stable pass: the tile is ranked by digit (per warp with match_digit, warps in order),
 // reordered in shared memory, and each digit's run is written out contiguously, so consecutive
 // threads store consecutive addresses.
 __global__ void __launch_bounds__(RS_THREADS) k_radix_scatter(const uint64_t* __restrict__ kin,
@@ -234,7 +247,7 @@ __global__ void __launch_bounds__(RS_THREADS) k_radix_scatter(const uint64_t* __
     k[j] = valid ? kin[i] : 0ull;
     v[j] = valid ? vin[i] : 0u;
     const uint32_t d = valid ? (uint32_t)((k[j] >> shift) & (RS_BINS - 1)) : (0x100u | (uint32_t)lane);
-    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    const uint32_t peers = match_digit(d);
     uint32_t prev = 0;
     if (valid) prev = wc[warp][d];
     __syncwarp();
