@@ -263,3 +263,18 @@ def test_nonfinite_position_is_reported(cpm):
     with pytest.raises(cpm.CpmError) as e:
         cpm.tree_accelerations(x, 1.0, cpm.ForceSplit(0.1, 0.3, 0.01, 0.5), 1.0)
     assert e.value.code == -6
+
+
+def test_tree_coincident_particles_match_oracle(cpm, orc):
+    """More than LEAF_SIZE particles at one exact position share all 21 key digits, so their node
+    at the key depth stays a leaf; the reference keeps splitting that one-child chain (to depth 40)
+    and sums the particles directly at its first node without an octant-0 child. The
+    accelerations agree all the same, and coincident pairs (r = 0) add nothing."""
+    x = orc.scattered_tree(5000, 10.0, 8)
+    x[:20] = x[0]
+    x[20:32] = x[100]
+    split = (0.5, 1.5, 0.05, 0.5)
+    got = cpm.tree_accelerations(x, 10.0, cpm.ForceSplit(*split), 1.0)
+    ref = orc.tree_accelerations(x, 10.0, orc.Split(*split), 1.0)
+    assert np.all(np.isfinite(got))
+    assert rel_rms(got, ref) < 1e-5
