@@ -143,6 +143,26 @@ def ncu_traffic() -> dict | None:
 
 # ------------------------------------------------------------------------------------------ ours
 
+def replica_seed(base: int, rank: int) -> int:
+    """The replicas of a multi-GPU run differ only in the seed of their initial conditions."""
+    return base + rank
+
+
+def max_over_ranks(ms: float, dist, device) -> float:
+    """The job's time: the slowest rank's device time. Every rank calls it, in the same order."""
+    if not dist:
+        return ms
+    import torch
+    t = torch.tensor([ms], device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(n: int, world: int, steps: int, ms: float) -> float:
+    """Whole-job throughput: each of `world` ranks advances its own n particles by `steps` steps."""
+    return n * world * steps / (ms / 1e3)
+
+
 def run_ours(args, rank: int, world: int, dist) -> dict | None:
     import torch
 
@@ -167,8 +187,8 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
     def make_sim(flags: int):
         if args.load_state:
             return cpm.Simulation(cosmo, box, mesh, st0["x"], st0["p"], a_saved, split, flags=flags)
-        return cpm.Simulation.from_zeldovich(cosmo, box, mesh, n_side, N_S, SIGMA8, A_INIT, wl["seed"] + rank, split,
-                                             flags=flags)
+        return cpm.Simulation.from_zeldovich(cosmo, box, mesh, n_side, N_S, SIGMA8, A_INIT, replica_seed(wl["seed"], rank),
+                                             split, flags=flags)
 
     # The timed run replays the step's captured CUDA graphs (no per-phase events).
     sim = make_sim(0)
@@ -195,11 +215,7 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
     ms_local = t_start.elapsed_time(t_end)
     if dist:
         dist.barrier()
-        t = torch.tensor([ms_local], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    else:
-        ms = ms_local
+    ms = max_over_ranks(ms_local, dist, dev)
     counters = sim.counters()
     graphs = sim.graphs()
     if args.save_state and rank == 0:
@@ -236,7 +252,7 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
     # End to end through the host-buffer C-ABI step, same schedule window, on a fresh simulation.
     e2e = None
     if not args.no_e2e:
-        sim2 = cpm.Simulation.from_zeldovich(cosmo, box, mesh, n_side, N_S, SIGMA8, A_INIT, wl["seed"] + rank, split)
+        sim2 = cpm.Simulation.from_zeldovich(cosmo, box, mesh, n_side, N_S, SIGMA8, A_INIT, replica_seed(wl["seed"], rank), split)
         for a1 in sched[:args.warmup]:
             sim2.step_to(a1)
         xs = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
@@ -257,13 +273,9 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
             sim2.step_host(a1, xh, ph)
         e1.record(s2)
         torch.cuda.synchronize()
-        ems = e0.elapsed_time(e1)
-        if dist:
-            t = torch.tensor([ems], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
+        ems = max_over_ranks(e0.elapsed_time(e1), dist, dev)
         sim2.close()
-        e2e = {"value": n * world * len(e2e_steps) / (ems / 1e3), "unit": "particle-steps/s",
+        e2e = {"value": job_rate(n, world, len(e2e_steps), ems), "unit": "particle-steps/s",
                "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": 24 * n, "steps": len(e2e_steps),
                "api": "cpm_sim_step_host (pinned host x, p in/out each step)"}
 
@@ -277,7 +289,7 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
     phase_names = ["kick_drift", "keys_sort_reorder", "deposit", "fft_poisson", "gather", "tree_build",
                    "tree_walk_kick2", "step"]
     line = {
-        "metric": "particle-steps/s", "value": n * world * args.steps / (ms / 1e3), "unit": "particle-steps/s",
+        "metric": "particle-steps/s", "value": job_rate(n, world, args.steps, ms), "unit": "particle-steps/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (Zel'dovich ICs generated on the GPU, Philox white noise)",
