@@ -221,7 +221,10 @@ int cpm_sim_step_to(cpm_sim* sim, float a1);
 /* `Simulation::step_to(a1)` for a caller that owns the state on the host (the reference's pub
  * `positions` and `momenta`, integrator.rs:39-40): uploads x3 and p3 (caller order), runs one step
  * with the simulation's cached acceleration for the first half-kick (the reference's private
- * `accel`), and writes the new x3 and p3 back. Synchronous. */
+ * `accel`), and writes the new x3 and p3 back. Synchronous. The step runs uncaptured: the new
+ * positions are copied back on a second, library-owned stream as soon as the step has sorted
+ * them, overlapping the force computation; x3 must not be read or written by the caller until
+ * the call returns (pinned host memory gives the fastest copies). */
 int cpm_sim_step_host(cpm_sim* sim, float a1, float* x3, float* p3);
 /* Reads the state in the caller's particle order. Any pointer may be NULL. delta is n^3. */
 int cpm_sim_get_state(cpm_sim* sim, float* x3, float* p3, float* acc3, float* delta, float* a);
