@@ -120,12 +120,9 @@ void launch_deposit_fixed(const float* x3, size_t n, float mass, int mesh_n, flo
   const size_t m = (size_t)mesh_n * mesh_n * mesh_n;
   cudaMemsetAsync(mesh_fx, 0, m * sizeof(unsigned long long), s);
   if (n == 0) return;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(k_deposit_fixed, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         DEP_SMEM_CELLS * (int)sizeof(unsigned long long));
-    attr_set = true;
-  }
+  // Per device (a cheap host call, so made on every launch): a failure shows up as the launch's error.
+  cudaFuncSetAttribute(k_deposit_fixed, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       DEP_SMEM_CELLS * (int)sizeof(unsigned long long));
   const float scale = std::ldexp(1.0f, shift);
   const unsigned blocks = (unsigned)((n + DEP_CHUNK - 1) / DEP_CHUNK);
   count_launch();

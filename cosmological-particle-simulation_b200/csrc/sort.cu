@@ -319,13 +319,10 @@ cudaError_t radix_sort_pairs(uint64_t* keys, uint32_t* vals, size_t n, int bits,
   uint32_t* vb = as<uint32_t>(sc.vals_alt);
   uint32_t* hist = as<uint32_t>(sc.block_hist);
   const int passes = (bits + 7) / 8;
-  static bool smem_set = false;  // the attribute is per function; set before the first launch
-  if (!smem_set) {
-    if ((e = cudaFuncSetAttribute(k_radix_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)RS_SCATTER_SMEM)) != cudaSuccess)
-      return e;
-    smem_set = true;
-  }
+  // The attribute belongs to the current device, so it is set on every call (a cheap host call).
+  if ((e = cudaFuncSetAttribute(k_radix_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)RS_SCATTER_SMEM)) != cudaSuccess)
+    return e;
   for (int p = 0; p < passes; ++p) {
     const int shift = 8 * p;
     count_launch();
