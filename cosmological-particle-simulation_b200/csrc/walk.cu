@@ -2,23 +2,28 @@
 //
 // Traversal. One warp walks for 32 consecutive sorted particles (one per lane). The unit of work
 // is a batch: the children of one opened node (contiguous in the node arrays), with the mask of
-// the lanes that opened it. Lanes c < count load node c of the batch (centre, centre of mass,
-// link: three coalesced 16-byte loads) and publish it to shared memory; every lane in the mask
-// then applies the reference's tests (tree.rs:264-310) to each node for itself: prune when
+// the lanes that opened it. Lanes c < count copy node c's three 16-byte records (centre and half,
+// centre of mass and mass, link) into shared memory with cp.async, double-buffered: the next
+// batch's copies are in flight while the current batch is summed. Lane c also derives the node's
+// constants once for the warp (prune radius squared, (2 half)^2), and a test against the bounding
+// box of the warp's particles drops nodes that every lane would prune. Every lane in the mask then
+// applies the reference's tests (tree.rs:264-310) to each remaining node for itself: prune when
 // |min_image(centre - x)| > r_cut + sqrt(3) half; direct sum over the node's particles when its
 // octant-0 child is missing (`children[0] == NO_CHILD`, which includes leaves); else accept the
-// centre of mass when 2 half < theta |min_image(com - x)|, or open the node. Each opened node
-// becomes a new batch on a per-warp stack, tagged with the lanes that opened it; the next batch is
-// loaded into registers before the current batch's forces are summed, so its load latency is
-// hidden. A lane's set of interactions is exactly the one its own reference walk visits (every
-// decision is computed with separately rounded f32 operations and an exact minimum image; where a
-// faster form is used, the square root of the opening test, it is checked against the exact one
-// whenever the two could disagree); only the order in which a lane adds them differs.
+// centre of mass when 2 half < theta |min_image(com - x)|, or open the node, which becomes a new
+// batch on a per-warp stack tagged with the lanes that opened it. A lane's set of interactions is
+// exactly the one its own reference walk visits: every decision uses separately rounded f32
+// operations and an exact minimum image (skipped for batches whose nodes are all far from the
+// box faces, where it is the identity), and the opening test, evaluated on squares, falls back to
+// the reference's square-root form whenever the two sides are within 1e-5; only the order in
+// which a lane adds its interactions differs.
 //
-// Direct sums concatenate the sources of all direct nodes of a batch into chunks of 32 float4 in
-// shared memory. Per chunk a lane first marks the sources within r_cut of it (bit mask), then
-// evaluates the pair force only for the marked ones, so lanes do not idle on sources outside the
-// cutoff of other lanes. A lane whose direct nodes all lie far enough from the box faces
+// Direct sums concatenate the sources of all direct nodes of a batch into chunks of 32 (negated
+// positions, one array per axis, in shared memory). Per chunk a lane first marks the sources
+// within r_cut of it (bit mask; differences and squares two sources per f32x2 instruction, the
+// sums scalar so that r^2 rounds like the reference's), then evaluates the pair force only for
+// the marked ones, two per iteration in f32x2, so lanes do not idle on sources outside the cutoff
+// of other lanes. A lane whose direct nodes all lie far enough from the box faces
 // (|centre - x| + half < 0.49 L on every axis) cannot need a periodic image, and skips the image
 // test.
 //
@@ -27,9 +32,11 @@
 // function fitted on the host for each split: Chebyshev interpolation in double precision
 // (erfc from the C library), converted to a degree-12 polynomial in x in [-1, 1] and evaluated
 // by f32 Horner — about 2e-7 relative over the range of the leaf pairs (checked by
-// cpm_walk_kernel_fit_error). e^{-u^2} uses exp2f with the FMA-exact residual of u*u; r and
-// (r^2 + eps^2)^{-3/2} come from rsqrtf. Against the reference's erfcf-based S the pair force
-// differs by a few 1e-7 relative; the 1e-5 RMS parity tests cover the sum.
+// cpm_walk_kernel_fit_error). e^{-u^2} takes the FMA-exact residual of u*u; for the direct pairs
+// e^{-u^2}, r and (r^2 + eps^2)^{-3/2} come from the hardware approximations (ex2, rsqrt; about
+// 2^-22 relative), for accepted nodes from exp2f and rsqrtf. The coupling K multiplies each
+// particle's sum once at the end. Against the reference's erfcf-based S the pair force differs
+// by a few 1e-7 relative; the 1e-5 RMS parity tests cover the sum.
 #include <algorithm>
 #include <cmath>
 #include <string>
