@@ -76,12 +76,14 @@ __device__ __forceinline__ uint32_t lower_bound_digit(const uint64_t* __restrict
 }
 
 // Splits the nodes of level d. A level with more nodes than the grid has warps takes one node
-// per thread: the 8 octant sub-ranges by binary search on digit d+1. A smaller level (the top
+// per thread: the 8 octant sub-ranges by counting the digits d+1 of a small node's keys, or by
+// binary search on them in a larger one. A smaller level (the top
 // levels, and the sparse deep levels of clustered states), where a thread's searches would be
 // a long chain of dependent loads with little else in flight, takes one node per warp: nodes of
 // up to SMALL_NODE particles count the digits of all their keys (coalesced loads, a ballot per
 // octant), larger ones search the 7 boundaries with warp_lower_bound.
 constexpr uint32_t SMALL_NODE = 256;
+constexpr uint32_t SCAN_NODE = 64;  // thread path: nodes up to this size count their digits
 
 __global__ void __launch_bounds__(BUILD_THREADS) k_tree_level(int d, const uint64_t* __restrict__ keys, uint4* link,
                                                               float4* geo, uint32_t* counters, uint32_t capacity,
@@ -97,34 +99,64 @@ __global__ void __launch_bounds__(BUILD_THREADS) k_tree_level(int d, const uint6
   const int shift = 3 * (KEY_LEVELS - 1 - d);
   const uint32_t warps = gridDim.x * (BUILD_THREADS / 32);
   if (cnt > warps) {
-    for (uint32_t node = lb + blockIdx.x * BUILD_THREADS + threadIdx.x; node < level_end;
-         node += gridDim.x * BUILD_THREADS) {
-      const uint4 L = link[node];
+    // Thread per node; each warp allocates the children of its 32 nodes with one atomic (an
+    // atomic per node on the level's single counter serialises wide levels).
+    for (uint32_t base = lb + blockIdx.x * BUILD_THREADS + (threadIdx.x & ~31u); base < level_end;
+         base += gridDim.x * BUILD_THREADS) {
+      const uint32_t node = base + (uint32_t)lane;
+      const bool valid = node < level_end;
+      const uint4 L = valid ? link[node] : make_uint4(0u, 0u, 0u, 0u);
       const uint32_t s = L.x, e = L.y, c = e - s;
-      if (c <= (uint32_t)LEAF_SIZE || d >= MAX_DEPTH) {
-        link[node] = make_uint4(s, e, 0u, (uint32_t)d << 8);
-        continue;
-      }
-      if (d >= KEY_LEVELS) {
-        atomicAdd(&counters[CNT_DEPTH_LIMIT], 1u);
-        link[node] = make_uint4(s, e, 0u, (uint32_t)d << 8);
-        continue;
+      bool split = false;
+      if (valid) {
+        if (c <= (uint32_t)LEAF_SIZE || d >= MAX_DEPTH) {
+          link[node] = make_uint4(s, e, 0u, (uint32_t)d << 8);
+        } else if (d >= KEY_LEVELS) {
+          atomicAdd(&counters[CNT_DEPTH_LIMIT], 1u);
+          link[node] = make_uint4(s, e, 0u, (uint32_t)d << 8);
+        } else {
+          split = true;
+        }
       }
       uint32_t b[9];
       b[0] = s;
       b[8] = e;
-      uint32_t lo = s;
-#pragma unroll
-      for (uint32_t o = 1; o < 8; ++o) {
-        lo = lower_bound_digit(keys, lo, e, o, shift);
-        b[o] = lo;
-      }
       uint32_t mask = 0;
+      if (split) {
+        if (c <= SCAN_NODE) {
+          // Small node: read its keys in order and count each digit (eight 8-bit counters in
+          // one word); a few sectors instead of the scattered probes of seven binary searches.
+          unsigned long long counts = 0ull;
+          for (uint32_t i = s; i < e; ++i) counts += 1ull << (8u * digit_at(__ldg(keys + i), shift));
 #pragma unroll
-      for (int o = 0; o < 8; ++o)
-        if (b[o + 1] > b[o]) mask |= 1u << o;
+          for (int o = 1; o < 8; ++o) b[o] = b[o - 1] + (uint32_t)((counts >> (8 * (o - 1))) & 0xFFull);
+        } else {
+          uint32_t lo = s;
+#pragma unroll
+          for (uint32_t o = 1; o < 8; ++o) {
+            lo = lower_bound_digit(keys, lo, e, o, shift);
+            b[o] = lo;
+          }
+        }
+#pragma unroll
+        for (int o = 0; o < 8; ++o)
+          if (b[o + 1] > b[o]) mask |= 1u << o;
+      }
+      // Children of the warp's nodes: an inclusive scan of their counts, one atomic by lane 31.
       const uint32_t nch = (uint32_t)__popc(mask);
-      const uint32_t first = next_base + atomicAdd(&counters[d + 1], nch);
+      uint32_t incl = nch;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += y;
+      }
+      uint32_t wbase = 0;
+      if (lane == 31 && incl > 0u) wbase = atomicAdd(&counters[d + 1], incl);
+      wbase = __shfl_sync(FULL, wbase, 31);
+      const uint32_t any_split = __ballot_sync(FULL, split);
+      if (lane == 0 && any_split != 0u) atomicMax(&counters[CNT_MAX_DEPTH], (uint32_t)(d + 1));
+      if (!split) continue;
+      const uint32_t first = next_base + wbase + incl - nch;
       if (first + nch > capacity) {
         dev_fail(st, DEV_NODE_CAPACITY, (int)(first + nch));
         link[node] = make_uint4(s, e, 0u, (uint32_t)d << 8);
@@ -142,7 +174,6 @@ __global__ void __launch_bounds__(BUILD_THREADS) k_tree_level(int d, const uint6
                                  __fadd_rn(G.z, (o & 4) ? q : -q), q);
       }
       link[node] = make_uint4(s, e, first, mask | ((uint32_t)d << 8));
-      atomicMax(&counters[CNT_MAX_DEPTH], (uint32_t)(d + 1));
     }
     return;
   }
