@@ -36,7 +36,7 @@ sys.path.insert(0, str(ROOT))
 PKG = "cosmological-particle-simulation_b200"
 
 WORKLOADS = {
-    # BASELINE configuration at scale: 256^3 particles, 512^3 mesh, 256 Mpc/h, seed 7, 128 steps.
+    # the headline workload: 256^3 particles, 512^3 mesh, 256 Mpc/h, seed 7, 128 steps to z = 0.
     "treepm-256": dict(n_side=256, mesh=512, box=256.0, seed=7, steps_total=128),
     # the reference's CPU-runnable case: 32^3 particles, 64^3 mesh, 64 Mpc/h, seed 42, 64 steps.
     "treepm-32": dict(n_side=32, mesh=64, box=64.0, seed=42, steps_total=64),
