@@ -195,6 +195,7 @@ constexpr int next_radix() {
   return L % 8 == 0 ? 8 : (L % 4 == 0 ? 4 : (L % 2 == 0 ? 2 : (L % 3 == 0 ? 3 : 5)));
 }
 constexpr bool smooth235(int n) {
+  if (n <= 0) return false;
   while (n % 2 == 0) n /= 2;
   while (n % 3 == 0) n /= 3;
   while (n % 5 == 0) n /= 5;
