@@ -1,4 +1,5 @@
-"""The multi-GPU side of bench.py on the host: two ranks over gloo on CPU (127.0.0.1).
+"""bench.py's host logic: the schedule, the PM byte count, and the multi-GPU side with two ranks
+over gloo on CPU (127.0.0.1).
 
 A run on N GPUs is N independent replicas (no data-path collective): each rank advances its own
 particles, the job's time is the slowest rank's, and the whole-job rate counts every rank's
@@ -65,3 +66,17 @@ def test_two_ranks_gloo():
     assert outs[0]["rate"] == outs[1]["rate"] == 1000 * 2 * 4 / 0.015
     # the reference arm does no work off rank 0
     assert outs[1]["ref_is_none"]
+
+
+def test_schedule_and_pm_bytes():
+    """The step schedule is uniform in ln a from the initial a and reaches a = 1 on its last step
+    (runner.rs:240); the PM byte count is the documented 36N + 64M."""
+    import math
+    sys.path.insert(0, str(ROOT))
+    import bench
+    a = bench.schedule(128, 128)
+    assert len(a) == 128 and abs(a[-1] - 1.0) < 1e-6
+    r = [math.log(a[i + 1] / a[i]) for i in range(len(a) - 1)]
+    assert max(r) - min(r) < 1e-5
+    assert a[0] > bench.A_INIT
+    assert bench.pm_bytes_per_step(256 ** 3, 512) == 36 * 256 ** 3 + 64 * 512 ** 3
