@@ -54,12 +54,25 @@ struct CicBase {
   float f[3];  // fractional part
 };
 
-__device__ __forceinline__ void cic_base(const float x[3], float h, CicBase& c) {
+// Cell base of one axis. The reference casts floor(s) to i64 (saturating; NaN -> 0) and wraps
+// base + d with rem_euclid (mesh.rs:36-53). Positions inside [0, L] give a base in [-1, n] and are
+// kept as is (the deposit's tiles rely on unwrapped neighbours being adjacent); any other value
+// is reduced modulo n in 64-bit arithmetic, which selects the same cells as the reference and
+// keeps every base in [-1, n], so no index or tile extent computed from it can overflow.
+__device__ __forceinline__ int cic_axis_base(float i0, int n) {
+  if (i0 >= -1.0f && i0 <= (float)n) return (int)i0;
+  const long long b = __float2ll_rz(i0);  // i0 is integral (or +-inf / NaN): saturating conversion
+  long long r = b % (long long)n;
+  if (r < 0) r += n;
+  return (int)r;
+}
+
+__device__ __forceinline__ void cic_base(const float x[3], float h, int n, CicBase& c) {
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     const float s = __fsub_rn(__fdiv_rn(x[k], h), 0.5f);
     const float i0 = floorf(s);
-    c.b[k] = (int)i0;
+    c.b[k] = cic_axis_base(i0, n);
     c.f[k] = __fsub_rn(s, i0);
   }
 }

@@ -52,7 +52,7 @@ __global__ void __launch_bounds__(DEP_THREADS) k_deposit_fixed(const float* __re
     valid[q] = i < n;
     if (valid[q]) {
       const float x[3] = {x3[3 * i], x3[3 * i + 1], x3[3 * i + 2]};
-      cic_base(x, h, cb[q]);
+      cic_base(x, h, mesh_n, cb[q]);
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
         lo[k] = min(lo[k], cb[q].b[k]);

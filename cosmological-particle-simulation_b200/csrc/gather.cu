@@ -13,7 +13,7 @@ __global__ void k_interpolate(const float* __restrict__ cells, const float* __re
   if (i >= n) return;
   const float x[3] = {x3[3 * i], x3[3 * i + 1], x3[3 * i + 2]};
   CicBase c;
-  cic_base(x, h, c);
+  cic_base(x, h, mesh_n, c);
   float sum = -0.0f;
 #pragma unroll
   for (int k = 0; k < 8; ++k) sum = __fadd_rn(sum, __fmul_rn(__ldg(cells + cic_index(c, k, mesh_n)), cic_weight(c, k)));
@@ -27,7 +27,7 @@ __global__ void k_interpolate3(const float* __restrict__ gx, const float* __rest
   if (i >= n) return;
   const float x[3] = {x3[3 * i], x3[3 * i + 1], x3[3 * i + 2]};
   CicBase c;
-  cic_base(x, h, c);
+  cic_base(x, h, mesh_n, c);
   float sx = -0.0f, sy = -0.0f, sz = -0.0f;
 #pragma unroll
   for (int k = 0; k < 8; ++k) {

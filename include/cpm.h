@@ -79,16 +79,18 @@ int cpm_ctx_destroy(cpm_ctx* ctx);
  * depend on particle order and is the exactly-rounded sum of the reference's f32 weights. */
 int cpm_mesh_deposit(cpm_ctx* ctx, const float* x3, size_t n, float mass, float* cells_out);
 
-/* No counterpart in the reference. A variant of cpm_mesh_deposit for callers that cannot call
- * cudaMalloc — code running while a CUDA stream is captured into a graph, or programs whose device
- * memory belongs to their own allocator. Positions (x3_dev, AoS [n][3]) and the output mesh
- * (cells_dev, n_mesh^3) are device pointers; the work is enqueued on `stream` (a cudaStream_t, NULL
- * for the default stream) and the call returns without waiting. The only scratch is a static
- * device array of 64^3 u64 cells (2 MiB per GPU, kept until exit): n_mesh above 64 returns
- * CPM_E_CAPACITY. Nothing is allocated. The first call on each device looks up the array's address
- * (cudaGetSymbolAddress): make it before any stream capture. All calls on a device share the array
- * (cleared by every call); calls that overlap on the GPU race on it. Results equal
- * cpm_mesh_deposit's. */
+/* No counterpart in the reference. A variant of cpm_mesh_deposit for callers that cannot let a
+ * library call cudaMalloc: programs whose device memory belongs to their own allocator or pool, or
+ * loops in which an allocation's implicit device synchronisation would stall other streams.
+ * Positions (x3_dev, AoS [n][3]) and the output mesh (cells_dev, n_mesh^3) are device pointers; the
+ * work is enqueued on `stream` (a cudaStream_t, NULL for the default stream) and the call returns
+ * without waiting. The only scratch is a static device array of 64^3 u64 cells plus a status word
+ * (2 MiB per GPU, kept until exit): n_mesh above 64 returns CPM_E_CAPACITY. Nothing is allocated.
+ * The first call on each device looks up the arrays' addresses (cudaGetSymbolAddress); make it
+ * before any stream capture. All calls on a device share the arrays (cleared by every call); calls
+ * that overlap on the GPU race on them. For finite positions the result equals cpm_mesh_deposit's;
+ * a NaN or infinite coordinate (which cpm_mesh_deposit reports as CPM_E_NONFINITE) sets every
+ * output cell to NaN, visible once the stream has synchronised. */
 int cpm_mesh_deposit_noalloc(const float* x3_dev, size_t n, int n_mesh, float box_size, float mass, float* cells_dev,
                              void* stream);
 

@@ -608,8 +608,24 @@ void drift(float* x3, const float* p3, size_t n, float factor, float box) {
 // poisson.rs:33-88
 // ---------------------------------------------------------------------------------------------
 
+// Per-axis 1 / sinc^4(pi m / n) (the CIC window of deposit and gather, squared), built in double and
+// rounded to f32. No counterpart in the reference, which does not deconvolve (poisson.rs:52-74); this
+// is the factor of the library's optional deconvolved Green's function.
+std::vector<float> cic_deconvolution_table(int n) {
+  std::vector<float> dc((size_t)n);
+  for (int i = 0; i < n; ++i) {
+    const int m = i <= n / 2 ? i : i - n;
+    const double x = 3.14159265358979323846 * (double)m / (double)n;
+    const double s = m == 0 ? 1.0 : std::sin(x) / x;
+    dc[(size_t)i] = (float)(1.0 / (s * s * s * s));
+  }
+  return dc;
+}
+
+// poisson.rs:33-88; with `deconvolve`, the Green's function of each mode is multiplied by
+// (d[ix] * d[iy]) * d[iz] from cic_deconvolution_table (f32 products in that order).
 void poisson_accel(int n_, float box, const float* delta, float omega_m, float a, float r_split, float* gx,
-                   float* gy, float* gz) {
+                   float* gy, float* gz, int deconvolve = 0) {
   const size_t n = (size_t)n_;
   const size_t n3 = n * n * n;
   std::vector<cpx<float>> delta_k(n3);
@@ -617,6 +633,7 @@ void poisson_accel(int n_, float box, const float* delta, float omega_m, float a
   fft3<float>(n_, delta_k.data(), 0);
 
   const float prefactor = 1.5f * omega_m / a;
+  const std::vector<float> dc = deconvolve ? cic_deconvolution_table(n_) : std::vector<float>();
   std::vector<cpx<float>> accel_k[3];
   for (int ax = 0; ax < 3; ++ax) accel_k[ax].assign(n3, cpx<float>{0.0f, 0.0f});
   for (size_t ix = 0; ix < n; ++ix)
@@ -628,7 +645,8 @@ void poisson_accel(int n_, float box, const float* delta, float omega_m, float a
         for (int q = 0; q < 3; ++q) k2 += k[q] * k[q];
         if (k2 == 0.0f) continue;
         const float filter = std::exp(-k2 * r_split * r_split);
-        const float sc = -prefactor / k2 * filter;
+        float sc = -prefactor / k2 * filter;
+        if (deconvolve) sc = sc * ((dc[ix] * dc[iy]) * dc[iz]);
         const cpx<float> phi = {delta_k[idx].re * sc, delta_k[idx].im * sc};
         for (int ax = 0; ax < 3; ++ax) accel_k[ax][idx] = cmul(phi, cpx<float>{0.0f, -k[ax]});
       }
@@ -823,6 +841,11 @@ float orc_wavenumber(size_t i, size_t n, float box) { return wavenumber(i, n, bo
 void orc_poisson_accel(int n, float box, const float* delta, float omega_m, float a, float r_split, float* gx,
                        float* gy, float* gz) {
   poisson_accel(n, box, delta, omega_m, a, r_split, gx, gy, gz);
+}
+
+void orc_poisson_accel_deconvolved(int n, float box, const float* delta, float omega_m, float a, float r_split,
+                                   float* gx, float* gy, float* gz) {
+  poisson_accel(n, box, delta, omega_m, a, r_split, gx, gy, gz, 1);
 }
 
 // tree.rs:40-50
@@ -1106,7 +1129,7 @@ void orc_sim_last_timings(const orc_sim* s, double* t6) {
 
 void orc_step_sample(const orc_cosmology* c, float box, int mesh_n, const float* x3, const float* p3,
                      const float* acc3, size_t n, float a0, float a1, const orc_split* split,
-                     const uint32_t* subset, size_t m, int threads, double* t7) {
+                     const uint32_t* subset, size_t m, int threads, double* t7, float* acc_subset) {
 #ifdef _OPENMP
   if (threads > 0) omp_set_num_threads(threads);
 #else
@@ -1152,6 +1175,9 @@ void orc_step_sample(const orc_cosmology* c, float box, int mesh_n, const float*
     }
     t6 = now_s();
   }
+  if (acc_subset)  // the force evaluated at a1 for the sampled particles (outside the timed phases)
+    for (size_t t = 0; t < m; ++t)
+      for (int q = 0; q < 3; ++q) acc_subset[3 * t + q] = acc[3 * (size_t)subset[t] + q];
   const float k2 = kick_factor(*c, am, a1);
   kick(p.data(), acc.data(), n, k2);
   const double t7e = now_s();

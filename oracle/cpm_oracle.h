@@ -53,7 +53,11 @@ void orc_fft3_f64(int n, double* data, int inverse);                           /
 
 /* poisson.rs */
 void orc_poisson_accel(int n, float box, const float* delta, float omega_m, float a, float r_split,
-                       float* gx, float* gy, float* gz);                       /* :33-88 */
+                       float* gx, float* gy, float* gz);
+/* orc_poisson_accel with the Green's function divided by the CIC window squared (the library's
+ * CPM_SIM_DECONVOLVE; the reference has no deconvolution). */
+void orc_poisson_accel_deconvolved(int n, float box, const float* delta, float omega_m, float a, float r_split,
+                                   float* gx, float* gy, float* gz);                       /* :33-88 */
 
 /* tree.rs */
 orc_split orc_split_with(float box, size_t mesh_n, size_t pps, float soft_scale, float theta); /* :40-50 */
@@ -112,7 +116,8 @@ void orc_sim_last_timings(const orc_sim* s, double* t6);
  * subset, second kick. `threads` > 0 sets the OpenMP thread count. */
 void orc_step_sample(const orc_cosmology* c, float box, int mesh_n, const float* x3, const float* p3,
                      const float* acc3, size_t n, float a0, float a1, const orc_split* split,
-                     const uint32_t* subset, size_t m, int threads, double* t7);
+                     const uint32_t* subset, size_t m, int threads, double* t7,
+                     float* acc_subset);
 
 /* ics.rs */
 float orc_power(const orc_cosmology* c, const orc_pspec* ps, float k);           /* :27-33 */

@@ -68,6 +68,7 @@ def lib() -> C.CDLL:
         "orc_fft3_f64": (None, [i, f64p, i]),
         "orc_wavenumber": (fl, [sz, sz, fl]),
         "orc_poisson_accel": (None, [i, fl, f32p, fl, fl, fl, f32p, f32p, f32p]),
+        "orc_poisson_accel_deconvolved": (None, [i, fl, f32p, fl, fl, fl, f32p, f32p, f32p]),
         "orc_split_with": (Split, [fl, sz, sz, fl, fl]),
         "orc_short_range_factor": (fl, [fl, fl]),
         "orc_tree_accelerations": (None, [f32p, sz, fl, C.POINTER(Split), fl, f32p]),
@@ -106,7 +107,7 @@ def lib() -> C.CDLL:
         "orc64_accelerations": (None, [f32p, sz, C.c_double, i, C.c_double, C.c_double, C.c_void_p, C.c_double,
                                        u32p, sz, f64p]),
         "orc_step_sample": (None, [C.POINTER(Cosmology), fl, i, f32p, f32p, f32p, sz, fl, fl, C.c_void_p, u32p, sz,
-                                   i, f64p]),
+                                   i, f64p, C.c_void_p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -195,10 +196,13 @@ def wavenumber(i: int, n: int, box: float) -> float:
     return lib().orc_wavenumber(i, n, box)
 
 
-def poisson_accel(n: int, box: float, delta, omega_m: float, a: float, r_split: float):
+def poisson_accel(n: int, box: float, delta, omega_m: float, a: float, r_split: float, deconvolve: bool = False):
+    """poisson.rs:33-88; `deconvolve` divides the Green's function by the CIC window squared (no
+    counterpart in the reference: the library's CPM_SIM_DECONVOLVE)."""
     d = _f32(delta).ravel()
     g = [np.empty(n ** 3, np.float32) for _ in range(3)]
-    lib().orc_poisson_accel(n, box, d, omega_m, a, r_split, g[0], g[1], g[2])
+    fn = lib().orc_poisson_accel_deconvolved if deconvolve else lib().orc_poisson_accel
+    fn(n, box, d, omega_m, a, r_split, g[0], g[1], g[2])
     return g
 
 
@@ -438,16 +442,18 @@ def num_threads() -> int:
 
 
 def step_sample(c: Cosmology, box: float, mesh_n: int, x, p, acc, a0: float, a1: float, split: Split | None,
-                subset, threads: int = 0) -> np.ndarray:
+                subset, threads: int = 0, want_acc: bool = False):
     """Seconds of each phase of one reference KDK step on (x, p, acc); the walk runs for `subset` only.
-    Returns [kick+drift, deposit, poisson, gather, tree build, walk(subset), second kick]."""
+    Returns [kick+drift, deposit, poisson, gather, tree build, walk(subset), second kick], and with
+    `want_acc` also the force at a1 (PM + tree) of the subset particles, shape (len(subset), 3)."""
     x, p, acc = _f32(x), _f32(p), _f32(acc)
     sub = np.ascontiguousarray(subset, dtype=np.uint32)
     t = np.zeros(7, np.float64)
+    out = np.empty((len(sub), 3), np.float32) if want_acc else None
     lib().orc_step_sample(C.byref(c), box, mesh_n, x, p, acc, len(x), a0, a1,
                           C.cast(C.pointer(split), C.c_void_p) if split is not None else None, sub, len(sub),
-                          threads, t)
-    return t
+                          threads, t, out.ctypes.data if want_acc else None)
+    return (t, out) if want_acc else t
 
 
 os.environ.setdefault("OMP_PROC_BIND", "false")

@@ -1,0 +1,73 @@
+"""Configuration 1 run end to end: 32^3 particles, 64^3 mesh, L = 64 Mpc/h, Zel'dovich ICs at z = 49
+from seed 42 (Omega_m 0.3, Omega_L 0.7, h 0.7, sigma8 0.8, n_s 0.96), r_s = 1.25 cells, r_cut = 4.5 r_s,
+theta = 0.5, softening 1/30 of the mean spacing, 64 KDK steps uniform in ln a to z = 0
+(integrator.rs:174-186 steps on the runner.rs:240 schedule), on the GPU and on the oracle from the
+same ICs. The matter P(k) of both runs (the oracle's FP64 estimator on each run's positions) is
+compared shell by shell for k <= k_Nyq/2 (shells 1..16).
+
+N-body trajectories are chaotic: two oracle runs whose ICs differ by one ulp already differ in P(k)
+by 2e-7 at z = 18, 9e-5 at z = 1.7, 8e-4 at z = 0.6 and 1e-2 at z = 0 near k_Nyq/2 (measured with
+this configuration). So the 0.1 % bar is asserted at every checkpoint down to z = 0.6 for all
+shells, and at z = 0 for the shells where the oracle's own one-ulp envelope stays below it; the
+other z = 0 shells must stay within three times that envelope (and 0.1 %, whichever is larger).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+CHECKPOINTS = (16, 32, 40, 48, 56, 64)
+PK_RTOL = 1e-3
+
+
+def _config1(orc):
+    c = orc.cosmology(0.0, 0.3, 0.7, 70.0)
+    ps = orc.power_normalized(c, 0.96, 0.8, 8.0)
+    x, p = orc.zeldovich(32, 64.0, c, ps, 0.02, 42)
+    split = orc.split_with(64.0, 64, 32, 1.0 / 30.0, 0.5)
+    return c, x, p, split, orc.ln_a_schedule(0.02, 1.0, 64)
+
+
+def _oracle_run(orc, c, x, p, split, sched):
+    sim = orc.Simulation(c, 64.0, 64, x, p, 0.02, split)
+    out = {}
+    for i, a in enumerate(sched, 1):
+        sim.step_to(a)
+        if i in CHECKPOINTS:
+            out[i] = sim.state()["x"]
+    sim.close()
+    return out
+
+
+def test_config1_final_power_spectrum_matches_oracle(cpm, orc):
+    c, x, p, split, sched = _config1(orc)
+    gpu = cpm.Simulation(cpm.Cosmology(c.omega_r, c.omega_m, c.omega_l, c.h0), 64.0, 64, x, p, 0.02,
+                         cpm.ForceSplit(split.r_split, split.r_cut, split.softening, split.theta))
+    got = {}
+    for i, a in enumerate(sched, 1):
+        gpu.step_to(a)
+        if i in CHECKPOINTS:
+            got[i] = gpu.state()["x"]
+    gpu.close()
+    ref = _oracle_run(orc, c, x, p, split, sched)
+    # the chaotic envelope: the oracle again from ICs moved by one ulp (alternating direction)
+    xp = x.copy()
+    flat = xp.reshape(-1)
+    flat[0::2] = np.nextafter(flat[0::2], np.float32(np.inf))
+    flat[1::2] = np.nextafter(flat[1::2], np.float32(-np.inf))
+    env = _oracle_run(orc, c, np.mod(xp, np.float32(64.0)).astype(np.float32), p, split, sched)
+
+    for i in CHECKPOINTS:
+        _, p_g, c_g = orc.power_spectrum(got[i], 64.0, 64, 16)
+        _, p_o, c_o = orc.power_spectrum(ref[i], 64.0, 64, 16)
+        _, p_e, _ = orc.power_spectrum(env[i], 64.0, 64, 16)
+        np.testing.assert_array_equal(c_g, c_o)
+        rel = np.abs(p_g / p_o - 1.0)
+        envelope = np.abs(p_e / p_o - 1.0)
+        if i < 64:
+            assert rel.max() < PK_RTOL, (i, rel.max(), int(np.argmax(rel)) + 1)
+        else:
+            quiet = envelope < PK_RTOL / 3
+            assert quiet[:4].all(), envelope  # the largest scales are not chaotic at z = 0
+            assert rel[quiet].max() < PK_RTOL, (rel, envelope)
+            assert np.all(rel <= np.maximum(PK_RTOL, 3.0 * envelope)), (rel, envelope)

@@ -96,6 +96,23 @@ def test_interpolate_bit_exact(cpm, orc):
     assert np.array_equal(got, orc.interpolate_many(16, 1.0, cells, x))
 
 
+def test_far_positions_wrap_like_the_reference(cpm, orc):
+    """Finite positions many boxes outside [0, L) (the reference accepts any finite position: floor
+    cast to i64, then rem_euclid, mesh.rs:36-53) in the deposit and the gather, including +-inf-free
+    values beyond 2^31 cells of opposite sign in one 1024-particle chunk."""
+    x = orc.scattered_mesh(6000, 16.0)
+    far = np.array([1e12, -3.7e9, 5.0e15, -2.5e11, 16.0, -16.5, 123456.789, -0.0, 2.2e9, -2.2e9], np.float32)
+    x.reshape(-1)[:3 * len(far)] = np.resize(far, 3 * len(far))
+    x[np.random.default_rng(5).integers(0, len(x), 64)] *= np.float32(-1e7)
+    m = cpm.Mesh(16, 16.0)
+    m.deposit(x, 1.0)
+    ref = orc.deposit_f64(16, 16.0, x, 1.0)
+    assert np.max(np.abs(m.cells - ref) / np.maximum(np.abs(ref), 1e-30)) < 1e-6
+    cells = np.random.default_rng(2).standard_normal(16 ** 3).astype(np.float32)
+    got = cpm.Mesh(16, 16.0, cells).interpolate_many(x)
+    assert np.array_equal(got, orc.interpolate_many(16, 16.0, cells, x))
+
+
 def test_interpolate_reference_cases(cpm):
     """mesh.rs:164-183 on the GPU."""
     from oracle import scattered_mesh
@@ -109,9 +126,11 @@ def test_interpolate_reference_cases(cpm):
 
 # ------------------------------------------------------------------ FFT / Poisson
 
-@pytest.mark.parametrize("n", [4, 8, 16, 32, 48, 64, 80, 96, 128, 160])
+@pytest.mark.parametrize("n", [4, 8, 16, 32, 48, 64, 80, 96, 128, 160, 192, 256, 320, 384, 512])
 @pytest.mark.parametrize("inverse", [False, True])
 def test_fft3_matches_oracle(cpm, orc, n, inverse):
+    """Every compiled length up to the 512-point transform of the 512^3 headline mesh (1024-thread
+    CTAs) against the oracle's FFT (fft.rs:40-72); numpy's FP64 FFT as a second reference to 256."""
     rng = np.random.default_rng(n)
     data = (rng.standard_normal(n ** 3) + 1j * rng.standard_normal(n ** 3)).astype(np.complex64)
     ref = orc.fft3(data.copy(), inverse)
@@ -119,9 +138,49 @@ def test_fft3_matches_oracle(cpm, orc, n, inverse):
     f = cpm.Fft3(n)
     (f.inverse if inverse else f.forward)(got)
     assert rel_rms(got.view(np.float32), ref.view(np.float32)) < 1e-5
-    exact = (np.fft.ifftn(data.reshape(n, n, n).astype(np.complex128)) * n ** 3 if inverse
-             else np.fft.fftn(data.reshape(n, n, n).astype(np.complex128))).ravel()
-    assert rel_rms(got.view(np.float32), exact.astype(np.complex64).view(np.float32)) < 1e-5
+    del ref
+    if n <= 256:
+        exact = (np.fft.ifftn(data.reshape(n, n, n).astype(np.complex128)) * n ** 3 if inverse
+                 else np.fft.fftn(data.reshape(n, n, n).astype(np.complex128))).ravel()
+        assert rel_rms(got.view(np.float32), exact.astype(np.complex64).view(np.float32)) < 1e-5
+
+
+def _dft_mode(field: np.ndarray, k: tuple) -> complex:
+    """One output mode of the unnormalised forward 3D DFT, summed in FP64 axis by axis."""
+    n = field.shape[0]
+    e = [np.exp(-2j * np.pi * ki * np.arange(n) / n) for ki in k]
+    total = 0j
+    for x0 in range(0, n, 32):  # x slabs keep the FP64 temporaries at 0.5 GB
+        s = field[x0:x0 + 32].astype(np.complex128) @ e[2]
+        total += complex((s @ e[1]) @ e[0][x0:x0 + 32])
+    return total
+
+
+def test_fft3_random_field_at_1024(cpm):
+    """A random complex field on the 1024^3 mesh (8 GB): forward then inverse returns n^3 times
+    the input, the forward obeys Parseval, and five modes equal their FP64 DFT sums."""
+    n = 1024
+    rng = np.random.default_rng(1024)
+    data = np.empty(n ** 3, np.complex64)
+    step = n ** 3 // 16
+    for i in range(16):
+        blk = slice(i * step, (i + 1) * step)
+        data.real[blk] = rng.standard_normal(step, dtype=np.float32)
+        data.imag[blk] = rng.standard_normal(step, dtype=np.float32)
+    f = cpm.Fft3(n)
+    spec = data.copy()
+    f.forward(spec)
+    e_x = float(np.vdot(data, data).real)
+    e_k = float(np.vdot(spec, spec).real)
+    assert abs(e_k / (e_x * n ** 3) - 1.0) < 1e-5
+    cube = data.reshape(n, n, n)
+    for k in [(0, 0, 0), (1, 0, 0), (3, 511, 7), (512, 512, 512), (1000, 17, 600)]:
+        want = _dft_mode(cube, k)
+        got = complex(spec[(k[0] * n + k[1]) * n + k[2]])
+        assert abs(got - want) < 1e-5 * np.sqrt(e_k / n ** 3) * 10 + 1e-5 * abs(want), k
+    f.inverse(spec)
+    spec /= np.float32(n ** 3)
+    assert rel_rms(spec.view(np.float32), data.view(np.float32)) < 1e-5
 
 
 def test_fft3_rejects_mesh_mismatch(cpm):
@@ -135,7 +194,9 @@ def test_fft3_rejects_mesh_mismatch(cpm):
 
 
 @pytest.mark.parametrize("n,box,a,r_split", [(16, 1.0, 0.5, 0.0), (32, 64.0, 0.3, 1.25), (64, 64.0, 1.0, 1.25),
-                                             (48, 50.0, 0.7, 1.25), (96, 100.0, 1.0, 1.25)])
+                                             (48, 50.0, 0.7, 1.25), (96, 100.0, 1.0, 1.25),
+                                             (192, 128.0, 0.6, 0.625), (256, 128.0, 1.0, 0.625),
+                                             (320, 128.0, 0.8, 0.5), (512, 256.0, 1.0, 0.625)])
 def test_poisson_matches_oracle(cpm, orc, n, box, a, r_split):
     x = orc.scattered_mesh(4 * n ** 3 // 8, box)
     delta = orc.density_contrast(n, box, x)

@@ -1,5 +1,5 @@
-"""The Rust declarations written out for the reference crate name entry points
-that include/cpm.h declares, with the same number of parameters."""
+"""The Rust declarations for the reference crate's `cuda` feature (include/cpm_ffi.rs) name entry
+points that include/cpm.h declares, with the same number of parameters."""
 import re
 from pathlib import Path
 
@@ -16,10 +16,10 @@ def _c_decls() -> dict:
 
 
 def _rust_decls() -> dict:
-    text = (ROOT / "INTEGRATION.md").read_text()
+    text = re.sub(r"//[^\n]*", "", (ROOT / "include" / "cpm_ffi.rs").read_text())
     out = {}
     for m in re.finditer(r"pub fn (cpm_[a-z0-9_]+)\(([^)]*)\)", text):
-        args = m.group(2).strip()
+        args = m.group(2).strip().rstrip(",")
         out[m.group(1)] = 0 if not args else args.count(",") + 1
     return out
 
@@ -30,3 +30,10 @@ def test_rust_declarations_match_the_c_header():
     for name, nargs in rust.items():
         assert name in c, name
         assert nargs == c[name], (name, nargs, c[name])
+
+
+def test_rust_file_declares_every_reference_facing_entry_point():
+    rust = _rust_decls()
+    for name in ("cpm_mesh_deposit", "cpm_mesh_interpolate3", "cpm_fft3", "cpm_poisson_accel", "cpm_tree_accel",
+                 "cpm_sim_create", "cpm_sim_step_host", "cpm_sim_get_state", "cpm_sim_destroy"):
+        assert name in rust, name
