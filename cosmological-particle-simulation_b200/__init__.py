@@ -8,5 +8,6 @@ from ._native import CpmError, Cosmology, exported_symbols, lib  # noqa: F401
 from .api import (Context, Fft3, ForceSplit, Mesh, PoissonSolver, Simulation, density_contrast, density_grid,  # noqa: F401
                   interpolate3, ln_a_schedule, octant_keys, power_spectrum, short_range_factor, tree_accelerations,
                   wavenumber, zeldovich)
+from .learned import ShortRangeNet  # noqa: F401
 
 __version__ = "0.1.0"

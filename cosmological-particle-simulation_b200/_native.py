@@ -118,6 +118,17 @@ def lib() -> C.CDLL:
         "cpm_sim_snapshot": (i, [vp, vp, vp, vp, vp, C.POINTER(i), C.POINTER(fl)]),
         "cpm_density_grid": (i, [vp, vp, i, vp, C.POINTER(i)]),
         "cpm_sim_destroy": (i, [vp]),
+        "cpm_net_weight_count": (i, []),
+        "cpm_net_create": (i, [i, C.POINTER(vp)]),
+        "cpm_net_destroy": (i, [vp]),
+        "cpm_net_last_error": (C.c_char_p, [vp]),
+        "cpm_net_set_weights": (i, [vp, vp]),
+        "cpm_net_get_weights": (i, [vp, vp]),
+        "cpm_net_get_grads": (i, [vp, vp]),
+        "cpm_net_forward": (i, [vp, vp, fl, fl, vp, vp]),
+        "cpm_net_backward": (i, [vp, vp, fl, vp]),
+        "cpm_net_activations": (i, [vp, i, vp, vp]),
+        "cpm_net_train_step": (i, [vp, vp, fl, vp, vp, vp, sz, fl, fl, fl, C.POINTER(C.c_double), vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

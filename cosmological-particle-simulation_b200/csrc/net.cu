@@ -1,0 +1,928 @@
+// net.cu — the learned short-range force: a 3-layer convolutional net on the CIC density mesh,
+// with hand-written BF16 tcgen05 implicit-GEMM kernels for inference and training.
+//
+// The reference computes the short-range force with a Barnes-Hut walk (tree.rs:264-310); it has no
+// learned component. Here a net maps the density contrast delta on the PM mesh to a 3-channel
+// short-range acceleration field, which the simulation gathers to particles with the CIC stencil
+// (mesh.rs:72-77) wherever the particle's density contrast is below a threshold; the tree walk
+// stays for the particles above it.
+//
+// Network: three 3x3x3 periodic convolutions without biases, 16 channels, leaky ReLU (slope 1/8)
+// after the first two:   y = W3 * lrelu(W2 * lrelu(W1 * (s_in delta))),   F = s_out y.
+// Without biases and with a positively homogeneous activation the net is homogeneous of degree one
+// (F(lambda delta) = lambda F(delta) for lambda > 0, F(0) = 0), like the linear map from density to
+// force it approximates. Convolution here is out[v] = sum_t W[t] in[v + t], t in {-1,0,1}^3,
+// tap index t = (dx+1)*9 + (dy+1)*3 + (dz+1).
+//
+// Layout of every activation tensor (BF16): [x][y][chunk 2][ZP][8], ZP = n + 8. Voxel z of row
+// (x, y) sits at padded index z + 1; index 0 holds a copy of z = n - 1 and index n + 1 a copy of
+// z = 0 (periodic halo), so one TMA box of a row covers the tile and its z neighbours. Channels
+// 0-7 form chunk 0, 8-15 chunk 1, each chunk a contiguous plane of 16-byte voxels. In shared memory
+// a row box lands as [chunk][136 voxels][8 channels]: the K-major canonical layout of an MMA A
+// operand (core matrix = 8 voxels x 8 channels, SBO = 128 B, LBO = one chunk plane), and a shift
+// of the tile by one voxel along z is a shift of the descriptor's start address by 16 bytes. So a
+// 3^3 convolution over a tile of 128 voxels is 9 row loads and 27 MMAs of 128 x 16 x 16 (implicit
+// GEMM: no im2col copy).
+//
+// Kernels (warp-specialised, persistent over tiles of 128 voxels of one row):
+//   k_conv3       forward convolution (also the data gradient, with transposed and flipped weights):
+//                 warp 0 = TMA producer, warp 1 = MMA issuer (one thread), warps 2-5 = epilogue
+//                 (TMEM -> registers, leaky ReLU or the activation-derivative gate, BF16 or FP32 out)
+//   k_conv3_wgrad weight gradient dW[t][co][ci] = sum_v dOut[v][co] In[v + t][ci]: 9 gradient rows
+//                 (x - dx, y - dy) and one input row per tile, both MN-major operands; M = 128 =
+//                 8 rows x 16 output channels, N = 32 = 4 z shifts x 8 input channels, K = voxels;
+//                 accumulated in TMEM over all tiles of the CTA, reduced with atomics at the end
+// plus elementwise kernels (input conversion, field gather and loss gradient, Adam).
+#include <cuda.h>
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "cpm_host.h"
+#include "cpm_internal.cuh"
+#include "umma.cuh"
+
+namespace cpm {
+
+constexpr int NET_C = 16;
+constexpr int NET_TAPS = 27;
+constexpr int NET_LAYERS = 3;
+constexpr int NET_OUT = 3;
+constexpr float NET_SLOPE = 0.125f;
+constexpr int NET_WEIGHTS = NET_LAYERS * NET_TAPS * NET_C * NET_C;  // master weights [3][27][16][16]
+
+constexpr int TILE_M = 128;                     // voxels per tile
+constexpr int ROW_BOX = 136;                    // voxels per input row load (tile, halo, rounding)
+constexpr int PLANE_BYTES = ROW_BOX * 16;       // one 8-channel chunk plane of a loaded row
+constexpr int ROW_BYTES = 2 * PLANE_BYTES;      // 4352
+constexpr int GRAD_PLANE = TILE_M * 16;         // a gradient row (weight-gradient kernel): 128 voxels
+constexpr int GRAD_ROW = 2 * GRAD_PLANE;        // 4096
+constexpr int W_TAP_BYTES = 2 * NET_C * 16;     // [chunk][cout 16][8 cin] bf16 = 512
+constexpr int W_BYTES = NET_TAPS * W_TAP_BYTES;  // 13824
+constexpr int CONV_THREADS = 192;               // 6 warps
+constexpr int CONV_STAGES = 3;
+constexpr int WG_STAGES = 2;
+constexpr long long WAIT_BUDGET = 1ll << 32;    // clock cycles (about 2 s) before a wait gives up
+
+enum NetError : int { NET_OK = 0, NET_TIMEOUT = 7 };
+
+// ---------------------------------------------------------------------------------------------
+// Device helpers
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ float lrelu(float v) { return v > 0.0f ? v : NET_SLOPE * v; }
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<const uint32_t*>(&h);
+}
+__device__ __forceinline__ float2 unpack_bf16x2(uint32_t v) {
+  __nv_bfloat162 h;
+  *reinterpret_cast<uint32_t*>(&h) = v;
+  return __bfloat1622float2(h);
+}
+
+struct TensorGeo {
+  int n;
+  int zp;  // n + 8
+  // element offset of (x, y, chunk, padded z, 0)
+  __host__ __device__ size_t at(int x, int y, int c, int pz) const {
+    return ((((size_t)x * n + y) * 2 + c) * (size_t)zp + pz) * 8;
+  }
+};
+
+// Stores 16 channels of voxel z (0..n-1) of row (x, y) and, for z = 0 and z = n - 1, its halo copy.
+__device__ __forceinline__ void store_voxel16(__nv_bfloat16* t, const TensorGeo& g, int x, int y, int z,
+                                              const uint4& c0, const uint4& c1) {
+  *reinterpret_cast<uint4*>(t + g.at(x, y, 0, z + 1)) = c0;
+  *reinterpret_cast<uint4*>(t + g.at(x, y, 1, z + 1)) = c1;
+  if (z == 0) {
+    *reinterpret_cast<uint4*>(t + g.at(x, y, 0, g.n + 1)) = c0;
+    *reinterpret_cast<uint4*>(t + g.at(x, y, 1, g.n + 1)) = c1;
+  }
+  if (z == g.n - 1) {
+    *reinterpret_cast<uint4*>(t + g.at(x, y, 0, 0)) = c0;
+    *reinterpret_cast<uint4*>(t + g.at(x, y, 1, 0)) = c1;
+  }
+}
+
+struct ConvArgs {
+  TensorGeo g;
+  int tiles_z;
+  long long tiles;
+  const __nv_bfloat16* w;     // packed weights [27][2][16][8]
+  __nv_bfloat16* out16;       // BF16 tensor output, or null
+  float4* out_f4;             // FP32 field output [n^3] (x, y, z, 0), or null
+  const __nv_bfloat16* gate;  // multiply channel c by lrelu'(gate[v][c]) (backward), or null
+  int act;                    // apply lrelu to the output
+  float out_scale;
+  const float* out_scale_dev;  // when set, the scale is read from device memory
+  int* status;
+};
+
+// ---------------------------------------------------------------------------------------------
+// Forward convolution
+// ---------------------------------------------------------------------------------------------
+template <int NSTAGE>
+__global__ void __launch_bounds__(CONV_THREADS, 1) k_conv3(const __grid_constant__ CUtensorMap in_map, ConvArgs a) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  uint8_t* rows = smem;                                // [NSTAGE][9][ROW_BYTES]
+  uint8_t* wsm = smem + NSTAGE * 9 * ROW_BYTES;        // packed weights
+  uint64_t* bars = reinterpret_cast<uint64_t*>(wsm + W_BYTES);
+  uint64_t* full = bars;                  // [NSTAGE] rows loaded
+  uint64_t* empty = bars + NSTAGE;        // [NSTAGE] rows consumed by the MMAs
+  uint64_t* acc_full = bars + 2 * NSTAGE;      // [2] accumulator ready
+  uint64_t* acc_empty = bars + 2 * NSTAGE + 2;  // [2] accumulator read by the epilogue
+  uint64_t* done = bars + 2 * NSTAGE + 4;
+  uint32_t* tmem_sh = reinterpret_cast<uint32_t*>(bars + 2 * NSTAGE + 5);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int n = a.g.n;
+  for (int i = threadIdx.x; i < W_BYTES / 16; i += CONV_THREADS)
+    reinterpret_cast<uint4*>(wsm)[i] = __ldg(reinterpret_cast<const uint4*>(a.w) + i);
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < NSTAGE; ++s) {
+      umma::mbar_init(&full[s], 1);
+      umma::mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      umma::mbar_init(&acc_full[b], 1);
+      umma::mbar_init(&acc_empty[b], 128);
+    }
+    umma::mbar_init(done, 1);
+    umma::fence_mbar_init();
+  }
+  if (warp == 0) {
+    umma::tmem_alloc(tmem_sh, 32);
+    umma::tmem_relinquish();
+  }
+  umma::fence_proxy_async();
+  umma::tc_fence_before();
+  __syncthreads();
+  umma::tc_fence_after();
+  const uint32_t tmem = *tmem_sh;
+
+  if (warp == 0) {
+    if (lane == 0) {  // TMA producer: the 9 rows (x+dx, y+dy) of each tile
+      umma::tma_prefetch_map(&in_map);
+      int s = 0;
+      uint32_t ph = 0;
+      long long issued = 0;
+      for (long long t = blockIdx.x; t < a.tiles; t += gridDim.x) {
+        if (!umma::mbar_wait(&empty[s], ph ^ 1, WAIT_BUDGET)) {
+          atomicCAS(a.status, 0, NET_TIMEOUT);
+          break;
+        }
+        const int zt = (int)(t % a.tiles_z);
+        const long long xy = t / a.tiles_z;
+        const int y = (int)(xy % n), x = (int)(xy / n);
+        umma::mbar_arrive_expect_tx(&full[s], 9 * ROW_BYTES);
+        for (int r = 0; r < 9; ++r) {
+          const int xs = (x + r / 3 - 1 + n) % n, ys = (y + r % 3 - 1 + n) % n;
+          umma::tma_load_5d(rows + (size_t)(s * 9 + r) * ROW_BYTES, &in_map, &full[s], 0, zt * TILE_M, 0, ys, xs);
+        }
+        ++issued;
+        if (++s == NSTAGE) {
+          s = 0;
+          ph ^= 1;
+        }
+      }
+      // drain: wait until the loads still in flight have landed (they complete without a consumer)
+      for (int k = 0; k < NSTAGE && issued > 0; ++k, --issued) {
+        s = s == 0 ? NSTAGE - 1 : s - 1;
+        if (s == NSTAGE - 1) ph ^= 1;
+        umma::mbar_wait(&full[s], ph, WAIT_BUDGET);
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {  // MMA issuer
+      constexpr uint32_t IDESC = umma::idesc_bf16(TILE_M, NET_C, false, false);
+      const uint32_t w_addr = umma::smem_u32(wsm);
+      int s = 0, ab = 0;
+      uint32_t ph = 0, aph = 0;
+      for (long long t = blockIdx.x; t < a.tiles; t += gridDim.x) {
+        if (!umma::mbar_wait(&full[s], ph, WAIT_BUDGET) || !umma::mbar_wait(&acc_empty[ab], aph ^ 1, WAIT_BUDGET)) {
+          atomicCAS(a.status, 0, NET_TIMEOUT);
+          break;
+        }
+        umma::tc_fence_after();
+        const uint32_t d = tmem + (uint32_t)(ab * NET_C);
+        const uint32_t base = umma::smem_u32(rows + (size_t)s * 9 * ROW_BYTES);
+        for (int r = 0; r < 9; ++r)
+#pragma unroll
+          for (int dz = 0; dz < 3; ++dz) {
+            const uint64_t ad = umma::sdesc(base + (uint32_t)(r * ROW_BYTES + dz * 16), PLANE_BYTES, 128);
+            const uint64_t bd = umma::sdesc(w_addr + (uint32_t)((r * 3 + dz) * W_TAP_BYTES), 256, 128);
+            umma::mma_bf16(d, ad, bd, IDESC, (r | dz) != 0 ? 1u : 0u);
+          }
+        umma::mma_commit(&empty[s]);
+        umma::mma_commit(&acc_full[ab]);
+        if (++s == NSTAGE) {
+          s = 0;
+          ph ^= 1;
+        }
+        if (++ab == 2) {
+          ab = 0;
+          aph ^= 1;
+        }
+      }
+      umma::mma_commit(done);
+      umma::mbar_wait(done, 0, WAIT_BUDGET);
+    }
+  } else {  // epilogue: warps 2..5, TMEM lane quarter warp % 4
+    const int q = warp & 3;
+    const int m = q * 32 + lane;
+    int ab = 0;
+    uint32_t aph = 0;
+    const float scale = a.out_scale_dev ? *a.out_scale_dev : a.out_scale;
+    for (long long t = blockIdx.x; t < a.tiles; t += gridDim.x) {
+      if (!umma::mbar_wait(&acc_full[ab], aph, WAIT_BUDGET)) {
+        atomicCAS(a.status, 0, NET_TIMEOUT);
+        break;
+      }
+      umma::tc_fence_after();
+      uint32_t r[16];
+      umma::tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(ab * NET_C), r);
+      umma::tmem_wait_ld();
+      umma::tc_fence_before();
+      umma::mbar_arrive(&acc_empty[ab]);
+      if (++ab == 2) {
+        ab = 0;
+        aph ^= 1;
+      }
+      const int zt = (int)(t % a.tiles_z);
+      const long long xy = t / a.tiles_z;
+      const int y = (int)(xy % n), x = (int)(xy / n);
+      const int z = zt * TILE_M + m;
+      if (z >= n) continue;
+      float v[16];
+#pragma unroll
+      for (int c = 0; c < 16; ++c) v[c] = __uint_as_float(r[c]);
+      if (a.out_f4) {
+        a.out_f4[((size_t)x * n + y) * n + z] = make_float4(v[0] * scale, v[1] * scale, v[2] * scale, 0.0f);
+        continue;
+      }
+      if (a.act) {
+#pragma unroll
+        for (int c = 0; c < 16; ++c) v[c] = lrelu(v[c]);
+      }
+      if (a.gate) {
+        const uint4 g0 = *reinterpret_cast<const uint4*>(a.gate + a.g.at(x, y, 0, z + 1));
+        const uint4 g1 = *reinterpret_cast<const uint4*>(a.gate + a.g.at(x, y, 1, z + 1));
+        const uint32_t gw[8] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w};
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const float2 gv = unpack_bf16x2(gw[k]);
+          v[2 * k] *= gv.x > 0.0f ? 1.0f : NET_SLOPE;
+          v[2 * k + 1] *= gv.y > 0.0f ? 1.0f : NET_SLOPE;
+        }
+      }
+      const uint4 c0 = make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]), pack_bf16x2(v[4], v[5]),
+                                  pack_bf16x2(v[6], v[7]));
+      const uint4 c1 = make_uint4(pack_bf16x2(v[8], v[9]), pack_bf16x2(v[10], v[11]), pack_bf16x2(v[12], v[13]),
+                                  pack_bf16x2(v[14], v[15]));
+      store_voxel16(a.out16, a.g, x, y, z, c0, c1);
+    }
+  }
+  umma::tc_fence_before();
+  __syncthreads();
+  umma::tc_fence_after();
+  if (warp == 0) umma::tmem_dealloc(tmem, 32);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Weight gradient
+// ---------------------------------------------------------------------------------------------
+struct WgradArgs {
+  TensorGeo g;
+  int tiles_z;
+  long long tiles;
+  float* dw;  // [27][16 co][16 ci] FP32, accumulated with atomics
+  int* status;
+};
+
+template <int NSTAGE>
+__global__ void __launch_bounds__(CONV_THREADS, 1)
+    k_conv3_wgrad(const __grid_constant__ CUtensorMap grad_map, const __grid_constant__ CUtensorMap in_map,
+                  WgradArgs a) {
+  constexpr int STAGE_BYTES = 9 * GRAD_ROW + ROW_BYTES;
+  extern __shared__ __align__(1024) uint8_t smem[];
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + NSTAGE * STAGE_BYTES);
+  uint64_t* full = bars;
+  uint64_t* empty = bars + NSTAGE;
+  uint64_t* done = bars + 2 * NSTAGE;
+  uint32_t* tmem_sh = reinterpret_cast<uint32_t*>(bars + 2 * NSTAGE + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int n = a.g.n;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < NSTAGE; ++s) {
+      umma::mbar_init(&full[s], 1);
+      umma::mbar_init(&empty[s], 1);
+    }
+    umma::mbar_init(done, 1);
+    umma::fence_mbar_init();
+  }
+  if (warp == 0) {
+    umma::tmem_alloc(tmem_sh, 128);
+    umma::tmem_relinquish();
+  }
+  umma::tc_fence_before();
+  __syncthreads();
+  umma::tc_fence_after();
+  const uint32_t tmem = *tmem_sh;
+  bool mma_started = false;
+
+  if (warp == 0) {
+    if (lane == 0) {  // producer: gradient rows j -> (x - dx, y - dy), input row (x, y)
+      umma::tma_prefetch_map(&grad_map);
+      umma::tma_prefetch_map(&in_map);
+      int s = 0;
+      uint32_t ph = 0;
+      long long issued = 0;
+      for (long long t = blockIdx.x; t < a.tiles; t += gridDim.x) {
+        if (!umma::mbar_wait(&empty[s], ph ^ 1, WAIT_BUDGET)) {
+          atomicCAS(a.status, 0, NET_TIMEOUT);
+          break;
+        }
+        const int zt = (int)(t % a.tiles_z);
+        const long long xy = t / a.tiles_z;
+        const int y = (int)(xy % n), x = (int)(xy / n);
+        uint8_t* st = smem + (size_t)s * STAGE_BYTES;
+        umma::mbar_arrive_expect_tx(&full[s], 9 * GRAD_ROW + ROW_BYTES);
+        for (int j = 0; j < 9; ++j) {
+          const int xs = (x - (j / 3 - 1) + n) % n, ys = (y - (j % 3 - 1) + n) % n;
+          umma::tma_load_5d(st + (size_t)j * GRAD_ROW, &grad_map, &full[s], 0, zt * TILE_M + 1, 0, ys, xs);
+        }
+        umma::tma_load_5d(st + 9 * GRAD_ROW, &in_map, &full[s], 0, zt * TILE_M, 0, y, x);
+        ++issued;
+        if (++s == NSTAGE) {
+          s = 0;
+          ph ^= 1;
+        }
+      }
+      for (int k = 0; k < NSTAGE && issued > 0; ++k, --issued) {
+        s = s == 0 ? NSTAGE - 1 : s - 1;
+        if (s == NSTAGE - 1) ph ^= 1;
+        umma::mbar_wait(&full[s], ph, WAIT_BUDGET);
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {  // MMA issuer
+      constexpr uint32_t IDESC = umma::idesc_bf16(TILE_M, 32, true, true);
+      int s = 0;
+      uint32_t ph = 0;
+      for (long long t = blockIdx.x; t < a.tiles; t += gridDim.x) {
+        if (!umma::mbar_wait(&full[s], ph, WAIT_BUDGET)) {
+          atomicCAS(a.status, 0, NET_TIMEOUT);
+          break;
+        }
+        umma::tc_fence_after();
+        const int zt = (int)(t % a.tiles_z);
+        const int ksteps = min(TILE_M, n - zt * TILE_M) / 16;
+        const uint32_t gbase = umma::smem_u32(smem + (size_t)s * STAGE_BYTES);
+        const uint32_t ibase = gbase + 9 * GRAD_ROW;
+        for (int k = 0; k < ksteps; ++k)
+#pragma unroll
+          for (int mt = 0; mt < 2; ++mt) {
+            // A: rows j = mt .. mt+7, MN-major: 8 output channels per core matrix, groups (j, chunk)
+            // 2048 B apart, 8-voxel K groups 128 B apart
+            const uint64_t ad = umma::sdesc(gbase + (uint32_t)(mt * GRAD_ROW + k * 256), 128, GRAD_PLANE);
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+              // B: input chunk c; N groups = z shifts s = 0..3 (16 B apart, overlapping), K groups 128 B
+              const uint64_t bd = umma::sdesc(ibase + (uint32_t)(c * PLANE_BYTES + k * 256), 128, 16);
+              umma::mma_bf16(tmem + (uint32_t)((mt * 2 + c) * 32), ad, bd, IDESC, mma_started ? 1u : 0u);
+            }
+            if (mt == 1) mma_started = true;
+          }
+        umma::mma_commit(&empty[s]);
+        if (++s == NSTAGE) {
+          s = 0;
+          ph ^= 1;
+        }
+      }
+      umma::mma_commit(done);
+    }
+  } else {  // epilogue: after every MMA of the CTA, reduce the accumulators into dW
+    if (!umma::mbar_wait(done, 0, WAIT_BUDGET)) atomicCAS(a.status, 0, NET_TIMEOUT);
+    umma::tc_fence_after();
+    const int q = warp & 3;
+    const int m = q * 32 + lane;
+    const bool any = blockIdx.x < a.tiles;  // every CTA of the grid owns at least one tile of >= 16 voxels
+#pragma unroll 1
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll 1
+      for (int c = 0; c < 2; ++c) {
+        uint32_t r0[16], r1[16];
+        const uint32_t ta = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)((mt * 2 + c) * 32);
+        umma::tmem_ld16(ta, r0);
+        umma::tmem_ld16(ta + 16, r1);
+        umma::tmem_wait_ld();
+        const int j = mt + m / 16, co = m % 16;
+        if (!any || (mt == 1 && j != 8)) continue;
+#pragma unroll
+        for (int nn = 0; nn < 24; ++nn) {
+          const float v = __uint_as_float(nn < 16 ? r0[nn] : r1[nn - 16]);
+          const int sft = nn / 8, ci = c * 8 + (nn % 8);
+          atomicAdd(&a.dw[((j * 3 + sft) * NET_C + co) * NET_C + ci], v);
+        }
+      }
+  }
+  umma::tc_fence_before();
+  __syncthreads();
+  umma::tc_fence_after();
+  if (warp == 0) umma::tmem_dealloc(tmem, 128);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Elementwise kernels
+// ---------------------------------------------------------------------------------------------
+// Input tensor: channel 0 = in_scale * delta, other channels 0. delta from an f32 mesh or from the
+// u64 fixed-point mass mesh (delta = c / mean - 1, integrator.rs:117-126).
+__global__ void k_net_input(const float* __restrict__ delta, const unsigned long long* __restrict__ fx, float inv_fx,
+                            float mean, float in_scale, TensorGeo g, __nv_bfloat16* __restrict__ out) {
+  const size_t m = (size_t)g.n * g.n * g.n;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (size_t)gridDim.x * blockDim.x) {
+    const int z = (int)(i % g.n);
+    const size_t xy = i / g.n;
+    const int y = (int)(xy % g.n), x = (int)(xy / g.n);
+    float d;
+    if (delta) {
+      d = delta[i];
+    } else {
+      const float c = __fmul_rn(__ull2float_rn(fx[i]), inv_fx);
+      d = __fsub_rn(__fdiv_rn(c, mean), 1.0f);
+    }
+    const uint4 c0 = make_uint4(pack_bf16x2(d * in_scale, 0.0f), 0u, 0u, 0u);
+    store_voxel16(out, g, x, y, z, c0, make_uint4(0u, 0u, 0u, 0u));
+  }
+}
+
+// Gradient of the loss with respect to the field, as a BF16 tensor: channels 0-2 = s * dF, rest 0.
+__global__ void k_net_grad_input(const float4* __restrict__ df, float s, TensorGeo g, __nv_bfloat16* __restrict__ out) {
+  const size_t m = (size_t)g.n * g.n * g.n;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (size_t)gridDim.x * blockDim.x) {
+    const int z = (int)(i % g.n);
+    const size_t xy = i / g.n;
+    const int y = (int)(xy % g.n), x = (int)(xy / g.n);
+    const float4 v = df[i];
+    const uint4 c0 = make_uint4(pack_bf16x2(v.x * s, v.y * s), pack_bf16x2(v.z * s, 0.0f), 0u, 0u);
+    store_voxel16(out, g, x, y, z, c0, make_uint4(0u, 0u, 0u, 0u));
+  }
+}
+
+// Packs master weights W[t][co][ci] (FP32) into the B-operand layout [t][chunk][co][8] (BF16):
+// forward, and (transpose) the data-gradient operand W'[t][ci][co] = W[26 - t][co][ci].
+__global__ void k_net_pack(const float* __restrict__ w, int transpose, __nv_bfloat16* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= NET_TAPS * NET_C * NET_C) return;
+  const int k = i % 8, o = (i / 8) % NET_C, c = (i / (8 * NET_C)) % 2, t = i / (16 * NET_C);
+  const int inner = c * 8 + k;  // K index (input channel of this operand)
+  const float v = transpose ? w[((NET_TAPS - 1 - t) * NET_C + inner) * NET_C + o] : w[(t * NET_C + o) * NET_C + inner];
+  out[i] = __float2bfloat16_rn(v);
+}
+
+// Which master weights exist: layer 0 reads channel 0 only; layer 2 writes channels 0-2 only.
+__device__ __forceinline__ bool net_weight_live(int idx) {
+  const int layer = idx / (NET_TAPS * NET_C * NET_C);
+  const int ci = idx % NET_C, co = (idx / NET_C) % NET_C;
+  if (layer == 0 && ci != 0) return false;
+  if (layer == NET_LAYERS - 1 && co >= NET_OUT) return false;
+  return true;
+}
+
+__global__ void k_net_mask(float* __restrict__ w) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < NET_WEIGHTS && !net_weight_live(i)) w[i] = 0.0f;
+}
+
+// Adam (Kingma & Ba 2015) on the live master weights; bias corrections c1 = 1 - b1^t, c2 = 1 - b2^t.
+__global__ void k_net_adam(float* __restrict__ w, float* __restrict__ m1, float* __restrict__ m2,
+                           const float* __restrict__ grad, float lr, float b1, float b2, float eps, float c1, float c2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= NET_WEIGHTS || !net_weight_live(i)) return;
+  const float gi = grad[i];
+  const float a = b1 * m1[i] + (1.0f - b1) * gi;
+  const float b = b2 * m2[i] + (1.0f - b2) * gi * gi;
+  m1[i] = a;
+  m2[i] = b;
+  w[i] -= lr * (a / c1) / (sqrtf(b / c2) + eps);
+}
+
+// Loss of one training sample and its gradient with respect to the field F (float4 mesh):
+// pred_i = CIC gather of F at x_i (mesh.rs:72-77 stencil); for particles with weight_i > 0,
+// L = sum_i weight_i |pred_i - target_i|^2 * inv_norm; dF += CIC scatter of dL/dpred_i.
+__global__ void k_net_loss_grad(const float4* __restrict__ f, const float* __restrict__ x3,
+                                const float* __restrict__ target3, const float* __restrict__ weight, size_t np,
+                                int n, float h, float inv_norm, float4* __restrict__ df, double* __restrict__ sums) {
+  double l_acc = 0.0;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < np; i += (size_t)gridDim.x * blockDim.x) {
+    const float wi = weight[i];
+    if (!(wi > 0.0f)) continue;
+    const float x[3] = {x3[3 * i], x3[3 * i + 1], x3[3 * i + 2]};
+    CicBase cb;
+    cic_base(x, h, n, cb);
+    float p0 = 0.0f, p1 = 0.0f, p2 = 0.0f;
+    size_t idx[8];
+    float w8[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      idx[c] = cic_index(cb, c, n);
+      w8[c] = cic_weight(cb, c);
+      const float4 v = __ldg(f + idx[c]);
+      p0 += w8[c] * v.x;
+      p1 += w8[c] * v.y;
+      p2 += w8[c] * v.z;
+    }
+    const float d0 = p0 - target3[3 * i], d1 = p1 - target3[3 * i + 1], d2 = p2 - target3[3 * i + 2];
+    l_acc += (double)(wi * (d0 * d0 + d1 * d1 + d2 * d2));
+    const float gs = 2.0f * wi * inv_norm;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      float* dst = reinterpret_cast<float*>(df + idx[c]);
+      atomicAdd(dst, gs * d0 * w8[c]);
+      atomicAdd(dst + 1, gs * d1 * w8[c]);
+      atomicAdd(dst + 2, gs * d2 * w8[c]);
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) l_acc += __shfl_xor_sync(0xffffffffu, l_acc, o);
+  if ((threadIdx.x & 31) == 0 && l_acc != 0.0) atomicAdd(&sums[0], l_acc * (double)inv_norm);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Host side: tensor maps, buffers, launches
+// ---------------------------------------------------------------------------------------------
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn(std::string* err) {
+  static std::once_flag once;
+  static EncodeTiledFn fn = nullptr;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  });
+  if (!fn && err) *err = "cuTensorMapEncodeTiled is not available from the driver";
+  return fn;
+}
+
+// Tensor map over a BF16 activation tensor viewed as 5-D (ch8, z, chunk, y, x), box (8, box_z, 2, 1, 1).
+static bool make_row_map(CUtensorMap* map, const __nv_bfloat16* t, int n, int box_z, std::string* err) {
+  EncodeTiledFn fn = encode_fn(err);
+  if (!fn) return false;
+  const cuuint64_t zp = (cuuint64_t)n + 8;
+  const cuuint64_t dims[5] = {8, zp, 2, (cuuint64_t)n, (cuuint64_t)n};
+  const cuuint64_t strides[4] = {16, zp * 16, 2 * zp * 16, (cuuint64_t)n * 2 * zp * 16};
+  const cuuint32_t box[5] = {8, (cuuint32_t)box_z, 2, 1, 1};
+  const cuuint32_t es[5] = {1, 1, 1, 1, 1};
+  const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<__nv_bfloat16*>(t), dims, strides, box, es,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS && err) *err = "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")";
+  return r == CUDA_SUCCESS;
+}
+
+constexpr size_t conv_smem_bytes(int stages) { return (size_t)stages * 9 * ROW_BYTES + W_BYTES + 8 * (2 * stages + 5) + 16; }
+constexpr size_t wgrad_smem_bytes(int stages) {
+  return (size_t)stages * (9 * GRAD_ROW + ROW_BYTES) + 8 * (2 * stages + 1) + 16;
+}
+
+static int sm_count() {
+  static int cached = 0;
+  if (!cached) {
+    int dev = 0, v = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+    cached = v > 0 ? v : 148;
+  }
+  return cached;
+}
+
+}  // namespace cpm
+
+using namespace cpm;
+
+struct cpm_net {
+  int n = 0;
+  TensorGeo g{};
+  std::string err;
+  cudaStream_t own = nullptr;
+  DevBuf t_in, t_a1, t_a2, t_g3, t_g2, t_g1;  // BF16 tensors
+  DevBuf w, m1, m2, grad;                     // FP32 master weights, Adam moments, gradient
+  DevBuf wf, wb;                              // packed BF16 operands: forward, data gradient (3 layers each)
+  DevBuf field, dfield;                       // float4 meshes
+  DevBuf scratch;                             // status word, loss sums
+  CUtensorMap map_in, map_a1, map_a2;         // row maps of the inputs of the three layers
+  CUtensorMap map_g3, map_g2;                 // row maps of the gradient tensors (data gradient input)
+  CUtensorMap gmap_g3, gmap_g2, gmap_g1;      // gradient-row maps of the weight-gradient kernel
+  long long adam_t = 0;
+  bool train_ready = false;
+};
+
+namespace {
+
+#define NET_CU(net, call)                                                                                    \
+  do {                                                                                                       \
+    cudaError_t e_ = (call);                                                                                 \
+    if (e_ != cudaSuccess)                                                                                   \
+      return set_error(&(net)->err, e_ == cudaErrorMemoryAllocation ? CPM_E_NOMEM : CPM_E_CUDA,              \
+                       std::string(#call) + ": " + cudaGetErrorString(e_));                                  \
+  } while (0)
+
+int* net_status(cpm_net* net) { return static_cast<int*>(net->scratch.p); }
+double* net_sums(cpm_net* net) { return reinterpret_cast<double*>(static_cast<char*>(net->scratch.p) + 16); }
+
+size_t tensor_bytes(int n) { return (size_t)n * n * 2 * ((size_t)n + 8) * 8 * sizeof(__nv_bfloat16); }
+
+void launch_conv(cpm_net* net, const CUtensorMap& in_map, int layer, bool transpose, __nv_bfloat16* out16,
+                 float4* out_f4, const __nv_bfloat16* gate, int act, float out_scale, const float* out_scale_dev,
+                 cudaStream_t s) {
+  ConvArgs a;
+  a.g = net->g;
+  a.tiles_z = (net->n + TILE_M - 1) / TILE_M;
+  a.tiles = (long long)net->n * net->n * a.tiles_z;
+  a.w = static_cast<const __nv_bfloat16*>(transpose ? net->wb.p : net->wf.p) + (size_t)layer * NET_TAPS * NET_C * NET_C;
+  a.out16 = out16;
+  a.out_f4 = out_f4;
+  a.gate = gate;
+  a.act = act;
+  a.out_scale = out_scale;
+  a.out_scale_dev = out_scale_dev;
+  a.status = net_status(net);
+  const size_t smem = conv_smem_bytes(CONV_STAGES);
+  cudaFuncSetAttribute(k_conv3<CONV_STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const long long grid = std::min<long long>(a.tiles, sm_count());
+  count_launch();
+  k_conv3<CONV_STAGES><<<(unsigned)grid, CONV_THREADS, smem, s>>>(in_map, a);
+}
+
+void launch_wgrad(cpm_net* net, const CUtensorMap& grad_map, const CUtensorMap& in_map, int layer, cudaStream_t s) {
+  WgradArgs a;
+  a.g = net->g;
+  a.tiles_z = (net->n + TILE_M - 1) / TILE_M;
+  a.tiles = (long long)net->n * net->n * a.tiles_z;
+  a.dw = static_cast<float*>(net->grad.p) + (size_t)layer * NET_TAPS * NET_C * NET_C;
+  a.status = net_status(net);
+  const size_t smem = wgrad_smem_bytes(WG_STAGES);
+  cudaFuncSetAttribute(k_conv3_wgrad<WG_STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const long long grid = std::min<long long>(a.tiles, sm_count());
+  count_launch();
+  k_conv3_wgrad<WG_STAGES><<<(unsigned)grid, CONV_THREADS, smem, s>>>(grad_map, in_map, a);
+}
+
+unsigned grid_1d(size_t work) {
+  size_t b = (work + 255) / 256;
+  if (b > (size_t)sm_count() * 16) b = (size_t)sm_count() * 16;
+  return (unsigned)(b ? b : 1);
+}
+
+void pack_weights(cpm_net* net, cudaStream_t s) {
+  const int per = NET_TAPS * NET_C * NET_C;
+  for (int l = 0; l < NET_LAYERS; ++l) {
+    const float* w = static_cast<const float*>(net->w.p) + (size_t)l * per;
+    count_launch();
+    k_net_pack<<<(per + 255) / 256, 256, 0, s>>>(w, 0, static_cast<__nv_bfloat16*>(net->wf.p) + (size_t)l * per);
+    count_launch();
+    k_net_pack<<<(per + 255) / 256, 256, 0, s>>>(w, 1, static_cast<__nv_bfloat16*>(net->wb.p) + (size_t)l * per);
+  }
+}
+
+int net_check(cpm_net* net, cudaStream_t s) {
+  NET_CU(net, cudaStreamSynchronize(s));
+  NET_CU(net, cudaGetLastError());
+  int st = 0;
+  NET_CU(net, cudaMemcpy(&st, net->scratch.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (st != NET_OK) {
+    cudaMemset(net->scratch.p, 0, sizeof(int));
+    return set_error(&net->err, CPM_E_DEVICE, "net kernel reported status " + std::to_string(st) + " (a wait timed out)");
+  }
+  return CPM_OK;
+}
+
+int ensure_train(cpm_net* net) {
+  if (net->train_ready) return CPM_OK;
+  const size_t tb = tensor_bytes(net->n);
+  for (DevBuf* b : {&net->t_g3, &net->t_g2, &net->t_g1}) NET_CU(net, ensure(*b, tb));
+  NET_CU(net, ensure(net->dfield, (size_t)net->n * net->n * net->n * sizeof(float4)));
+  NET_CU(net, cudaMemset(net->t_g3.p, 0, tb));
+  NET_CU(net, cudaMemset(net->t_g2.p, 0, tb));
+  NET_CU(net, cudaMemset(net->t_g1.p, 0, tb));
+  const __nv_bfloat16* g3 = static_cast<const __nv_bfloat16*>(net->t_g3.p);
+  const __nv_bfloat16* g2 = static_cast<const __nv_bfloat16*>(net->t_g2.p);
+  const __nv_bfloat16* g1 = static_cast<const __nv_bfloat16*>(net->t_g1.p);
+  if (!make_row_map(&net->map_g3, g3, net->n, ROW_BOX, &net->err) ||
+      !make_row_map(&net->map_g2, g2, net->n, ROW_BOX, &net->err) ||
+      !make_row_map(&net->gmap_g3, g3, net->n, TILE_M, &net->err) ||
+      !make_row_map(&net->gmap_g2, g2, net->n, TILE_M, &net->err) ||
+      !make_row_map(&net->gmap_g1, g1, net->n, TILE_M, &net->err))
+    return set_error(&net->err, CPM_E_CUDA, net->err);
+  net->train_ready = true;
+  return CPM_OK;
+}
+
+// Input tensor from delta (f32 mesh) or the fixed-point mass mesh, then the three layers into `field`.
+void net_forward_launch(cpm_net* net, const float* delta, const unsigned long long* fx, int fx_shift, float mean,
+                        float in_scale, float out_scale, const float* out_scale_dev, float4* field, cudaStream_t s) {
+  const size_t m = (size_t)net->n * net->n * net->n;
+  count_launch();
+  k_net_input<<<grid_1d(m), 256, 0, s>>>(delta, fx, std::ldexp(1.0f, -fx_shift), mean, in_scale, net->g,
+                                         static_cast<__nv_bfloat16*>(net->t_in.p));
+  launch_conv(net, net->map_in, 0, false, static_cast<__nv_bfloat16*>(net->t_a1.p), nullptr, nullptr, 1, 1.0f, nullptr, s);
+  launch_conv(net, net->map_a1, 1, false, static_cast<__nv_bfloat16*>(net->t_a2.p), nullptr, nullptr, 1, 1.0f, nullptr, s);
+  launch_conv(net, net->map_a2, 2, false, nullptr, field, nullptr, 0, out_scale, out_scale_dev, s);
+}
+
+// Backward from dL/dF (float4 mesh `dfield`, F = out_scale * y) into the weight gradient (zeroed first).
+void net_backward_launch(cpm_net* net, float out_scale, cudaStream_t s) {
+  const size_t m = (size_t)net->n * net->n * net->n;
+  cudaMemsetAsync(net->grad.p, 0, NET_WEIGHTS * sizeof(float), s);
+  __nv_bfloat16* g3 = static_cast<__nv_bfloat16*>(net->t_g3.p);
+  __nv_bfloat16* g2 = static_cast<__nv_bfloat16*>(net->t_g2.p);
+  __nv_bfloat16* g1 = static_cast<__nv_bfloat16*>(net->t_g1.p);
+  count_launch();
+  k_net_grad_input<<<grid_1d(m), 256, 0, s>>>(static_cast<const float4*>(net->dfield.p), out_scale, net->g, g3);
+  launch_wgrad(net, net->gmap_g3, net->map_a2, 2, s);
+  launch_conv(net, net->map_g3, 2, true, g2, nullptr, static_cast<const __nv_bfloat16*>(net->t_a2.p), 0, 1.0f,
+              nullptr, s);
+  launch_wgrad(net, net->gmap_g2, net->map_a1, 1, s);
+  launch_conv(net, net->map_g2, 1, true, g1, nullptr, static_cast<const __nv_bfloat16*>(net->t_a1.p), 0, 1.0f,
+              nullptr, s);
+  launch_wgrad(net, net->gmap_g1, net->map_in, 0, s);
+}
+
+}  // namespace
+
+namespace cpm {
+// Simulation hook (sim.cu): the field of the learned short-range force from the fixed-point mesh.
+void net_field_from_mesh(cpm_net* net, const unsigned long long* fx, int fx_shift, float mean, float in_scale,
+                         const float* out_scale_dev, float4* field, cudaStream_t s) {
+  net_forward_launch(net, nullptr, fx, fx_shift, mean, in_scale, 1.0f, out_scale_dev, field, s);
+}
+int net_mesh(const cpm_net* net) { return net ? net->n : 0; }
+int* net_status_word(cpm_net* net) { return net_status(net); }
+}  // namespace cpm
+
+extern "C" {
+
+int cpm_net_create(int n_mesh, cpm_net** out) {
+  if (!out) return set_error(nullptr, CPM_E_INVALID, "cpm_net_create: out is NULL");
+  *out = nullptr;
+  if (n_mesh < 16 || n_mesh > 1024 || n_mesh % 16 != 0)
+    return set_error(nullptr, CPM_E_INVALID, "cpm_net_create: n_mesh must be a multiple of 16 in [16, 1024]");
+  int rc = check_device_once(nullptr);
+  if (rc) return rc;
+  cpm_net* net = new cpm_net();
+  net->n = n_mesh;
+  net->g = TensorGeo{n_mesh, n_mesh + 8};
+  auto fail = [&](int code) {
+    g_last_error = net->err;
+    cpm_net_destroy(net);
+    return code;
+  };
+  const size_t tb = tensor_bytes(n_mesh);
+  bool ok = true;
+  for (DevBuf* b : {&net->t_in, &net->t_a1, &net->t_a2}) ok = ok && ensure(*b, tb) == cudaSuccess;
+  for (DevBuf* b : {&net->w, &net->m1, &net->m2, &net->grad}) ok = ok && ensure(*b, NET_WEIGHTS * sizeof(float)) == cudaSuccess;
+  for (DevBuf* b : {&net->wf, &net->wb}) ok = ok && ensure(*b, NET_WEIGHTS * sizeof(__nv_bfloat16)) == cudaSuccess;
+  ok = ok && ensure(net->field, (size_t)n_mesh * n_mesh * n_mesh * sizeof(float4)) == cudaSuccess;
+  ok = ok && ensure(net->scratch, 64) == cudaSuccess;
+  if (!ok) {
+    net->err = "cpm_net_create: device allocation failed";
+    return fail(CPM_E_NOMEM);
+  }
+  for (DevBuf* b : {&net->t_in, &net->t_a1, &net->t_a2}) cudaMemset(b->p, 0, tb);
+  for (DevBuf* b : {&net->w, &net->m1, &net->m2, &net->grad}) cudaMemset(b->p, 0, NET_WEIGHTS * sizeof(float));
+  cudaMemset(net->scratch.p, 0, 64);
+  if (!make_row_map(&net->map_in, static_cast<const __nv_bfloat16*>(net->t_in.p), n_mesh, ROW_BOX, &net->err) ||
+      !make_row_map(&net->map_a1, static_cast<const __nv_bfloat16*>(net->t_a1.p), n_mesh, ROW_BOX, &net->err) ||
+      !make_row_map(&net->map_a2, static_cast<const __nv_bfloat16*>(net->t_a2.p), n_mesh, ROW_BOX, &net->err))
+    return fail(set_error(&net->err, CPM_E_CUDA, net->err));
+  pack_weights(net, nullptr);
+  if (cudaDeviceSynchronize() != cudaSuccess) {
+    net->err = "cpm_net_create: initialisation failed";
+    return fail(CPM_E_CUDA);
+  }
+  *out = net;
+  return CPM_OK;
+}
+
+int cpm_net_destroy(cpm_net* net) {
+  if (!net) return CPM_OK;
+  cudaDeviceSynchronize();
+  for (DevBuf* b : {&net->t_in, &net->t_a1, &net->t_a2, &net->t_g3, &net->t_g2, &net->t_g1, &net->w, &net->m1,
+                    &net->m2, &net->grad, &net->wf, &net->wb, &net->field, &net->dfield, &net->scratch})
+    release(*b);
+  delete net;
+  return CPM_OK;
+}
+
+const char* cpm_net_last_error(const cpm_net* net) { return net ? net->err.c_str() : g_last_error.c_str(); }
+
+int cpm_net_weight_count(void) { return NET_WEIGHTS; }
+
+int cpm_net_set_weights(cpm_net* net, const float* w) {
+  if (!net || !w) return set_error(net ? &net->err : nullptr, CPM_E_INVALID, "cpm_net_set_weights: null pointer");
+  NET_CU(net, cudaMemcpy(net->w.p, w, NET_WEIGHTS * sizeof(float), cudaMemcpyHostToDevice));
+  count_launch();
+  k_net_mask<<<(NET_WEIGHTS + 255) / 256, 256>>>(static_cast<float*>(net->w.p));
+  NET_CU(net, cudaMemset(net->m1.p, 0, NET_WEIGHTS * sizeof(float)));
+  NET_CU(net, cudaMemset(net->m2.p, 0, NET_WEIGHTS * sizeof(float)));
+  net->adam_t = 0;
+  pack_weights(net, nullptr);
+  return net_check(net, nullptr);
+}
+
+int cpm_net_get_weights(cpm_net* net, float* w) {
+  if (!net || !w) return set_error(net ? &net->err : nullptr, CPM_E_INVALID, "cpm_net_get_weights: null pointer");
+  NET_CU(net, cudaMemcpy(w, net->w.p, NET_WEIGHTS * sizeof(float), cudaMemcpyDeviceToHost));
+  return CPM_OK;
+}
+
+int cpm_net_get_grads(cpm_net* net, float* g) {
+  if (!net || !g) return set_error(net ? &net->err : nullptr, CPM_E_INVALID, "cpm_net_get_grads: null pointer");
+  NET_CU(net, cudaDeviceSynchronize());
+  NET_CU(net, cudaMemcpy(g, net->grad.p, NET_WEIGHTS * sizeof(float), cudaMemcpyDeviceToHost));
+  return CPM_OK;
+}
+
+int cpm_net_forward(cpm_net* net, const float* delta_dev, float in_scale, float out_scale, float* field4_dev,
+                    void* stream) {
+  if (!net || !delta_dev || !field4_dev)
+    return set_error(net ? &net->err : nullptr, CPM_E_INVALID, "cpm_net_forward: null pointer");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  net_forward_launch(net, delta_dev, nullptr, 0, 1.0f, in_scale, out_scale, nullptr,
+                     reinterpret_cast<float4*>(field4_dev), s);
+  return net_check(net, s);
+}
+
+int cpm_net_backward(cpm_net* net, const float* dfield4_dev, float out_scale, void* stream) {
+  if (!net || !dfield4_dev) return set_error(net ? &net->err : nullptr, CPM_E_INVALID, "cpm_net_backward: null pointer");
+  int rc = ensure_train(net);
+  if (rc) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  NET_CU(net, cudaMemcpyAsync(net->dfield.p, dfield4_dev, (size_t)net->n * net->n * net->n * sizeof(float4),
+                              cudaMemcpyDeviceToDevice, s));
+  net_backward_launch(net, out_scale, s);
+  return net_check(net, s);
+}
+
+int cpm_net_activations(cpm_net* net, int which, void* dst_dev, void* stream) {
+  if (!net || !dst_dev || which < 0 || which > 5)
+    return set_error(net ? &net->err : nullptr, CPM_E_INVALID, "cpm_net_activations: bad arguments");
+  const DevBuf* src[6] = {&net->t_in, &net->t_a1, &net->t_a2, &net->t_g3, &net->t_g2, &net->t_g1};
+  if (!src[which]->p) return set_error(&net->err, CPM_E_INVALID, "cpm_net_activations: tensor not allocated yet");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  NET_CU(net, cudaMemcpyAsync(dst_dev, src[which]->p, tensor_bytes(net->n), cudaMemcpyDeviceToDevice, s));
+  return net_check(net, s);
+}
+
+int cpm_net_train_step(cpm_net* net, const float* delta_dev, float in_scale, const float* x3_dev,
+                       const float* target3_dev, const float* weight_dev, size_t n_particles, float box_size,
+                       float inv_norm, float lr, double* loss_out, void* stream) {
+  if (!net || !delta_dev || !x3_dev || !target3_dev || !weight_dev)
+    return set_error(net ? &net->err : nullptr, CPM_E_INVALID, "cpm_net_train_step: null pointer");
+  if (!(box_size > 0.0f) || !(lr >= 0.0f))
+    return set_error(&net->err, CPM_E_INVALID, "cpm_net_train_step: box_size must be > 0 and lr >= 0");
+  int rc = ensure_train(net);
+  if (rc) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const size_t m = (size_t)net->n * net->n * net->n;
+  float4* field = static_cast<float4*>(net->field.p);
+  net_forward_launch(net, delta_dev, nullptr, 0, 1.0f, in_scale, 1.0f, nullptr, field, s);
+  NET_CU(net, cudaMemsetAsync(net->dfield.p, 0, m * sizeof(float4), s));
+  NET_CU(net, cudaMemsetAsync(net_sums(net), 0, 2 * sizeof(double), s));
+  if (n_particles) {
+    count_launch();
+    k_net_loss_grad<<<grid_1d(n_particles), 256, 0, s>>>(field, x3_dev, target3_dev, weight_dev, n_particles, net->n,
+                                                         box_size / (float)net->n, inv_norm,
+                                                         static_cast<float4*>(net->dfield.p), net_sums(net));
+  }
+  net_backward_launch(net, 1.0f, s);
+  if (lr > 0.0f) {
+    net->adam_t += 1;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.0f - std::pow(b1, (float)net->adam_t), c2 = 1.0f - std::pow(b2, (float)net->adam_t);
+    count_launch();
+    k_net_adam<<<(NET_WEIGHTS + 255) / 256, 256, 0, s>>>(static_cast<float*>(net->w.p), static_cast<float*>(net->m1.p),
+                                                         static_cast<float*>(net->m2.p),
+                                                         static_cast<const float*>(net->grad.p), lr, b1, b2, 1e-8f, c1,
+                                                         c2);
+    pack_weights(net, s);
+  }
+  double sums[2] = {0.0, 0.0};
+  NET_CU(net, cudaMemcpyAsync(sums, net_sums(net), sizeof(sums), cudaMemcpyDeviceToHost, s));
+  rc = net_check(net, s);
+  if (rc) return rc;
+  if (loss_out) *loss_out = sums[0];
+  return CPM_OK;
+}
+
+}  // extern "C"

@@ -176,6 +176,45 @@ int cpm_power_spectrum(cpm_ctx* ctx, const float* x3, size_t n, int n_shells, do
  * reference's f32 sums. */
 int cpm_density_grid(cpm_ctx* ctx, const float* delta, int n, float* grid, int* grid_n);
 
+/* ------------------------------------------------------------------ learned short-range force */
+/* No counterpart in the reference, which computes the whole short-range force with the tree walk
+ * (tree.rs:264-310). A 3-layer 3x3x3 periodic convolutional net (16 channels, leaky ReLU with slope
+ * 1/8 after layers 1 and 2, no biases) maps the density contrast delta of an n^3 mesh to a 3-channel
+ * acceleration field F = out_scale * net(in_scale * delta), evaluated with BF16 tcgen05 tensor-core
+ * kernels accumulating in FP32; a simulation gathers F to particles with the CIC stencil
+ * (mesh.rs:72-77). Weights are FP32 masters W[layer][tap][out][in], 3 x 27 x 16 x 16 floats, tap
+ * (dx+1)*9 + (dy+1)*3 + (dz+1), out[v] = sum_t W[t] in[v + t]; layer 1 reads input channel 0 only,
+ * layer 3 writes channels 0-2 only (other entries are kept at 0). Device pointers; calls enqueue on
+ * `stream` (cudaStream_t, NULL = default) and synchronise it before returning. */
+typedef struct cpm_net cpm_net;
+/* Number of master weights (3 * 27 * 16 * 16). */
+int cpm_net_weight_count(void);
+/* A net with device buffers for n_mesh^3 meshes (n_mesh a multiple of 16 in [16, 1024]); weights 0. */
+int cpm_net_create(int n_mesh, cpm_net** out);
+int cpm_net_destroy(cpm_net* net);
+const char* cpm_net_last_error(const cpm_net* net);
+/* Host arrays of cpm_net_weight_count() floats. Setting weights resets the Adam state. */
+int cpm_net_set_weights(cpm_net* net, const float* w);
+int cpm_net_get_weights(cpm_net* net, float* w);
+/* The weight gradient of the last cpm_net_backward or cpm_net_train_step (host array). */
+int cpm_net_get_grads(cpm_net* net, float* g);
+/* field4_dev[(x*n + y)*n + z] = (F_x, F_y, F_z, 0) from delta_dev[n^3] (f32). */
+int cpm_net_forward(cpm_net* net, const float* delta_dev, float in_scale, float out_scale, float* field4_dev,
+                    void* stream);
+/* Weight gradient of a loss L from dL/dF (dfield4_dev, float4 per cell) for the last forward of this
+ * net with output scale out_scale. */
+int cpm_net_backward(cpm_net* net, const float* dfield4_dev, float out_scale, void* stream);
+/* Copies one internal BF16 tensor ([x][y][2][n+8][8], z padded by a periodic halo) to dst_dev:
+ * 0 input, 1 and 2 the activations of layers 1 and 2, 3..5 the gradients of layers 3, 2, 1. */
+int cpm_net_activations(cpm_net* net, int which, void* dst_dev, void* stream);
+/* One training step on one mesh and its particles: F = net(in_scale * delta) (out_scale 1), the
+ * loss L = inv_norm * sum_i weight_i |F(x_i) - target_i|^2 (CIC gather of F at x_i), its gradient by
+ * the backward kernels, then one Adam step (b1 0.9, b2 0.999, eps 1e-8) with learning rate lr
+ * (lr = 0: gradient only). loss_out (may be NULL) receives L before the update. */
+int cpm_net_train_step(cpm_net* net, const float* delta_dev, float in_scale, const float* x3_dev,
+                       const float* target3_dev, const float* weight_dev, size_t n_particles, float box_size,
+                       float inv_norm, float lr, double* loss_out, void* stream);
+
 /* ------------------------------------------------------------------ device-resident simulation */
 /* Replaces `Simulation` (integrator.rs:34-186) under a `cuda` feature: state stays in HBM and
  * `step_to` runs one KDK step (kick, drift, deposit, FFT-Poisson, gather, tree build and walk,
