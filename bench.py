@@ -44,7 +44,12 @@ WORKLOADS = {
     "treepm-128": dict(n_side=128, mesh=256, box=128.0, seed=7, steps_total=128),
     # profiling case for the PM kernels: full-size 512^3 mesh, 128^3 particles.
     "pm512-128": dict(n_side=128, mesh=512, box=128.0, seed=7, steps_total=128),
+    # the headline workload with the learned short-range force (trained weights, tree walk kept for
+    # particles in cells with density contrast >= the trained threshold)
+    "learned-256": dict(n_side=256, mesh=512, box=256.0, seed=7, steps_total=128, learned=True),
+    "learned-128": dict(n_side=128, mesh=256, box=128.0, seed=7, steps_total=128, learned=True),
 }
+NET_WEIGHTS = ROOT / PKG / "weights" / "short_range_net.npz"
 COSMO = dict(omega_r=0.0, omega_m=0.3, omega_l=0.7, h0=70.0)
 N_S, SIGMA8, A_INIT, A_END, THETA, SOFT = 0.96, 0.8, 0.02, 1.0, 0.5, 1.0 / 30.0
 
@@ -184,11 +189,21 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
         i0 = int(np.searchsorted(np.asarray(full, np.float32), np.float32(a_saved), side="right"))
         sched = full[i0:i0 + args.warmup + args.steps]
 
-    def make_sim(flags: int):
+    net, net_threshold = None, None
+    if wl.get("learned"):
+        z = np.load(NET_WEIGHTS)
+        net = cpm.ShortRangeNet(mesh, z["weights"])
+        net_threshold = float(z["threshold"])
+
+    def make_sim(flags: int, learned: bool = bool(wl.get("learned"))):
         if args.load_state:
-            return cpm.Simulation(cosmo, box, mesh, st0["x"], st0["p"], a_saved, split, flags=flags)
-        return cpm.Simulation.from_zeldovich(cosmo, box, mesh, n_side, N_S, SIGMA8, A_INIT, replica_seed(wl["seed"], rank),
-                                             split, flags=flags)
+            sim_ = cpm.Simulation(cosmo, box, mesh, st0["x"], st0["p"], a_saved, split, flags=flags)
+        else:
+            sim_ = cpm.Simulation.from_zeldovich(cosmo, box, mesh, n_side, N_S, SIGMA8, A_INIT,
+                                                 replica_seed(wl["seed"], rank), split, flags=flags)
+        if learned:
+            sim_.set_learned(net, net_threshold)
+        return sim_
 
     # The timed run replays the step's captured CUDA graphs (no per-phase events).
     sim = make_sim(0)
@@ -218,6 +233,7 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
     ms = max_over_ranks(ms_local, dist, dev)
     counters = sim.counters()
     graphs = sim.graphs()
+    walked = sim.walked()
     if args.save_state and rank == 0:
         st = sim.state()
         np.savez(args.save_state, x=st["x"], p=st["p"], a=np.float32(st["a"]))
@@ -252,7 +268,7 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
     # End to end through the host-buffer C-ABI step, same schedule window, on a fresh simulation.
     e2e = None
     if not args.no_e2e:
-        sim2 = cpm.Simulation.from_zeldovich(cosmo, box, mesh, n_side, N_S, SIGMA8, A_INIT, replica_seed(wl["seed"], rank), split)
+        sim2 = make_sim(0)
         for a1 in sched[:args.warmup]:
             sim2.step_to(a1)
         xs = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
@@ -311,6 +327,11 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
                  "node_accepts_last_step": counters["node_accepts"],
                  "candidates_last_step": counters["candidates"]},
         "tree_walk_end_state": walk,
+        "walked_last_step": walked,
+        "learned": ({"net": "3-layer 3^3 conv, 16 channels, BF16 tcgen05 kernels", "weights": str(NET_WEIGHTS.name),
+                     "delta_threshold": net_threshold,
+                     "note": "phase gather_ms includes the net inference; walk only for particles at or above "
+                             "the threshold"} if net is not None else None),
         "gpu_launches": counters["launches_per_step"] * args.steps,
         "launches_per_step": counters["launches_per_step"],
         "clocks": clk,

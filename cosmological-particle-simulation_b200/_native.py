@@ -118,6 +118,13 @@ def lib() -> C.CDLL:
         "cpm_sim_snapshot": (i, [vp, vp, vp, vp, vp, C.POINTER(i), C.POINTER(fl)]),
         "cpm_density_grid": (i, [vp, vp, i, vp, C.POINTER(i)]),
         "cpm_sim_destroy": (i, [vp]),
+        "cpm_sim_set_learned": (i, [vp, vp, fl, fl]),
+        "cpm_sim_learned_walked": (i, [vp, C.POINTER(u64)]),
+        "cpm_sim_short_range": (i, [vp, vp]),
+        "cpm_sim_save": (i, [vp, C.c_char_p]),
+        "cpm_step_factors": (i, [C.POINTER(Cosmology), C.c_double, C.c_double, i, C.POINTER(C.c_double),
+                                 C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+        "cpm_sim_load": (i, [C.c_char_p, u32, C.POINTER(vp)]),
         "cpm_net_weight_count": (i, []),
         "cpm_net_create": (i, [i, C.POINTER(vp)]),
         "cpm_net_destroy": (i, [vp]),

@@ -392,6 +392,48 @@ class Simulation:
         """Captured step graphs: 2 once both sorted-buffer parities replay a graph."""
         return int(nat.lib().cpm_sim_graphs(self.h))
 
+    def save(self, path) -> None:
+        """Writes the state file (positions, momenta, a and every parameter; cpm_sim_save)."""
+        check(nat.lib().cpm_sim_save(self.h, str(path).encode()), sim=True)
+
+    @staticmethod
+    def load(path, extra_flags: int = 0) -> "Simulation":
+        """A simulation created from a state file written by `save` (cpm_sim_load)."""
+        h = C.c_void_p()
+        check(nat.lib().cpm_sim_load(str(path).encode(), int(extra_flags), C.byref(h)), sim=True)
+        with open(path, "rb") as f:
+            hdr = f.read(128)
+        n = int(np.frombuffer(hdr[16:24], np.uint64)[0])
+        box = float(np.frombuffer(hdr[28:32], np.float32)[0])
+        mesh = int(np.frombuffer(hdr[32:36], np.int32)[0])
+        use_tree = int(np.frombuffer(hdr[36:40], np.int32)[0])
+        cf = np.frombuffer(hdr[40:56], np.float32)
+        sp = np.frombuffer(hdr[56:72], np.float32)
+        cosmo = Cosmology(*(float(v) for v in cf))
+        split = ForceSplit(*(float(v) for v in sp)) if use_tree else None
+        a = float(np.frombuffer(hdr[24:28], np.float32)[0])
+        return Simulation(cosmo, box, mesh, None, None, a, split, extra_flags, _handle=h, _n=n)
+
+    def set_learned(self, net, delta_threshold: float = 50.0, in_scale: float = 1.0) -> None:
+        """Attach a learned short-range net (a `ShortRangeNet` on this mesh; None detaches): particles
+        below `delta_threshold` take the net's field, the others keep the tree walk. The simulation
+        keeps a reference to the net."""
+        check(nat.lib().cpm_sim_set_learned(self.h, net.h if net is not None else None, float(delta_threshold),
+                                            float(in_scale)), sim=True)
+        self._net = net
+
+    def short_range(self) -> np.ndarray:
+        """tree::accelerations (tree.rs:314-323) alone on the current state, caller order."""
+        out = np.empty((self.n, 3), np.float32)
+        check(nat.lib().cpm_sim_short_range(self.h, ptr(out)), sim=True)
+        return out
+
+    def walked(self) -> int:
+        """Particles the last step walked the tree for."""
+        v = C.c_uint64()
+        check(nat.lib().cpm_sim_learned_walked(self.h, C.byref(v)), sim=True)
+        return int(v.value)
+
     def stream(self) -> int:
         return nat.lib().cpm_sim_stream(self.h) or 0
 

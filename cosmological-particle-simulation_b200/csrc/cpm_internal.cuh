@@ -244,10 +244,11 @@ cudaError_t tree_build(TreeNodes& t, const uint64_t* sorted_keys, const float* s
                        DevStatus* st, cudaStream_t s);
 // Walks the tree for every sorted particle; acc3 (sorted order) receives g_sr, or g + g_sr
 // when `accumulate` (the reference's g[c] += s[c], integrator.rs:154-158).
-// The coupling k is read from *k_dev when k_dev is set.
+// The coupling k is read from *k_dev when k_dev is set. With `list`, only the sorted particles
+// list[0 .. *list_n - 1] are walked (the grid is sized for n; the count is read on the device).
 void launch_tree_walk(const TreeNodes& t, const float* sorted_x3, size_t n, float box, const cpm_force_split& split,
                       float k, float* acc3, int accumulate, TreeCounters* counters, DevStatus* st, cudaStream_t s,
-                      const float* k_dev = nullptr);
+                      const float* k_dev = nullptr, const uint32_t* list = nullptr, const uint32_t* list_n = nullptr);
 // Releases the walk's per-tree state (the fitted pair-force coefficients).
 void tree_walk_free(TreeNodes& t);
 
@@ -262,8 +263,17 @@ struct StepScalars {
   float k2;         // second half-kick factor, kick_factor(a_mid, a1)
   float prefactor;  // Green's function prefactor 1.5 Omega_m / a1
   float tree_k;     // short-range coupling K(a1)
+  float net_scale;  // output scale of the learned short-range field, K(a1) (N / M) / h
+  float pad_;
+  double d64;       // drift factor in FP64 (precision mode: the fixed-point drift uses it)
 };
 void launch_set_step_scalars(StepScalars* dev, const StepScalars& v, cudaStream_t s);
+// Precision mode: every scalar of the step from a0 to a1 computed on the device in FP64 (kick and
+// drift integrals by Simpson's rule with 256 intervals, the midpoint by 60 bisection steps, the
+// Green's prefactor, the tree coupling and the net scale), rounded once to f32 (d64 kept).
+// net_per_cell_h = (N / M) / h.
+void launch_step_factors64(StepScalars* dev, const cpm_cosmology& c, double a0, double a1, double box,
+                           double n_particles, double net_per_cell_h, cudaStream_t s);
 // p += g * k (integrator.rs:301-307); k is read from *k_dev when k_dev is set.
 void launch_kick(float* p3, const float* g3, size_t n, float k, cudaStream_t s, const float* k_dev = nullptr);
 // Optional kick with k_prev, then kick with k1, then drift (integrator.rs:301-316); k1 and d are
@@ -308,5 +318,22 @@ void launch_downsample_grid(const float* delta, int n, float* out, cudaStream_t 
 cudaError_t generate_zeldovich(int n, float box, const cpm_cosmology& c, float n_s, float sigma8, float a_init,
                                uint64_t seed, float* x3_dev, float* p3_dev, DevBuf& modes, DevBuf& work,
                                FftPlan& plan, cudaStream_t s);
+
+// ---------------------------------------------------------------------------------------------
+// Learned short-range force — net.cu, learned_step.cu
+// ---------------------------------------------------------------------------------------------
+// The net's field F = out_scale * net(in_scale * delta) (float4 per cell, in the net's own buffer,
+// returned) from the u64 fixed-point mass mesh; the scale is read from *out_scale_dev when set.
+float4* net_field_from_mesh(cpm_net* net, const unsigned long long* fx, int fx_shift, float mean, float in_scale,
+                            float out_scale, const float* out_scale_dev, cudaStream_t s);
+int net_mesh(const cpm_net* net);
+int* net_status_word(cpm_net* net);
+// acc = g_pm + F (delta_i < threshold) or g_pm with flag_i = 1 (delta_i >= threshold), one stencil.
+void launch_learned_gather(const float* gx, const float* gy, const float* gz, const unsigned long long* fx, int shift,
+                           float mean, const float4* field, const float* x3, size_t n, int mesh_n, float h,
+                           float threshold, float* out3, uint32_t* flag, cudaStream_t s);
+// list = indices i with flag_i = 1 in increasing order, *count = their number (offset: scratch).
+cudaError_t launch_compact(const uint32_t* flag, uint32_t* offset, size_t n, uint32_t* list, uint32_t* count,
+                           DevBuf& scan_tmp, cudaStream_t s);
 
 }  // namespace cpm

@@ -36,12 +36,13 @@ __device__ __forceinline__ float fixed_to_x(uint32_t q, double unit) { return (f
 __global__ void k_kick_drift_fixed(uint32_t* __restrict__ q3, float* __restrict__ x3, float* __restrict__ p3,
                                    const float* __restrict__ g3, size_t n3, float box,
                                    const StepScalars* __restrict__ sc) {
-  const float k1 = sc->k1, d = sc->d;
+  const float k1 = sc->k1;
+  const double d = sc->d64;
   const double per_length = 4294967296.0 / (double)box, unit = (double)box / 4294967296.0;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += (size_t)gridDim.x * blockDim.x) {
     const float p = __fadd_rn(p3[i], __fmul_rn(g3[i], k1));
     p3[i] = p;
-    const long long dq = __double2ll_rn((double)p * (double)d * per_length);
+    const long long dq = __double2ll_rn((double)p * d * per_length);
     const uint32_t q = q3[i] + (uint32_t)(unsigned long long)dq;  // modulo 2^32: the periodic wrap
     q3[i] = q;
     x3[i] = fixed_to_x(q, unit);
@@ -101,6 +102,67 @@ static unsigned grid_for(size_t work) {
 }
 
 __global__ void k_set_step_scalars(StepScalars* dev, StepScalars v) { *dev = v; }
+
+// cosmology.rs:32-34 in FP64.
+__device__ __forceinline__ double cosmo_e64(const cpm_cosmology& c, double a) {
+  const double a2 = a * a;
+  return sqrt((double)c.omega_r / (a2 * a2) + (double)c.omega_m / (a2 * a) + (double)c.omega_l);
+}
+
+// Simpson's rule (integrator.rs:288-297) with 256 intervals in FP64, summed by one warp:
+// kind 0: 1 / (a E(a)) (kick, integrator.rs:263-265); kind 1: 1 / (a^3 E(a)) (drift, :268-270).
+__device__ double simpson_warp64(const cpm_cosmology& c, double lo, double hi, int kind) {
+  constexpr int N = 256;
+  const int lane = threadIdx.x & 31;
+  const double h = (hi - lo) / N;
+  double sum = 0.0;
+  for (int i = lane; i <= N; i += 32) {
+    const double a = lo + i * h;
+    const double f = kind == 0 ? 1.0 / (a * cosmo_e64(c, a)) : 1.0 / (a * a * a * cosmo_e64(c, a));
+    const double w = (i == 0 || i == N) ? 1.0 : ((i & 1) ? 4.0 : 2.0);
+    sum += w * f;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+  return sum * h / 3.0;
+}
+
+__global__ void k_step_factors64(StepScalars* dev, cpm_cosmology c, double a0, double a1, double box, double n_part,
+                                 double net_per_cell_h) {
+  // integrator.rs:273-285: the scale factor where the kick integral is half its total
+  const double half = 0.5 * simpson_warp64(c, a0, a1, 0);
+  double lo = a0, hi = a1;
+  for (int it = 0; it < 60; ++it) {
+    const double mid = 0.5 * (lo + hi);
+    if (simpson_warp64(c, a0, mid, 0) < half)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  const double am = 0.5 * (lo + hi);
+  const double k1 = simpson_warp64(c, a0, am, 0), k2 = simpson_warp64(c, am, a1, 0);
+  const double d = simpson_warp64(c, a0, a1, 1);
+  if ((threadIdx.x & 31) == 0) {
+    const double pi = 3.14159265358979323846;
+    const double tree_k = 1.5 * (double)c.omega_m * box * box * box / (4.0 * pi * a1 * n_part);  // integrator.rs:152
+    StepScalars v;
+    v.k1 = (float)k1;
+    v.d = (float)d;
+    v.k2 = (float)k2;
+    v.prefactor = (float)(1.5 * (double)c.omega_m / a1);  // poisson.rs:46
+    v.tree_k = (float)tree_k;
+    v.net_scale = (float)(tree_k * net_per_cell_h);
+    v.pad_ = 0.0f;
+    v.d64 = d;
+    *dev = v;
+  }
+}
+
+void launch_step_factors64(StepScalars* dev, const cpm_cosmology& c, double a0, double a1, double box,
+                           double n_particles, double net_per_cell_h, cudaStream_t s) {
+  count_launch();
+  k_step_factors64<<<1, 32, 0, s>>>(dev, c, a0, a1, box, n_particles, net_per_cell_h);
+}
 
 void launch_set_step_scalars(StepScalars* dev, const StepScalars& v, cudaStream_t s) {
   count_launch();

@@ -762,9 +762,11 @@ void net_backward_launch(cpm_net* net, float out_scale, cudaStream_t s) {
 
 namespace cpm {
 // Simulation hook (sim.cu): the field of the learned short-range force from the fixed-point mesh.
-void net_field_from_mesh(cpm_net* net, const unsigned long long* fx, int fx_shift, float mean, float in_scale,
-                         const float* out_scale_dev, float4* field, cudaStream_t s) {
-  net_forward_launch(net, nullptr, fx, fx_shift, mean, in_scale, 1.0f, out_scale_dev, field, s);
+float4* net_field_from_mesh(cpm_net* net, const unsigned long long* fx, int fx_shift, float mean, float in_scale,
+                            float out_scale, const float* out_scale_dev, cudaStream_t s) {
+  float4* field = static_cast<float4*>(net->field.p);
+  net_forward_launch(net, nullptr, fx, fx_shift, mean, in_scale, out_scale, out_scale_dev, field, s);
+  return field;
 }
 int net_mesh(const cpm_net* net) { return net ? net->n : 0; }
 int* net_status_word(cpm_net* net) { return net_status(net); }

@@ -18,10 +18,15 @@
 // CPM_SIM_NO_GRAPH launches every kernel directly, and so does CPM_SIM_TIMING, whose per-phase
 // event records are made on the stream between the kernels.
 //
+// With a net attached (cpm_sim_set_learned), the gather phase also evaluates the learned
+// short-range field on the mesh and adds it for particles whose density contrast is below the
+// threshold; the tree walk then runs for the other particles only (learned_step.cu).
+//
 // CPM_SIM_FIXED_POINT keeps the master positions as uint32 fixed point q (x = q L / 2^32) in key
 // order beside x: the drift adds round(p d 2^32 / L) to q, so the periodic wrap is exact and the
 // resolution is L / 2^32 everywhere in the box; x (f32, what every force kernel reads) is
 // rewritten from q after each drift. Positions given by the caller are rounded to the grid.
+#include <cstdio>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -71,6 +76,12 @@ struct cpm_sim {
   cudaEvent_t ev_sorted = nullptr;
   float* x_out = nullptr;      // caller-order destination of this step's positions, or null
   bool direct_step = false;    // run the next step uncaptured
+  // Learned short-range force (cpm_sim_set_learned): the net, the density-contrast threshold above
+  // which particles keep the tree walk, the net's input scale, and the dense-particle list.
+  cpm_net* net = nullptr;
+  float net_threshold = 50.0f;
+  float net_in_scale = 1.0f;
+  DevBuf flag, offset, list, list_n, scan_tmp;
 };
 
 #define SIM_CU(s, call)                                                                                      \
@@ -94,6 +105,15 @@ static int sim_check(cpm_sim* s) {
       return set_error(&s->err, CPM_E_NONFINITE, "non-finite position at particle " + std::to_string(st.detail));
     return set_error(&s->err, CPM_E_DEVICE,
                      "device status " + std::to_string(st.code) + " detail " + std::to_string(st.detail));
+  }
+  if (s->net) {  // the net's kernels report a wait that ran out in their own status word
+    int ns = 0;
+    e = cudaMemcpy(&ns, net_status_word(s->net), sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return set_error(&s->err, CPM_E_CUDA, cudaGetErrorString(e));
+    if (ns != 0) {
+      cudaMemset(net_status_word(s->net), 0, sizeof(int));
+      return set_error(&s->err, CPM_E_DEVICE, "learned short-range net: status " + std::to_string(ns));
+    }
   }
   return CPM_OK;
 }
@@ -138,6 +158,13 @@ static void swap_sorted(cpm_sim* s) {
 
 static bool fixed_point(const cpm_sim* s) { return (s->P.flags & CPM_SIM_FIXED_POINT) != 0; }
 
+// Output scale of the learned short-range field: the tree coupling K(a) (integrator.rs:150-152) times
+// the mean particles per cell over the cell size, which makes the net's output dimensionless.
+static float net_field_scale(const cpm_sim* s, float a) {
+  const float m = (float)((double)s->P.mesh_n * s->P.mesh_n * s->P.mesh_n);
+  return tree_coupling(s->P.cosmo.omega_m, s->box, a, s->n) * ((float)s->n / m) / s->h;
+}
+
 // Sort into key order, then the force: deposit, FFT-Poisson, gather, tree. Phases 1..6. With
 // `dev`, the Poisson prefactor and the tree coupling are read from the device step block.
 static int sim_accelerations(cpm_sim* s, float a, const StepScalars* dev = nullptr) {
@@ -170,8 +197,20 @@ static int sim_accelerations(cpm_sim* s, float a, const StepScalars* dev = nullp
   launch_poisson(s->plan, pp, nullptr, as<unsigned long long>(s->fx), s->shift, s->mean, as<float2>(s->spec),
                  as<float>(s->gx), as<float>(s->gy), as<float>(s->gz), s->stream);
   mark(s, 4);
-  launch_interpolate3(as<float>(s->gx), as<float>(s->gy), as<float>(s->gz), as<float>(s->x), n, mn, s->h,
-                      as<float>(s->acc), s->stream);
+  const bool learned = s->net && s->P.use_tree;
+  if (learned) {
+    const float scale = net_field_scale(s, a);
+    const float4* field = net_field_from_mesh(s->net, as<unsigned long long>(s->fx), s->shift, s->mean, s->net_in_scale,
+                                              scale, dev ? &dev->net_scale : nullptr, s->stream);
+    launch_learned_gather(as<float>(s->gx), as<float>(s->gy), as<float>(s->gz), as<unsigned long long>(s->fx),
+                          s->shift, s->mean, field, as<float>(s->x), n, mn, s->h, s->net_threshold, as<float>(s->acc),
+                          as<uint32_t>(s->flag), s->stream);
+    SIM_CU(s, launch_compact(as<uint32_t>(s->flag), as<uint32_t>(s->offset), n, as<uint32_t>(s->list),
+                             as<uint32_t>(s->list_n), s->scan_tmp, s->stream));
+  } else {
+    launch_interpolate3(as<float>(s->gx), as<float>(s->gy), as<float>(s->gz), as<float>(s->x), n, mn, s->h,
+                        as<float>(s->acc), s->stream);
+  }
   mark(s, 5);
   if (s->P.use_tree) {
     SIM_CU(s, tree_build(s->tree, as<uint64_t>(s->keys), as<float>(s->x), n, s->box, as<DevStatus>(s->status),
@@ -181,7 +220,8 @@ static int sim_accelerations(cpm_sim* s, float a, const StepScalars* dev = nullp
     const float k = tree_coupling(s->P.cosmo.omega_m, s->box, a, n);
     launch_tree_walk(s->tree, as<float>(s->x), n, s->box, s->P.split, k, as<float>(s->acc), 1,
                      as<TreeCounters>(s->counters), as<DevStatus>(s->status), s->stream,
-                     dev ? &dev->tree_k : nullptr);
+                     dev ? &dev->tree_k : nullptr, learned ? as<uint32_t>(s->list) : nullptr,
+                     learned ? as<uint32_t>(s->list_n) : nullptr);
   } else {
     mark(s, 6);
   }
@@ -367,10 +407,19 @@ int cpm_sim_step_to(cpm_sim* s, float a1) {
   sc.k2 = kick_factor(c, am, a1);
   sc.prefactor = make_poisson_params(s->P.mesh_n, s->box, c.omega_m, a1, 0.0f, 0).prefactor;
   sc.tree_k = tree_coupling(c.omega_m, s->box, a1, s->n);
+  sc.net_scale = net_field_scale(s, a1);
   const int q = s->parity;
   int rc;
   if ((s->P.flags & CPM_SIM_TIMING) && (rc = flush_set(s, q))) return rc;
-  launch_set_step_scalars(as<StepScalars>(s->stepv), sc, s->stream);
+  sc.pad_ = 0.0f;
+  sc.d64 = (double)sc.d;
+  if (fixed_point(s)) {  // precision mode: the step's scalars in FP64 on the device
+    const double m = (double)s->P.mesh_n * s->P.mesh_n * s->P.mesh_n;
+    launch_step_factors64(as<StepScalars>(s->stepv), s->P.cosmo, (double)a0, (double)a1, (double)s->box,
+                          (double)s->n, ((double)s->n / m) / (double)s->h, s->stream);
+  } else {
+    launch_set_step_scalars(as<StepScalars>(s->stepv), sc, s->stream);
+  }
   const unsigned long long l0 = launch_count();
   s->ev_set = q;
   const bool graphs =
@@ -559,6 +608,184 @@ int cpm_sim_counters(cpm_sim* s, uint64_t* nodes, uint64_t* leaf_pairs, uint64_t
   return CPM_OK;
 }
 
+// State file: a 128-byte little-endian header, then x[n][3] and p[n][3] (f32, caller order).
+//   0  char[8]  "CPMSTATE"        8 u32 version (1)       12 u32 flags (CPM_SIM_*)
+//  16  u64 n_particles            24 f32 a                28 f32 box_size
+//  32  i32 mesh_n                 36 i32 use_tree         40 f32 omega_r, omega_m, omega_l, h0
+//  56  f32 r_split, r_cut, softening, theta               72 u64 payload bytes (24 n)
+//  80  u64 FNV-1a 64 hash of the payload                  88 .. 127 zero
+namespace {
+constexpr size_t STATE_HEADER = 128;
+
+uint64_t fnv1a64(const unsigned char* p, size_t len, uint64_t h) {
+  for (size_t i = 0; i < len; ++i) {
+    h ^= p[i];
+    h *= 0x100000001B3ull;
+  }
+  return h;
+}
+}  // namespace
+
+int cpm_sim_save(cpm_sim* s, const char* path) {
+  if (!s || !path) return set_error(s ? &s->err : nullptr, CPM_E_INVALID, "cpm_sim_save: null pointer");
+  const size_t n = s->n;
+  std::vector<float> xp(6 * n);
+  float a = 0.0f;
+  int rc = cpm_sim_get_state(s, xp.data(), xp.data() + 3 * n, nullptr, nullptr, &a);
+  if (rc) return rc;
+  unsigned char hdr[STATE_HEADER] = {};
+  const uint32_t version = 1, flags = s->P.flags;
+  const uint64_t nn = n, payload = 24 * (uint64_t)n;
+  const int32_t mesh = s->P.mesh_n, use_tree = s->P.use_tree;
+  const float cosmo[4] = {s->P.cosmo.omega_r, s->P.cosmo.omega_m, s->P.cosmo.omega_l, s->P.cosmo.h0};
+  const float split[4] = {s->P.split.r_split, s->P.split.r_cut, s->P.split.softening, s->P.split.theta};
+  const uint64_t hash = fnv1a64(reinterpret_cast<const unsigned char*>(xp.data()), payload, 0xCBF29CE484222325ull);
+  std::memcpy(hdr, "CPMSTATE", 8);
+  std::memcpy(hdr + 8, &version, 4);
+  std::memcpy(hdr + 12, &flags, 4);
+  std::memcpy(hdr + 16, &nn, 8);
+  std::memcpy(hdr + 24, &a, 4);
+  std::memcpy(hdr + 28, &s->P.box_size, 4);
+  std::memcpy(hdr + 32, &mesh, 4);
+  std::memcpy(hdr + 36, &use_tree, 4);
+  std::memcpy(hdr + 40, cosmo, 16);
+  std::memcpy(hdr + 56, split, 16);
+  std::memcpy(hdr + 72, &payload, 8);
+  std::memcpy(hdr + 80, &hash, 8);
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return set_error(&s->err, CPM_E_INVALID, std::string("cpm_sim_save: cannot open ") + path);
+  const bool ok = std::fwrite(hdr, 1, STATE_HEADER, f) == STATE_HEADER &&
+                  std::fwrite(xp.data(), 1, payload, f) == payload;
+  const bool closed = std::fclose(f) == 0;
+  if (!ok || !closed) return set_error(&s->err, CPM_E_INVALID, std::string("cpm_sim_save: write failed: ") + path);
+  return CPM_OK;
+}
+
+int cpm_sim_load(const char* path, uint32_t extra_flags, cpm_sim** out) {
+  if (!path || !out) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_load: null pointer");
+  *out = nullptr;
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return set_error(nullptr, CPM_E_INVALID, std::string("cpm_sim_load: cannot open ") + path);
+  unsigned char hdr[STATE_HEADER];
+  if (std::fread(hdr, 1, STATE_HEADER, f) != STATE_HEADER || std::memcmp(hdr, "CPMSTATE", 8) != 0) {
+    std::fclose(f);
+    return set_error(nullptr, CPM_E_INVALID, std::string("cpm_sim_load: not a state file: ") + path);
+  }
+  uint32_t version, flags;
+  uint64_t nn, payload, hash;
+  float a, box, cosmo[4], split[4];
+  int32_t mesh, use_tree;
+  std::memcpy(&version, hdr + 8, 4);
+  std::memcpy(&flags, hdr + 12, 4);
+  std::memcpy(&nn, hdr + 16, 8);
+  std::memcpy(&a, hdr + 24, 4);
+  std::memcpy(&box, hdr + 28, 4);
+  std::memcpy(&mesh, hdr + 32, 4);
+  std::memcpy(&use_tree, hdr + 36, 4);
+  std::memcpy(cosmo, hdr + 40, 16);
+  std::memcpy(split, hdr + 56, 16);
+  std::memcpy(&payload, hdr + 72, 8);
+  std::memcpy(&hash, hdr + 80, 8);
+  if (version != 1 || nn == 0 || nn > 0x7FFFFFFFull || payload != 24 * nn) {
+    std::fclose(f);
+    return set_error(nullptr, CPM_E_INVALID, std::string("cpm_sim_load: unsupported or corrupt header: ") + path);
+  }
+  std::vector<float> xp(6 * nn);
+  const bool ok = std::fread(xp.data(), 1, payload, f) == payload;
+  std::fclose(f);
+  if (!ok || fnv1a64(reinterpret_cast<const unsigned char*>(xp.data()), payload, 0xCBF29CE484222325ull) != hash)
+    return set_error(nullptr, CPM_E_INVALID, std::string("cpm_sim_load: truncated or corrupt payload: ") + path);
+  cpm_sim_params P{};
+  P.cosmo = cpm_cosmology{cosmo[0], cosmo[1], cosmo[2], cosmo[3]};
+  P.box_size = box;
+  P.mesh_n = mesh;
+  P.n_particles = nn;
+  P.use_tree = use_tree;
+  P.split = cpm_force_split{split[0], split[1], split[2], split[3]};
+  P.flags = flags | extra_flags;
+  return cpm_sim_create(&P, xp.data(), xp.data() + 3 * nn, a, out);
+}
+
+int cpm_step_factors(const cpm_cosmology* c, double a0, double a1, int fp64, double* k1, double* d, double* k2) {
+  if (!c || !k1 || !d || !k2) return set_error(nullptr, CPM_E_INVALID, "cpm_step_factors: null pointer");
+  if (!(a0 > 0.0) || !(a1 > 0.0)) return set_error(nullptr, CPM_E_INVALID, "cpm_step_factors: a0, a1 must be > 0");
+  if (!fp64) {  // the reference's f32 arithmetic on the host
+    const float fa0 = (float)a0, fa1 = (float)a1;
+    const float am = midpoint(*c, fa0, fa1);
+    *k1 = kick_factor(*c, fa0, am);
+    *d = drift_factor(*c, fa0, fa1);
+    *k2 = kick_factor(*c, am, fa1);
+    return CPM_OK;
+  }
+  int rc = check_device_once(nullptr);
+  if (rc) return rc;
+  DevBuf b;
+  cudaError_t e = ensure(b, sizeof(StepScalars));
+  if (e == cudaSuccess) {
+    launch_step_factors64(as<StepScalars>(b), *c, a0, a1, 1.0, 1.0, 1.0, nullptr);
+    StepScalars v{};
+    e = cudaMemcpy(&v, b.p, sizeof(v), cudaMemcpyDeviceToHost);
+    *k1 = v.k1;
+    *d = v.d64;
+    *k2 = v.k2;
+  }
+  release(b);
+  if (e != cudaSuccess) return set_error(nullptr, CPM_E_CUDA, std::string("cpm_step_factors: ") + cudaGetErrorString(e));
+  return CPM_OK;
+}
+
+int cpm_sim_set_learned(cpm_sim* s, cpm_net* net, float delta_threshold, float in_scale) {
+  if (!s) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_set_learned: sim is NULL");
+  if (net && net_mesh(net) != s->P.mesh_n)
+    return set_error(&s->err, CPM_E_MESH_MISMATCH, "cpm_sim_set_learned: the net's mesh differs from the simulation's");
+  if (net && !s->P.use_tree)
+    return set_error(&s->err, CPM_E_INVALID, "cpm_sim_set_learned: a pure PM simulation has no short-range force");
+  if (net && (!std::isfinite(delta_threshold) || !(in_scale > 0.0f) || !std::isfinite(in_scale)))
+    return set_error(&s->err, CPM_E_INVALID, "cpm_sim_set_learned: threshold must be finite and in_scale > 0");
+  if (net) {
+    for (DevBuf* b : {&s->flag, &s->offset, &s->list}) SIM_CU(s, ensure(*b, s->n * sizeof(uint32_t)));
+    SIM_CU(s, ensure(s->list_n, sizeof(uint32_t)));
+    SIM_CU(s, cudaMemsetAsync(s->list_n.p, 0, sizeof(uint32_t), s->stream));
+  }
+  SIM_CU(s, cudaStreamSynchronize(s->stream));
+  // the captured step graphs hold the previous force assembly: capture again
+  for (int q = 0; q < 2; ++q) {
+    if (s->graph[q]) cudaGraphExecDestroy(s->graph[q]);
+    s->graph[q] = nullptr;
+    s->warm[q] = false;
+    s->no_graph[q] = false;
+  }
+  s->net = net;
+  s->net_threshold = delta_threshold;
+  s->net_in_scale = in_scale;
+  return CPM_OK;
+}
+
+int cpm_sim_short_range(cpm_sim* s, float* sr3) {
+  if (!s || !sr3) return set_error(s ? &s->err : nullptr, CPM_E_INVALID, "cpm_sim_short_range: null pointer");
+  if (!s->P.use_tree || !s->tree.geo.p)
+    return set_error(&s->err, CPM_E_INVALID, "cpm_sim_short_range: the simulation has no tree");
+  const size_t n = s->n;
+  SIM_CU(s, ensure(s->host_tmp, 3 * n * sizeof(float)));
+  // the tree of the last force evaluation was built on the current positions (the kick that ends a
+  // step changes the momenta only)
+  const float k = tree_coupling(s->P.cosmo.omega_m, s->box, s->a, n);
+  launch_tree_walk(s->tree, as<float>(s->x), n, s->box, s->P.split, k, as<float>(s->host_tmp), 0, nullptr,
+                   as<DevStatus>(s->status), s->stream);
+  launch_scatter3(as<float>(s->host_tmp), as<uint32_t>(s->id), n, as<float>(s->x2), s->stream);
+  SIM_CU(s, cudaMemcpyAsync(sr3, s->x2.p, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+  return sim_check(s);
+}
+
+int cpm_sim_learned_walked(cpm_sim* s, uint64_t* walked) {
+  if (!s || !walked) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_learned_walked: null pointer");
+  SIM_CU(s, cudaStreamSynchronize(s->stream));
+  uint32_t v = 0;
+  if (s->net && s->list_n.p) SIM_CU(s, cudaMemcpy(&v, s->list_n.p, sizeof(v), cudaMemcpyDeviceToHost));
+  *walked = s->net ? (uint64_t)v : (uint64_t)s->n;
+  return CPM_OK;
+}
+
 void* cpm_sim_stream(cpm_sim* s) { return s ? (void*)s->stream : nullptr; }
 
 int cpm_sim_graphs(cpm_sim* s) { return s ? (s->graph[0] ? 1 : 0) + (s->graph[1] ? 1 : 0) : 0; }
@@ -571,7 +798,8 @@ int cpm_sim_destroy(cpm_sim* s) {
   for (DevBuf* b : {&s->sort.keys_alt, &s->sort.vals_alt, &s->sort.block_hist, &s->sort.scan_tmp, &s->tree.geo,
                     &s->tree.mass, &s->tree.link, &s->tree.counters, &s->tree.prefix, &s->tree.scan_tmp, &s->tree.x4, &s->x, &s->p,
                     &s->acc, &s->id, &s->x2, &s->p2, &s->id2, &s->keys, &s->vals, &s->fx, &s->gx, &s->gy, &s->gz,
-                    &s->spec, &s->status, &s->counters, &s->pk, &s->q, &s->q2, &s->snap})
+                    &s->spec, &s->status, &s->counters, &s->pk, &s->q, &s->q2, &s->snap, &s->flag, &s->offset,
+                    &s->list, &s->list_n, &s->scan_tmp})
     release(*b);
   tree_walk_free(s->tree);
   release(s->host_tmp);

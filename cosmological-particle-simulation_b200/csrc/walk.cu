@@ -361,12 +361,17 @@ __global__ void __launch_bounds__(WALK_THREADS) k_tree_walk(const uint4* __restr
                                                             const float4* __restrict__ x4, size_t n, WalkParams w,
                                                             const float* __restrict__ far, float* __restrict__ acc3,
                                                             int accumulate, unsigned long long* counters,
-                                                            DevStatus* st, const float* __restrict__ k_dev) {
+                                                            DevStatus* st, const float* __restrict__ k_dev,
+                                                            const uint32_t* __restrict__ list,
+                                                            const uint32_t* __restrict__ list_n) {
   __shared__ WalkShared shared[WALK_WARPS];
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const size_t i = ((size_t)blockIdx.x * WALK_WARPS + warp) * 32 + lane;
-  const bool valid = i < n;
+  // Lane t of the grid walks for sorted particle t, or, with a list, for particle list[t] (t below
+  // *list_n): the list keeps the sorted order, so a warp's particles stay spatially coherent.
+  const size_t t = ((size_t)blockIdx.x * WALK_WARPS + warp) * 32 + lane;
+  const bool valid = list ? t < (size_t)*list_n : t < n;
+  const size_t i = list ? (valid ? (size_t)list[t] : 0) : t;
   const unsigned group = __ballot_sync(FULL, valid);
   if (group == 0) return;
   WalkShared& sh = shared[warp];
@@ -660,7 +665,7 @@ void tree_walk_free(TreeNodes& t) {
 
 void launch_tree_walk(const TreeNodes& t, const float* sorted_x3, size_t n, float box, const cpm_force_split& split,
                       float k, float* acc3, int accumulate, TreeCounters* counters, DevStatus* st, cudaStream_t s,
-                      const float* k_dev) {
+                      const float* k_dev, const uint32_t* list, const uint32_t* list_n) {
   if (n == 0) return;
   TreeNodes& tm = const_cast<TreeNodes&>(t);
   if (!tm.walk_fit) tm.walk_fit = new FitCache();
@@ -703,7 +708,8 @@ void launch_tree_walk(const TreeNodes& t, const float* sorted_x3, size_t n, floa
   k_tree_walk<<<blocks, WALK_THREADS, 0, s>>>(static_cast<const uint4*>(t.link.p), static_cast<const float4*>(t.geo.p),
                                               static_cast<const float4*>(t.mass.p), as<float4>(tm.x4), n, w,
                                               static_cast<const float*>(fc.far_dev.p), acc3, accumulate,
-                                              reinterpret_cast<unsigned long long*>(counters), st, k_dev);
+                                              reinterpret_cast<unsigned long long*>(counters), st, k_dev, list,
+                                              list_n);
 }
 
 }  // namespace cpm

@@ -1,0 +1,173 @@
+#!/usr/bin/env python
+"""Trains the learned short-range net on the GPU and writes its weights.
+
+Training data: (density, tree-force) pairs from plain TreePM runs of 128^3 particles on a 256^3 mesh
+in a 128 Mpc/h box (the resolution of the 256^3 / 512^3 headline run: 0.5 Mpc/h cells, 1/8 particle
+per cell), seeds 1000-1015, Zel'dovich ICs at z = 49 (Omega_m 0.3, Omega_L 0.7, h 0.7, sigma8 0.8,
+n_s 0.96), 128 KDK steps uniform in ln a, snapshots at z = 3, 1, 0.5 and 0. For each snapshot the
+sample is the density contrast mesh, the particle positions and, as the target, the tree's
+short-range force (tree.rs:314-323) divided by the field scale K(a) (N / n^3) / h; only particles
+whose CIC density contrast is below the threshold (they are the net's) enter the loss, which is the
+relative squared error of the sample. Held-out seed 2000 is the validation set.
+
+Every computation runs in libcpm_cuda.so: the plain runs, the tree forces, and the training step
+(forward convolutions, CIC gather and loss, backward convolutions and weight gradients on the
+tcgen05 tensor cores, Adam).
+
+  python cosmological-particle-simulation_b200/train_net.py --out PATH.npz [--iters 1500]
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import math
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE.parent))
+cpm = importlib.import_module(HERE.name)
+
+COSMO = dict(omega_r=0.0, omega_m=0.3, omega_l=0.7, h0=70.0)
+N_S, SIGMA8, A_INIT, THETA, SOFT = 0.96, 0.8, 0.02, 0.5, 1.0 / 30.0
+SNAP_Z = (3.0, 1.0, 0.5, 0.0)
+DELTA_THRESHOLD = 50.0
+DEFAULT_WEIGHTS = HERE / "weights" / "short_range_net.npz"
+
+
+def field_scale(omega_m: float, box: float, a: float, n_part: int, mesh: int) -> float:
+    """K(a) (N / M) / h, with K(a) = 1.5 Omega_m L^3 / (4 pi a N) (integrator.rs:150-152)."""
+    k = 1.5 * omega_m * box ** 3 / (4.0 * math.pi * a * n_part)
+    return k * (n_part / mesh ** 3) / (box / mesh)
+
+
+def snapshot_steps(steps_total: int) -> list[int]:
+    """Steps of the ln-a schedule (runner.rs:240) closest to the snapshot redshifts."""
+    out = []
+    for z in SNAP_Z:
+        a = 1.0 / (1.0 + z)
+        out.append(int(round(steps_total * math.log(a / A_INIT) / math.log(1.0 / A_INIT))))
+    return out
+
+
+def generate(seed: int, n_side: int = 128, mesh: int = 256, box: float = 128.0, steps_total: int = 128,
+             threshold: float = DELTA_THRESHOLD):
+    """Plain TreePM run; for each snapshot: (a, x, delta mesh, normalised target, loss weight)."""
+    cosmo = cpm.Cosmology(**COSMO)
+    split = cpm.ForceSplit.with_(box, mesh, n_side, SOFT, THETA)
+    sim = cpm.Simulation.from_zeldovich(cosmo, box, mesh, n_side, N_S, SIGMA8, A_INIT, seed, split)
+    sched = cpm.ln_a_schedule(A_INIT, 1.0, steps_total)
+    want = set(snapshot_steps(steps_total))
+    out = []
+    for i, a in enumerate(sched, 1):
+        sim.step_to(a)
+        if i in want:
+            st = sim.state(want_delta=True)
+            sr = sim.short_range()
+            d_i = cpm.Mesh(mesh, box, st["delta"]).interpolate_many(st["x"])
+            scale = field_scale(COSMO["omega_m"], box, st["a"], n_side ** 3, mesh)
+            out.append(dict(a=st["a"], x=st["x"], delta=st["delta"], target=(sr / np.float32(scale)).astype(np.float32),
+                            weight=(d_i < threshold).astype(np.float32), sr=sr, acc=st["acc"]))
+    sim.close()
+    return out
+
+
+def init_weights(seed: int) -> np.ndarray:
+    """He-normal initial weights on the live entries (fan-in 27 x input channels); the last layer 10x smaller."""
+    rng = np.random.default_rng(seed)
+    w = np.zeros((3, 27, 16, 16), np.float32)
+    w[0, :, :, 0] = rng.standard_normal((27, 16)) * math.sqrt(2.0 / 27.0)
+    w[1] = rng.standard_normal((27, 16, 16)) * math.sqrt(2.0 / (27.0 * 16.0))
+    w[2, :, :3, :] = rng.standard_normal((27, 3, 16)) * 0.1 * math.sqrt(2.0 / (27.0 * 16.0))
+    return w
+
+
+def to_device(samples):
+    import torch
+
+    dev = []
+    for s in samples:
+        t = torch.from_numpy(s["target"]).cuda()
+        wgt = torch.from_numpy(s["weight"]).cuda()
+        norm = float((s["target"].astype(np.float64) ** 2 * s["weight"][:, None]).sum())
+        dev.append(dict(a=s["a"], delta=torch.from_numpy(s["delta"]).cuda(), x=torch.from_numpy(s["x"]).cuda(),
+                        target=t, weight=wgt, inv_norm=1.0 / max(norm, 1e-30)))
+    return dev
+
+
+def evaluate(net, samples_host, box: float, in_scale: float, n_part: int) -> dict:
+    """Validation on held-out snapshots, for the particles the net serves (density contrast below the
+    threshold): relative squared error of the net's short-range force against the tree's, its median
+    relative error, and the median error relative to the total (PM + tree) force."""
+    import torch
+
+    mesh = net.n
+    rows = []
+    for s in samples_host:
+        field = net.forward(torch.from_numpy(s["delta"]).cuda(), in_scale=in_scale).cpu().numpy()
+        pred = np.stack([cpm.Mesh(mesh, box, np.ascontiguousarray(field[:, c])).interpolate_many(s["x"])
+                         for c in range(3)], 1).astype(np.float64)
+        g_net = pred * field_scale(COSMO["omega_m"], box, s["a"], n_part, mesh)
+        m = s["weight"] > 0
+        sr = s["sr"][m].astype(np.float64)
+        err = np.linalg.norm(g_net[m] - sr, axis=1)
+        tot = s["acc"][m].astype(np.float64)
+        rows.append(dict(a=float(s["a"]), net_particles=float(m.mean()),
+                         rel_mse=float((err ** 2).sum() / max((sr ** 2).sum(), 1e-300)),
+                         median_rel_err_short_range=float(np.median(err / np.maximum(np.linalg.norm(sr, axis=1), 1e-30))),
+                         median_rel_err_total=float(np.median(err / np.maximum(np.linalg.norm(tot, axis=1), 1e-30)))))
+    return {"snapshots": rows}
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--out", default=str(DEFAULT_WEIGHTS))
+    ap.add_argument("--iters", type=int, default=1500)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--seeds", default="1000-1015")
+    ap.add_argument("--val-seed", type=int, default=2000)
+    ap.add_argument("--n-side", type=int, default=128)
+    ap.add_argument("--threshold", type=float, default=DELTA_THRESHOLD)
+    ap.add_argument("--init-seed", type=int, default=0)
+    args = ap.parse_args()
+    import torch
+
+    lo, hi = (int(v) for v in args.seeds.split("-"))
+    n_side, mesh, box = args.n_side, 2 * args.n_side, float(args.n_side)
+    t0 = time.time()
+    train_host = []
+    for seed in range(lo, hi + 1):
+        train_host += generate(seed, n_side, mesh, box, threshold=args.threshold)
+    val_host = generate(args.val_seed, n_side, mesh, box, threshold=args.threshold)
+    t_data = time.time() - t0
+    samples = to_device(train_host)
+    for s in train_host:  # keep only what evaluation needs on the host
+        s.pop("delta", None)
+    net = cpm.ShortRangeNet(mesh, init_weights(args.init_seed))
+    rng = np.random.default_rng(1)
+    losses = []
+    t1 = time.time()
+    for it in range(args.iters):
+        lr = args.lr * 0.5 * (1.0 + math.cos(math.pi * it / args.iters)) + 1e-5
+        s = samples[int(rng.integers(len(samples)))]
+        losses.append(net.train_step(s["delta"], s["x"], s["target"], s["weight"], box, s["inv_norm"], lr))
+    torch.cuda.synchronize()
+    t_train = time.time() - t1
+    report = {"data_s": round(t_data, 1), "train_s": round(t_train, 1), "iters": args.iters,
+              "samples": len(samples), "loss_first50": float(np.mean(losses[:50])),
+              "loss_last50": float(np.mean(losses[-50:])), "threshold": args.threshold,
+              "validation": evaluate(net, val_host, box, 1.0, n_side ** 3)}
+    Path(args.out).parent.mkdir(parents=True, exist_ok=True)
+    np.savez(args.out, weights=net.weights, threshold=np.float32(args.threshold), in_scale=np.float32(1.0),
+             report=json.dumps(report))
+    print(json.dumps(report, indent=1))
+    net.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

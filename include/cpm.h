@@ -300,6 +300,32 @@ int cpm_walk_kernel_fit_error(float r_split, float r_cut, int samples, double* m
 /* Device-side counters of the last step: nodes, leaf pairs, accepted nodes, kernels launched per step. */
 int cpm_sim_counters(cpm_sim* sim, uint64_t* nodes, uint64_t* leaf_pairs, uint64_t* node_accepts,
                      uint32_t* launches_per_step);
+/* No counterpart in the reference. Attaches a learned short-range net (NULL detaches it): from the
+ * next step on, the short-range force of particles whose CIC-interpolated density contrast is below
+ * delta_threshold is the net's field F = K(a) (N / n^3) / h * net(in_scale * delta), gathered with
+ * the CIC stencil (mesh.rs:72-77); the tree walk (tree.rs:264-310) runs only for the others. The
+ * net's mesh must equal the simulation's (CPM_E_MESH_MISMATCH) and the simulation must use the tree.
+ * The captured step graphs are rebuilt. The simulation does not own the net. */
+int cpm_sim_set_learned(cpm_sim* sim, cpm_net* net, float delta_threshold, float in_scale);
+/* The short-range tree force alone of the current state, tree::accelerations (tree.rs:314-323) on
+ * the current positions with K(a) of the current a, in the caller's particle order (AoS [n][3]).
+ * No counterpart as a separate call in the reference (integrator.rs:149-159 adds it to the PM
+ * force); the training targets of the learned short-range net. */
+int cpm_sim_short_range(cpm_sim* sim, float* sr3);
+/* State file (the snapshot writer the reference planned but did not build, plan.md:160-161): the
+ * positions and momenta in the caller's order, a, and every cpm_sim_params field, with a checksum of
+ * the payload. cpm_sim_load creates a simulation from it (flags | extra_flags) whose next steps equal
+ * those of the saved simulation; CPM_E_INVALID for a missing, foreign or corrupt file. */
+int cpm_sim_save(cpm_sim* sim, const char* path);
+int cpm_sim_load(const char* path, uint32_t extra_flags, cpm_sim** out);
+/* The factors of one KDK step from a0 to a1: k1 = kick_factor(a0, a_mid), d = drift_factor(a0, a1),
+ * k2 = kick_factor(a_mid, a1) with a_mid = midpoint(a0, a1) (integrator.rs:263-297, private there).
+ * fp64 = 0: the reference's f32 Simpson/bisection on the host (what every plain simulation step
+ * uses); fp64 = 1: the FP64 device computation of CPM_SIM_FIXED_POINT steps (256 Simpson
+ * intervals; d is returned unrounded, k1 and k2 as the f32 values the kicks use). */
+int cpm_step_factors(const cpm_cosmology* cosmo, double a0, double a1, int fp64, double* k1, double* d, double* k2);
+/* Particles the last step walked the tree for (all of them without a net). */
+int cpm_sim_learned_walked(cpm_sim* sim, uint64_t* walked);
 /* The CUDA stream the simulation launches on (cudaStream_t), for callers that time with events. */
 void* cpm_sim_stream(cpm_sim* sim);
 int cpm_sim_destroy(cpm_sim* sim);

@@ -90,3 +90,18 @@ def test_walk_pair_kernel_fit_is_accurate(native, r_split, r_cut):
     err = C.c_double()
     assert native.lib().cpm_walk_kernel_fit_error(r_split, r_cut, 20001, C.byref(err)) == 0
     assert err.value < 5e-7, err.value
+
+
+def test_reference_step_factors_on_the_host(cpm, orc):
+    """cpm_step_factors(fp64 = 0) is host code: the reference's f32 kick/drift/midpoint
+    (integrator.rs:263-297), equal to the oracle's restatement bit for bit."""
+    import ctypes as C
+
+    c = orc.cosmology(0.0, 0.3, 0.7, 70.0)
+    cc = cpm.Cosmology(c.omega_r, c.omega_m, c.omega_l, c.h0)
+    for a0, a1 in [(0.02, 0.0206), (0.5, 0.52), (0.97, 1.0)]:
+        k1, d, k2 = C.c_double(), C.c_double(), C.c_double()
+        assert cpm.lib().cpm_step_factors(C.byref(cc), a0, a1, 0, C.byref(k1), C.byref(d), C.byref(k2)) == 0
+        am = orc.midpoint(c, a0, a1)
+        assert (k1.value, d.value, k2.value) == (orc.kick_factor(c, a0, am), orc.drift_factor(c, a0, a1),
+                                                 orc.kick_factor(c, am, a1))

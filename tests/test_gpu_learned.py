@@ -1,0 +1,143 @@
+"""The simulation step with the learned short-range force (cpm_sim_set_learned), through the C ABI.
+
+- With a threshold below every density contrast, every particle keeps the tree walk: the step must
+  equal the plain TreePM step bit for bit (the fused gather's PM sum, the compaction and the walk
+  over the list reproduce the plain kernels exactly).
+- With a threshold above every density contrast, no particle walks: the acceleration is the PM force
+  plus the net's field gathered with the CIC stencil, checked against the net oracle.
+- The gain test (held-out seed 2000, 128^3 particles, 256^3 mesh, 128 steps to z = 0): the trained
+  net (weights/short_range_net.npz, made by train_net.py) against the plain TreePM run from the same
+  ICs: particle-steps/s of both, the median relative force error of the particles the net serves,
+  and the ratio of the final matter P(k) for k <= k_Nyq/2 (the bar is 1 %).
+"""
+import math
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import net_oracle as no
+
+pytestmark = pytest.mark.gpu
+
+ROOT = Path(__file__).resolve().parents[1]
+WEIGHTS = ROOT / "cosmological-particle-simulation_b200" / "weights" / "short_range_net.npz"
+
+
+def rel_rms(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.sqrt(((a - b) ** 2).sum() / max((b ** 2).sum(), 1e-300)))
+
+
+def _sims(cpm, n_side, mesh, box, seed, steps, net=None, threshold=50.0, flags=0):
+    cosmo = cpm.Cosmology(0.0, 0.3, 0.7, 70.0)
+    split = cpm.ForceSplit.with_(box, mesh, n_side, 1.0 / 30.0, 0.5)
+    sim = cpm.Simulation.from_zeldovich(cosmo, box, mesh, n_side, 0.96, 0.8, 0.02, seed, split, flags=flags)
+    if net is not None:
+        sim.set_learned(net, threshold)
+    return sim
+
+
+def test_learned_step_with_every_particle_dense_equals_plain_step(cpm):
+    n_side, mesh, box = 32, 64, 64.0
+    net = cpm.ShortRangeNet(mesh, no.random_weights(3))
+    plain = _sims(cpm, n_side, mesh, box, 42, 0)
+    learned = _sims(cpm, n_side, mesh, box, 42, 0, net, threshold=-1e30)
+    for a in cpm.ln_a_schedule(0.02, 1.0, 64)[:40]:
+        plain.step_to(a)
+        learned.step_to(a)
+    p, q = plain.state(), learned.state()
+    assert np.array_equal(p["x"], q["x"]) and np.array_equal(p["p"], q["p"]) and np.array_equal(p["acc"], q["acc"])
+    assert learned.walked() == n_side ** 3
+    assert learned.graphs() == 2
+    plain.close()
+    learned.close()
+    net.close()
+
+
+def test_learned_step_without_tree_walk_is_pm_plus_net_field(cpm):
+    import torch
+
+    n_side, mesh, box = 32, 64, 64.0
+    w = no.random_weights(4, scale=0.5)
+    net = cpm.ShortRangeNet(mesh, w)
+    sim = _sims(cpm, n_side, mesh, box, 7, 0)
+    for a in cpm.ln_a_schedule(0.02, 1.0, 64)[:48]:
+        sim.step_to(a)
+    st = sim.state(want_delta=True)
+    a = st["a"]
+    # the same positions with the net for every particle (threshold +inf): re-evaluate the force
+    sim.set_learned(net, 1e30)
+    sim.set_state(st["x"], st["p"])
+    got = sim.state()["acc"]
+    assert sim.walked() == 0
+    sim.set_learned(None)
+    sim.set_state(st["x"], st["p"])
+    st2 = sim.state()
+    sr = sim.short_range()
+    pm = st2["acc"].astype(np.float64) - sr.astype(np.float64)
+    # the net's field from the simulation's own density contrast, by the oracle
+    n_part, m = n_side ** 3, mesh ** 3
+    k = 1.5 * 0.3 * box ** 3 / (4.0 * math.pi * a * n_part)
+    scale = k * (n_part / m) / (box / mesh)
+    field = no.forward_bf16(st["delta"], w, 1.0, 1.0, mesh)["field"].astype(np.float64) * scale
+    want = pm + no.cic_gather(field, st["x"], box, mesh)
+    assert rel_rms(got - pm, want - pm) < 2e-3
+    assert rel_rms(got, want) < 1e-4
+    del torch
+    sim.close()
+    net.close()
+
+
+def test_learned_gain_on_held_out_seed(cpm, orc):
+    """Config 5 at 128^3 from held-out seed 2000: the trained net against the plain TreePM run."""
+    import torch
+
+    assert WEIGHTS.exists(), f"{WEIGHTS} is missing: run train_net.py"
+    z = np.load(WEIGHTS)
+    n_side, mesh, box, seed, steps = 128, 256, 128.0, 2000, 128
+    threshold = float(z["threshold"])
+    net = cpm.ShortRangeNet(mesh, z["weights"])
+    sched = cpm.ln_a_schedule(0.02, 1.0, steps)
+    results = {}
+    for name in ("plain", "learned"):
+        sim = _sims(cpm, n_side, mesh, box, seed, steps, net if name == "learned" else None, threshold)
+        stream = torch.cuda.ExternalStream(sim.stream())
+        for a1 in sched[:3]:
+            sim.step_to(a1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for a1 in sched[3:]:
+            sim.step_to(a1)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        st = sim.state()
+        results[name] = dict(rate=n_side ** 3 * (steps - 3) / (ms / 1e3), x=st["x"], acc=st["acc"], sim=sim,
+                             walked=sim.walked())
+    # forces on the final positions of the plain run: learned force assembly vs the plain one
+    plain, learned = results["plain"]["sim"], results["learned"]["sim"]
+    st = plain.state()
+    learned.set_state(st["x"], st["p"])
+    acc_l = learned.state()["acc"].astype(np.float64)
+    acc_p = st["acc"].astype(np.float64)
+    err = np.linalg.norm(acc_l - acc_p, axis=1) / np.maximum(np.linalg.norm(acc_p, axis=1), 1e-30)
+    served = err > 0.0
+    median_err = float(np.median(err[served])) if served.any() else 0.0
+    # final P(k) of the two runs (the oracle's FP64 estimator), k <= k_Nyq / 2
+    shells = mesh // 4
+    _, p_p, c_p = orc.power_spectrum(results["plain"]["x"], box, mesh, shells)
+    _, p_l, c_l = orc.power_spectrum(results["learned"]["x"], box, mesh, shells)
+    ratio = p_l / p_p
+    gain = results["learned"]["rate"] / results["plain"]["rate"]
+    print(f"plain {results['plain']['rate']:.3e} learned {results['learned']['rate']:.3e} particle-steps/s "
+          f"(x{gain:.2f}); walked at z=0: {results['learned']['walked']} of {n_side ** 3}; "
+          f"median rel. force error (net particles) {median_err:.3e}; "
+          f"P(k) ratio range {ratio.min():.4f}..{ratio.max():.4f}")
+    for r in results.values():
+        r["sim"].close()
+    net.close()
+    np.testing.assert_array_equal(c_p, c_l)
+    assert gain > 1.0
+    assert np.all(np.abs(ratio - 1.0) < 0.01), ratio

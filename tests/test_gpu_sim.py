@@ -291,3 +291,75 @@ def test_sim_rejects_bad_arguments(cpm):
     with pytest.raises(cpm.CpmError) as e:
         cpm.Simulation(cpm.Cosmology.lcdm_default(), 1.0, 8, x, np.zeros_like(x), 0.1, None)
     assert e.value.code == -6
+
+
+def test_state_file_round_trip(cpm, tmp_path):
+    """cpm_sim_save / cpm_sim_load: the loaded simulation holds the same x, p and a, and steps on
+    exactly like the saved one; a corrupted file is rejected."""
+    cc = cpm.Cosmology(0.0, 0.3, 0.7, 70.0)
+    split = cpm.ForceSplit.with_(64.0, 64, 32, 1.0 / 30.0, 0.5)
+    sim = cpm.Simulation.from_zeldovich(cc, 64.0, 64, 32, 0.96, 0.8, 0.02, 42, split)
+    sched = cpm.ln_a_schedule(0.02, 1.0, 64)
+    for a1 in sched[:20]:
+        sim.step_to(a1)
+    path = tmp_path / "state.cpm"
+    sim.save(path)
+    other = cpm.Simulation.load(path)
+    s0, s1 = sim.state(), other.state()
+    assert np.array_equal(s0["x"], s1["x"]) and np.array_equal(s0["p"], s1["p"]) and s0["a"] == s1["a"]
+    assert rel_rms(s1["acc"], s0["acc"]) < 1e-6
+    for a1 in sched[20:24]:
+        sim.step_to(a1)
+        other.step_to(a1)
+    s0, s1 = sim.state(), other.state()
+    assert periodic_max_diff(s1["x"], s0["x"], 64.0) < 1e-5
+    raw = bytearray(path.read_bytes())
+    raw[200] ^= 0xFF
+    bad = tmp_path / "bad.cpm"
+    bad.write_bytes(bytes(raw))
+    with pytest.raises(cpm.CpmError) as e:
+        cpm.Simulation.load(bad)
+    assert e.value.code == -1
+    sim.close()
+    other.close()
+
+
+def test_step_factors_fp64_and_reference(cpm, orc):
+    """cpm_step_factors: the f32 path equals the oracle's restatement of integrator.rs:263-297 bit for
+    bit; the FP64 device path (precision mode) agrees with a 4096-interval Simpson and bisection in
+    double to 1e-12 relative (d) and to f32 rounding (k1, k2)."""
+    import ctypes as C
+    import math
+
+    c = orc.cosmology(0.0, 0.3, 0.7, 70.0)
+    cc = cpm.Cosmology(c.omega_r, c.omega_m, c.omega_l, c.h0)
+    L = cpm.lib()
+
+    def factors(a0, a1, fp64):
+        k1, d, k2 = C.c_double(), C.c_double(), C.c_double()
+        assert L.cpm_step_factors(C.byref(cc), a0, a1, fp64, C.byref(k1), C.byref(d), C.byref(k2)) == 0
+        return k1.value, d.value, k2.value
+
+    def e64(a):
+        return math.sqrt(0.3 / a ** 3 + 0.7)
+
+    def simpson(f, lo, hi, m=4096):
+        h = (hi - lo) / m
+        return (f(lo) + f(hi) + sum((4 if i % 2 else 2) * f(lo + i * h) for i in range(1, m))) * h / 3
+
+    kick = lambda a: 1.0 / (a * e64(a))
+    drift = lambda a: 1.0 / (a ** 3 * e64(a))
+    for a0, a1 in [(0.02, 0.0206), (0.3, 0.31), (0.95, 1.0)]:
+        r = factors(a0, a1, 0)
+        am = orc.midpoint(c, a0, a1)
+        assert r == (orc.kick_factor(c, a0, am), orc.drift_factor(c, a0, a1), orc.kick_factor(c, am, a1))
+        half = simpson(kick, a0, a1) / 2
+        lo, hi = a0, a1
+        for _ in range(60):
+            mid = 0.5 * (lo + hi)
+            lo, hi = (mid, hi) if simpson(kick, a0, mid, 512) < half else (lo, mid)
+        am64 = 0.5 * (lo + hi)
+        k1, d, k2 = factors(a0, a1, 1)
+        assert abs(d / simpson(drift, a0, a1) - 1.0) < 1e-12
+        assert abs(k1 / simpson(kick, a0, am64) - 1.0) < 2e-7
+        assert abs(k2 / simpson(kick, am64, a1) - 1.0) < 2e-7
