@@ -25,6 +25,7 @@ SIM_FIXED_POINT = 0x1
 SIM_DECONVOLVE = 0x2
 SIM_TIMING = 0x4
 SIM_NO_GRAPH = 0x8
+SIM_QUADRUPOLE = 0x10
 
 
 class CpmError(RuntimeError):

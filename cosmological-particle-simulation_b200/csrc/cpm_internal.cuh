@@ -229,6 +229,8 @@ struct TreeNodes {
   DevBuf prefix;    // double prefix sums of sorted positions (3 per particle + 3)
   DevBuf scan_tmp;
   DevBuf x4;        // float4 copy of the sorted positions for the walk
+  DevBuf quad;      // per node 2 float4: second moments about the centre of mass (quadrupole mode)
+  bool has_quad = false;  // the last build computed `quad`; the walk then adds quadrupole terms
   size_t capacity = 0;
   void* walk_fit = nullptr;  // fitted pair-force coefficients of the last split (walk.cu)
 };
@@ -239,9 +241,13 @@ struct TreeCounters {
   unsigned long long reserved;
 };
 // Builds the octree over sorted keys/positions (sorted x as AoS f32). Returns the node count
-// through the counters buffer (read by tree_node_count).
+// through the counters buffer (read by tree_node_count). quad_half_max > 0 also computes the second
+// moments of every node with half < quad_half_max (the walk then adds quadrupole terms).
 cudaError_t tree_build(TreeNodes& t, const uint64_t* sorted_keys, const float* sorted_x3, size_t n, float box,
-                       DevStatus* st, cudaStream_t s);
+                       DevStatus* st, cudaStream_t s, float quad_half_max = 0.0f);
+// Half size from which a node can never be accepted by the walk (prune radius r_cut + sqrt(3) half
+// from the centre, centre of mass inside the cube, 2 half < theta r): +inf when theta >= 1/sqrt(3).
+float quad_half_bound(const cpm_force_split& split);
 // Walks the tree for every sorted particle; acc3 (sorted order) receives g_sr, or g + g_sr
 // when `accumulate` (the reference's g[c] += s[c], integrator.rs:154-158).
 // The coupling k is read from *k_dev when k_dev is set. With `list`, only the sorted particles

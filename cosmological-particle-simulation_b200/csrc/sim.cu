@@ -213,8 +213,9 @@ static int sim_accelerations(cpm_sim* s, float a, const StepScalars* dev = nullp
   }
   mark(s, 5);
   if (s->P.use_tree) {
+    const float quad_half = (s->P.flags & CPM_SIM_QUADRUPOLE) ? quad_half_bound(s->P.split) : 0.0f;
     SIM_CU(s, tree_build(s->tree, as<uint64_t>(s->keys), as<float>(s->x), n, s->box, as<DevStatus>(s->status),
-                         s->stream));
+                         s->stream, quad_half));
     mark(s, 6);
     SIM_CU(s, cudaMemsetAsync(s->counters.p, 0, sizeof(TreeCounters), s->stream));
     const float k = tree_coupling(s->P.cosmo.omega_m, s->box, a, n);
@@ -796,7 +797,7 @@ int cpm_sim_destroy(cpm_sim* s) {
   if (s->side) cudaStreamSynchronize(s->side);
   fft_plan_free(s->plan);
   for (DevBuf* b : {&s->sort.keys_alt, &s->sort.vals_alt, &s->sort.block_hist, &s->sort.scan_tmp, &s->tree.geo,
-                    &s->tree.mass, &s->tree.link, &s->tree.counters, &s->tree.prefix, &s->tree.scan_tmp, &s->tree.x4, &s->x, &s->p,
+                    &s->tree.mass, &s->tree.link, &s->tree.counters, &s->tree.prefix, &s->tree.scan_tmp, &s->tree.x4, &s->tree.quad, &s->x, &s->p,
                     &s->acc, &s->id, &s->x2, &s->p2, &s->id2, &s->keys, &s->vals, &s->fx, &s->gx, &s->gy, &s->gz,
                     &s->spec, &s->status, &s->counters, &s->pk, &s->q, &s->q2, &s->snap, &s->flag, &s->offset,
                     &s->list, &s->list_n, &s->scan_tmp})

@@ -356,8 +356,47 @@ __global__ void k_tree_com(const uint4* __restrict__ link, const double* __restr
   }
 }
 
+// Second moments about the centre of mass, T = sum_j (x_j - com)(x_j - com)^T over the node's
+// particles (unit masses), one warp per node with FP64 sums; stored as (Txx, Tyy, Tzz, Txy),
+// (Txz, Tyz, 0, 0). Nodes with half >= half_max are never accepted by the walk and get zeros.
+// No counterpart in the reference, whose tree carries monopoles only (tree.rs:68-80).
+__global__ void k_tree_quad(const uint4* __restrict__ link, const float4* __restrict__ geo,
+                            const float4* __restrict__ mass, const float* __restrict__ x3, float4* __restrict__ quad,
+                            const uint32_t* __restrict__ counters, uint32_t capacity, float half_max) {
+  uint32_t total = 0;
+  for (int j = 0; j <= KEY_LEVELS; ++j) total += counters[j];
+  total = min(total, capacity);
+  const int lane = threadIdx.x & 31;
+  const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t node = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); node < total; node += warps) {
+    double t[6] = {0, 0, 0, 0, 0, 0};
+    if (geo[node].w < half_max) {
+      const uint4 L = link[node];
+      const float4 M = mass[node];
+      for (uint32_t i = L.x + lane; i < L.y; i += 32) {
+        const double dx = (double)x3[3 * (size_t)i] - M.x, dy = (double)x3[3 * (size_t)i + 1] - M.y,
+                     dz = (double)x3[3 * (size_t)i + 2] - M.z;
+        t[0] += dx * dx;
+        t[1] += dy * dy;
+        t[2] += dz * dz;
+        t[3] += dx * dy;
+        t[4] += dx * dz;
+        t[5] += dy * dz;
+      }
+#pragma unroll
+      for (int k = 0; k < 6; ++k)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t[k] += __shfl_xor_sync(0xffffffffu, t[k], o);
+    }
+    if (lane == 0) {
+      quad[2 * (size_t)node] = make_float4((float)t[0], (float)t[1], (float)t[2], (float)t[3]);
+      quad[2 * (size_t)node + 1] = make_float4((float)t[4], (float)t[5], 0.0f, 0.0f);
+    }
+  }
+}
+
 cudaError_t tree_build(TreeNodes& t, const uint64_t* sorted_keys, const float* sorted_x3, size_t n, float box,
-                       DevStatus* st, cudaStream_t s) {
+                       DevStatus* st, cudaStream_t s, float quad_half_max) {
   if (n == 0) return cudaSuccess;
   const size_t cap = 2 * n + 64;
   cudaError_t e;
@@ -392,6 +431,13 @@ cudaError_t tree_build(TreeNodes& t, const uint64_t* sorted_keys, const float* s
   k_pos_prefix<<<(unsigned)nb, PS_THREADS, 0, s>>>(sorted_x3, n, partial, P);
   count_launch();
   k_tree_com<<<BUILD_BLOCKS, BUILD_THREADS, 0, s>>>(link, P, as<float4>(t.mass), counters, (uint32_t)t.capacity);
+  t.has_quad = quad_half_max > 0.0f;
+  if (t.has_quad) {
+    if ((e = ensure(t.quad, 2 * t.capacity * sizeof(float4))) != cudaSuccess) return e;
+    count_launch();
+    k_tree_quad<<<BUILD_BLOCKS, BUILD_THREADS, 0, s>>>(link, geo, as<float4>(t.mass), sorted_x3, as<float4>(t.quad),
+                                                       counters, (uint32_t)t.capacity, quad_half_max);
+  }
   return cudaGetLastError();
 }
 

@@ -355,6 +355,38 @@ __device__ __forceinline__ void chunk_forces(const WalkShared& sh, uint32_t pm, 
   }
 }
 
+// Quadrupole term of an accepted node (no counterpart in the reference, whose nodes are monopoles,
+// tree.rs:68-80): the second-order Taylor term of a = sum_j g(|d_j|) d_j about the centre of mass,
+// d_j = D + e_j with sum_j e_j = 0, T = sum_j e_j e_j^T, g(r) = S(r / 2 r_s) (r^2 + eps^2)^(-3/2):
+//   da = (1/2) [ h (D.T.D) D + (g'/r) (tr(T) D + 2 T D) ],   h = (g'' - g'/r) / r^2,
+// with S' = -(2/sqrt(pi)) u^2 e^{-u^2} / r_s and S'' = -(2/sqrt(pi)) u (1 - u^2) e^{-u^2} / r_s^2
+// (u = r / 2 r_s). Unit coupling, like the walk's sums; precision mode only (CUDA's erfcf / expf).
+__device__ __forceinline__ void quad_term(float d0, float d1, float d2, const float4& Q0, const float4& Q1,
+                                          const WalkParams& w, float2& A0, float2& A1, float2& A2) {
+  const float r2 = d0 * d0 + d1 * d1 + d2 * d2;
+  if (!(r2 > 0.0f)) return;
+  const float r = sqrtf(r2), inv_r = 1.0f / r;
+  const float rs = 0.5f / w.inv_two_rs;
+  const float u = r * w.inv_two_rs, e = expf(-u * u);
+  const float S = erfcf(u) + TWO_OVER_SQRT_PI * u * e;
+  const float S1 = -TWO_OVER_SQRT_PI * u * u * e / rs;
+  const float S2 = -TWO_OVER_SQRT_PI * u * (1.0f - u * u) * e / (rs * rs);
+  const float q = r2 + w.eps2, iq = 1.0f / q, rq = rsqrtf(q);
+  const float P = rq * iq, P1 = -3.0f * r * P * iq, P2 = -3.0f * P * iq + 15.0f * r2 * P * iq * iq;
+  const float g1 = S1 * P + S * P1;
+  const float g2 = S2 * P + 2.0f * S1 * P1 + S * P2;
+  const float h = (g2 - g1 * inv_r) / r2;
+  const float td0 = Q0.x * d0 + Q0.w * d1 + Q1.x * d2;
+  const float td1 = Q0.w * d0 + Q0.y * d1 + Q1.y * d2;
+  const float td2 = Q1.x * d0 + Q1.y * d1 + Q0.z * d2;
+  const float dtd = d0 * td0 + d1 * td1 + d2 * td2, tr = Q0.x + Q0.y + Q0.z;
+  const float a = 0.5f * h * dtd, b = 0.5f * g1 * inv_r;
+  A0.y += a * d0 + b * (tr * d0 + 2.0f * td0);
+  A1.y += a * d1 + b * (tr * d1 + 2.0f * td1);
+  A2.y += a * d2 + b * (tr * d2 + 2.0f * td2);
+}
+
+template <bool QUAD>
 __global__ void __launch_bounds__(WALK_THREADS) k_tree_walk(const uint4* __restrict__ link,
                                                             const float4* __restrict__ geo,
                                                             const float4* __restrict__ mass,
@@ -363,7 +395,8 @@ __global__ void __launch_bounds__(WALK_THREADS) k_tree_walk(const uint4* __restr
                                                             int accumulate, unsigned long long* counters,
                                                             DevStatus* st, const float* __restrict__ k_dev,
                                                             const uint32_t* __restrict__ list,
-                                                            const uint32_t* __restrict__ list_n) {
+                                                            const uint32_t* __restrict__ list_n,
+                                                            const float4* __restrict__ quad) {
   __shared__ WalkShared shared[WALK_WARPS];
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -405,7 +438,7 @@ __global__ void __launch_bounds__(WALK_THREADS) k_tree_walk(const uint4* __restr
   // The current batch: sibling nodes first .. first + count - 1, walked by the lanes in mask.
   // Lane c < count copies node first + c into shared buffer `cur` asynchronously; the next batch
   // is copied into the other buffer while the current one is summed.
-  uint32_t b_count = 1, b_mask = group;
+  uint32_t b_count = 1, b_mask = group, b_first = 0;
   int cur = 0;
   if (lane == 0) {
     cp_async16(&sh.geo[0][0], geo);
@@ -523,10 +556,11 @@ __global__ void __launch_bounds__(WALK_THREADS) k_tree_walk(const uint4* __restr
 
     // Start copying the next batch; the copies complete during the work below.
     const bool more = sp > 0;
-    uint32_t nx_count = 0, nx_mask = 0;
+    uint32_t nx_count = 0, nx_mask = 0, nx_first = 0;
     if (more) {
       const uint2 top = sh.stack[--sp];
       const uint32_t first = top.x;
+      nx_first = first;
       nx_count = sh.count[sp];
       nx_mask = top.y;
       if ((uint32_t)lane < nx_count) {
@@ -546,6 +580,10 @@ __global__ void __launch_bounds__(WALK_THREADS) k_tree_walk(const uint4* __restr
       A0.x = fmaf(-s0, f, A0.x);
       A1.x = fmaf(-s1, f, A1.x);
       A2.x = fmaf(-s2, f, A2.x);
+      if constexpr (QUAD) {
+        const size_t node = (size_t)b_first + (size_t)c;
+        quad_term(s0, s1, s2, __ldg(quad + 2 * node), __ldg(quad + 2 * node + 1), w, A0, A1, A2);
+      }
       ++n_accepts;
     }
 
@@ -603,6 +641,7 @@ __global__ void __launch_bounds__(WALK_THREADS) k_tree_walk(const uint4* __restr
     if (!more) break;
     b_count = nx_count;
     b_mask = nx_mask;
+    b_first = nx_first;
     cur ^= 1;
   }
   asm volatile("cp.async.wait_all;\n" ::: "memory");
@@ -705,11 +744,19 @@ void launch_tree_walk(const TreeNodes& t, const float* sorted_x3, size_t n, floa
   const size_t groups = (n + 31) / 32;
   const unsigned blocks = (unsigned)((groups + WALK_WARPS - 1) / WALK_WARPS);
   count_launch();
-  k_tree_walk<<<blocks, WALK_THREADS, 0, s>>>(static_cast<const uint4*>(t.link.p), static_cast<const float4*>(t.geo.p),
-                                              static_cast<const float4*>(t.mass.p), as<float4>(tm.x4), n, w,
-                                              static_cast<const float*>(fc.far_dev.p), acc3, accumulate,
-                                              reinterpret_cast<unsigned long long*>(counters), st, k_dev, list,
-                                              list_n);
+  auto kernel = t.has_quad ? k_tree_walk<true> : k_tree_walk<false>;
+  kernel<<<blocks, WALK_THREADS, 0, s>>>(static_cast<const uint4*>(t.link.p), static_cast<const float4*>(t.geo.p),
+                                         static_cast<const float4*>(t.mass.p), as<float4>(tm.x4), n, w,
+                                         static_cast<const float*>(fc.far_dev.p), acc3, accumulate,
+                                         reinterpret_cast<unsigned long long*>(counters), st, k_dev, list, list_n,
+                                         t.has_quad ? static_cast<const float4*>(t.quad.p) : nullptr);
+}
+
+float quad_half_bound(const cpm_force_split& split) {
+  const double th = split.theta;
+  const double den = 2.0 - 2.0 * std::sqrt(3.0) * th;
+  if (!(den > 0.0)) return INFINITY;
+  return (float)(1.01 * th * (double)split.r_cut / den);
 }
 
 }  // namespace cpm

@@ -245,6 +245,12 @@ typedef struct {
  * one of two captured graphs (the sorted particle buffers alternate between them); CPM_SIM_TIMING
  * also runs every step uncaptured. */
 #define CPM_SIM_NO_GRAPH 0x8u
+/* Quadrupole moments in the tree (no counterpart in the reference, whose nodes are monopoles,
+ * tree.rs:68-80): every node that the walk can accept carries the second moments of its particles
+ * about their centre of mass, and an accepted node adds the second-order Taylor term of the
+ * short-range kernel to its monopole force. Precision mode (use with CPM_SIM_FIXED_POINT); it
+ * changes the forces, so plain parity with the reference holds without it. */
+#define CPM_SIM_QUADRUPOLE 0x10u
 
 /* integrator.rs:54-79 `Simulation::new`: uploads x3, p3 (AoS [n][3]) and computes the initial
  * acceleration at a0. */

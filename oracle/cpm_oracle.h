@@ -142,6 +142,11 @@ void orc_power_spectrum(const float* x3, size_t np, float box, int n, int n_shel
 void orc64_accelerations(const float* x3, size_t n, double box, int mesh_n, double omega_m, double a,
                          const orc_split* split, double k_tree, const uint32_t* sample, size_t n_sample,
                          double* acc3);
+/* orc64_accelerations with quadrupole terms at accepted nodes when `quadrupole` (the library's
+ * CPM_SIM_QUADRUPOLE; the reference's nodes are monopoles). */
+void orc64_accelerations_ex(const float* x3, size_t n, double box, int mesh_n, double omega_m, double a,
+                            const orc_split* split, double k_tree, const uint32_t* sample, size_t n_sample,
+                            double* acc3, int quadrupole);
 
 int orc_num_threads(void);
 

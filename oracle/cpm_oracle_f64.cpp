@@ -58,6 +58,7 @@ double wavenumber64(size_t i, size_t n, double box) {
 
 struct Node64 {
   double center[3], half, com[3];
+  double quad[6];  // second moments about com: xx, yy, zz, xy, xz, yz (library quadrupole mode)
   uint32_t count, start, end;
   uint32_t children[8];
 };
@@ -90,6 +91,17 @@ struct Tree64 {
     for (int k = 0; k < 3; ++k) {
       nd.center[k] = center[k];
       nd.com[k] = com[k] / (double)(end - start);
+    }
+    for (double& q : nd.quad) q = 0.0;
+    for (size_t t = start; t < end; ++t) {
+      const double* p = pos + 3 * (size_t)order[t];
+      const double e0 = p[0] - nd.com[0], e1 = p[1] - nd.com[1], e2 = p[2] - nd.com[2];
+      nd.quad[0] += e0 * e0;
+      nd.quad[1] += e1 * e1;
+      nd.quad[2] += e2 * e2;
+      nd.quad[3] += e0 * e1;
+      nd.quad[4] += e0 * e2;
+      nd.quad[5] += e1 * e2;
     }
     nd.half = half;
     nd.count = (uint32_t)(end - start);
@@ -134,8 +146,11 @@ struct Tree64 {
     }
   }
 
-  // tree.rs:264-310 in double (opening test 2 half < theta r).
-  void accel_on(size_t i, const orc_split& s, double kk, std::vector<uint32_t>& stack, double* acc) const {
+  // tree.rs:264-310 in double (opening test 2 half < theta r). With `quad`, an accepted node also
+  // adds the second-order Taylor term of sum_j g(|d_j|) d_j about its centre of mass (the library's
+  // CPM_SIM_QUADRUPOLE): (1/2)[h (D.T.D) D + (g'/r)(tr T D + 2 T D)], h = (g'' - g'/r) / r^2.
+  void accel_on(size_t i, const orc_split& s, double kk, std::vector<uint32_t>& stack, double* acc,
+                bool quad = false) const {
     const double* xi = pos + 3 * i;
     const double rs = s.r_split, rc = s.r_cut, eps2 = (double)s.softening * s.softening, theta = s.theta;
     auto pair = [&](const double* d, double mass) {
@@ -171,6 +186,19 @@ struct Tree64 {
         if (2.0 * nd.half < theta * r) {
           const double d[3] = {-to[0], -to[1], -to[2]};
           pair(d, (double)nd.count);
+          if (quad && r > 0.0) {
+            const double D[3] = {to[0], to[1], to[2]};  // from the particle to the centre of mass
+            const double r2 = r * r, u = r / (2.0 * rs), e = std::exp(-u * u), c = 2.0 / std::sqrt(PI);
+            const double S = std::erfc(u) + c * u * e, S1 = -c * u * u * e / rs, S2 = -c * u * (1 - u * u) * e / (rs * rs);
+            const double q = r2 + eps2, P = 1.0 / (q * std::sqrt(q)), P1 = -3.0 * r * P / q;
+            const double P2 = -3.0 * P / q + 15.0 * r2 * P / (q * q);
+            const double g1 = S1 * P + S * P1, g2 = S2 * P + 2.0 * S1 * P1 + S * P2, h = (g2 - g1 / r) / r2;
+            const double* T = nd.quad;
+            const double td[3] = {T[0] * D[0] + T[3] * D[1] + T[4] * D[2], T[3] * D[0] + T[1] * D[1] + T[5] * D[2],
+                                  T[4] * D[0] + T[5] * D[1] + T[2] * D[2]};
+            const double dtd = D[0] * td[0] + D[1] * td[1] + D[2] * td[2], tr = T[0] + T[1] + T[2];
+            for (int k = 0; k < 3; ++k) acc[k] += kk * 0.5 * (h * dtd * D[k] + g1 / r * (tr * D[k] + 2.0 * td[k]));
+          }
         } else {
           for (int o = 0; o < 8; ++o)
             if (nd.children[o] != NONE) stack.push_back(nd.children[o]);
@@ -184,9 +212,19 @@ struct Tree64 {
 
 extern "C" {
 
+void orc64_accelerations_ex(const float* x3, size_t n, double box, int mesh_n, double omega_m, double a,
+                            const orc_split* split, double k_tree, const uint32_t* sample, size_t n_sample,
+                            double* acc3, int quadrupole);
+
 void orc64_accelerations(const float* x3, size_t n, double box, int mesh_n, double omega_m, double a,
                          const orc_split* split, double k_tree, const uint32_t* sample, size_t n_sample,
                          double* acc3) {
+  orc64_accelerations_ex(x3, n, box, mesh_n, omega_m, a, split, k_tree, sample, n_sample, acc3, 0);
+}
+
+void orc64_accelerations_ex(const float* x3, size_t n, double box, int mesh_n, double omega_m, double a,
+                            const orc_split* split, double k_tree, const uint32_t* sample, size_t n_sample,
+                            double* acc3, int quadrupole) {
   const size_t mn = (size_t)mesh_n;
   const size_t m = mn * mn * mn;
   std::vector<double> x(3 * n);
@@ -256,7 +294,7 @@ void orc64_accelerations(const float* x3, size_t n, double box, int mesh_n, doub
       double a3[3];
 #pragma omp for schedule(dynamic, 64)
       for (long long s = 0; s < (long long)n_sample; ++s) {
-        tree.accel_on(sample[s], *split, k_tree, stack, a3);
+        tree.accel_on(sample[s], *split, k_tree, stack, a3, quadrupole != 0);
         for (int k = 0; k < 3; ++k) acc3[3 * s + k] += a3[k];
       }
     }

@@ -106,6 +106,8 @@ def lib() -> C.CDLL:
         "orc_num_threads": (i, []),
         "orc64_accelerations": (None, [f32p, sz, C.c_double, i, C.c_double, C.c_double, C.c_void_p, C.c_double,
                                        u32p, sz, f64p]),
+        "orc64_accelerations_ex": (None, [f32p, sz, C.c_double, i, C.c_double, C.c_double, C.c_void_p, C.c_double,
+                                          u32p, sz, f64p, i]),
         "orc_step_sample": (None, [C.POINTER(Cosmology), fl, i, f32p, f32p, f32p, sz, fl, fl, C.c_void_p, u32p, sz,
                                    i, f64p, C.c_void_p]),
     }
@@ -424,16 +426,17 @@ def tree_coupling64(omega_m: float, box: float, a: float, n: int) -> float:
 
 
 def accelerations_f64(x, box: float, mesh_n: int, omega_m: float, a: float, split: Split | None,
-                      sample) -> np.ndarray:
+                      sample, quadrupole: bool = False) -> np.ndarray:
     """FP64 build: PM + short-range tree force (coupling tree_coupling64) at the sampled particles,
-    everything in double precision; returns (len(sample), 3) float64."""
+    everything in double precision; `quadrupole` adds the quadrupole terms of accepted nodes (the
+    library's CPM_SIM_QUADRUPOLE). Returns (len(sample), 3) float64."""
     x = _f32(x)
     sample = np.ascontiguousarray(sample, np.uint32)
     out = np.empty((len(sample), 3), np.float64)
     k = tree_coupling64(omega_m, box, a, len(x))
     sp = C.cast(C.pointer(split), C.c_void_p) if split is not None else None
-    lib().orc64_accelerations(x, len(x), float(box), int(mesh_n), float(omega_m), float(a), sp, k, sample,
-                              len(sample), out)
+    lib().orc64_accelerations_ex(x, len(x), float(box), int(mesh_n), float(omega_m), float(a), sp, k, sample,
+                                 len(sample), out, 1 if quadrupole else 0)
     return out
 
 

@@ -79,3 +79,38 @@ def test_precision_config3(cpm, orc):
     for key in ("start", "end"):
         r = res[key]
         assert r["acc_rel_rms"] < 1e-3 and r["pk_counts_equal"] and r["pk_max_rel"] < 1e-3, r
+
+
+def test_quadrupole_forces_match_fp64_oracle_and_beat_monopoles(cpm, orc):
+    """CPM_SIM_QUADRUPOLE (no counterpart in the reference): the GPU's quadrupole tree force equals the
+    FP64 oracle's quadrupole force to 1e-5 relative RMS of the total, and its short-range error
+    against the exact pair sum (the FP64 oracle at theta = 0) is at most a third of the monopole's."""
+    rng = np.random.default_rng(4)
+    box, mesh, n_side = 32.0, 32, 27
+    centres = rng.uniform(0.0, box, (20, 3))
+    x = np.mod(centres[rng.integers(0, 20, n_side ** 3)] + rng.normal(0.0, 1.0, (n_side ** 3, 3)),
+               box).astype(np.float32)
+    p = np.zeros_like(x)
+    split = orc.split_with(box, mesh, n_side, 1.0 / 30.0, 0.5)
+    exact_split = orc.split_with(box, mesh, n_side, 1.0 / 30.0, 0.0)
+    cc = cpm.Cosmology(*COSMO)
+    cs = cpm.ForceSplit(split.r_split, split.r_cut, split.softening, split.theta)
+    a = 1.0
+    nat = cpm._native
+    quad = cpm.Simulation(cc, box, mesh, x, p, a, cs, flags=nat.SIM_QUADRUPOLE).state()["acc"]
+    mono = cpm.Simulation(cc, box, mesh, x, p, a, cs).state()["acc"]
+    sample = np.arange(0, len(x), 29).astype(np.uint32)
+    ref_q = orc.accelerations_f64(x, box, mesh, COSMO[1], a, split, sample, quadrupole=True)
+    exact = orc.accelerations_f64(x, box, mesh, COSMO[1], a, exact_split, sample)
+    pm = orc.accelerations_f64(x, box, mesh, COSMO[1], a, None, sample)
+
+    def rel(u, v):
+        return float(np.sqrt(((u - v) ** 2).sum() / (v ** 2).sum()))
+
+    gq = quad[sample].astype(np.float64)
+    gm = mono[sample].astype(np.float64)
+    assert rel(gq, ref_q) < 1e-5
+    err_q = rel(gq - pm, exact - pm)
+    err_m = rel(gm - pm, exact - pm)
+    print(f"short-range force error vs exact: monopole {err_m:.3e}, quadrupole {err_q:.3e}")
+    assert err_q < err_m / 3.0
