@@ -386,7 +386,7 @@ __device__ __forceinline__ void quad_term(float d0, float d1, float d2, const fl
   A2.y += a * d2 + b * (tr * d2 + 2.0f * td2);
 }
 
-template <bool QUAD>
+template <bool QUAD, bool LIST>
 __global__ void __launch_bounds__(WALK_THREADS) k_tree_walk(const uint4* __restrict__ link,
                                                             const float4* __restrict__ geo,
                                                             const float4* __restrict__ mass,
@@ -403,8 +403,8 @@ __global__ void __launch_bounds__(WALK_THREADS) k_tree_walk(const uint4* __restr
   // Lane t of the grid walks for sorted particle t, or, with a list, for particle list[t] (t below
   // *list_n): the list keeps the sorted order, so a warp's particles stay spatially coherent.
   const size_t t = ((size_t)blockIdx.x * WALK_WARPS + warp) * 32 + lane;
-  const bool valid = list ? t < (size_t)*list_n : t < n;
-  const size_t i = list ? (valid ? (size_t)list[t] : 0) : t;
+  const bool valid = LIST ? t < (size_t)*list_n : t < n;
+  const size_t i = LIST ? (valid ? (size_t)list[t] : 0) : t;
   const unsigned group = __ballot_sync(FULL, valid);
   if (group == 0) return;
   WalkShared& sh = shared[warp];
@@ -744,7 +744,8 @@ void launch_tree_walk(const TreeNodes& t, const float* sorted_x3, size_t n, floa
   const size_t groups = (n + 31) / 32;
   const unsigned blocks = (unsigned)((groups + WALK_WARPS - 1) / WALK_WARPS);
   count_launch();
-  auto kernel = t.has_quad ? k_tree_walk<true> : k_tree_walk<false>;
+  auto kernel = t.has_quad ? (list ? k_tree_walk<true, true> : k_tree_walk<true, false>)
+                            : (list ? k_tree_walk<false, true> : k_tree_walk<false, false>);
   kernel<<<blocks, WALK_THREADS, 0, s>>>(static_cast<const uint4*>(t.link.p), static_cast<const float4*>(t.geo.p),
                                          static_cast<const float4*>(t.mass.p), as<float4>(tm.x4), n, w,
                                          static_cast<const float*>(fc.far_dev.p), acc3, accumulate,
