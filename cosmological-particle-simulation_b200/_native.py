@@ -26,6 +26,7 @@ SIM_DECONVOLVE = 0x2
 SIM_TIMING = 0x4
 SIM_NO_GRAPH = 0x8
 SIM_QUADRUPOLE = 0x10
+SIM_NO_AUTOTUNE = 0x20
 
 
 class CpmError(RuntimeError):
@@ -123,6 +124,8 @@ def lib() -> C.CDLL:
         "cpm_sim_learned_walked": (i, [vp, C.POINTER(u64)]),
         "cpm_sim_short_range": (i, [vp, vp]),
         "cpm_sim_save": (i, [vp, C.c_char_p]),
+        "cpm_sim_autotune_report": (i, [vp, C.POINTER(i), C.POINTER(i), C.POINTER(i), vp]),
+        "cpm_sim_set_tuning": (i, [vp, i, i, i]),
         "cpm_step_factors": (i, [C.POINTER(Cosmology), C.c_double, C.c_double, i, C.POINTER(C.c_double),
                                  C.POINTER(C.c_double), C.POINTER(C.c_double)]),
         "cpm_sim_load": (i, [C.c_char_p, u32, C.POINTER(vp)]),

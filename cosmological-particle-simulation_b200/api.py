@@ -428,6 +428,19 @@ class Simulation:
         check(nat.lib().cpm_sim_short_range(self.h, ptr(out)), sim=True)
         return out
 
+    def tuning(self) -> dict:
+        """The autotuner's choices and the measured ms of every candidate (cpm_sim_autotune_report)."""
+        r, t, wp = C.c_int(), C.c_int(), C.c_int()
+        ms = np.zeros(8, np.float32)
+        check(nat.lib().cpm_sim_autotune_report(self.h, C.byref(r), C.byref(t), C.byref(wp), ptr(ms)), sim=True)
+        names = ["fft_radix8", "fft_radix4", "deposit_tile512", "deposit_tile1024", "deposit_tile2048",
+                 "walk_warps2", "walk_warps4", "walk_warps8"]
+        return {"fft_radix": r.value, "deposit_tile": t.value, "walk_warps": wp.value,
+                "ms": {k: round(float(v), 4) for k, v in zip(names, ms)}}
+
+    def set_tuning(self, fft_radix: int, deposit_tile: int, walk_warps: int) -> None:
+        check(nat.lib().cpm_sim_set_tuning(self.h, int(fft_radix), int(deposit_tile), int(walk_warps)), sim=True)
+
     def walked(self) -> int:
         """Particles the last step walked the tree for."""
         v = C.c_uint64()

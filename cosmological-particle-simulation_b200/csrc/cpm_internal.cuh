@@ -149,9 +149,10 @@ cudaError_t exclusive_scan_u32(const uint32_t* in, uint32_t* out, size_t n, DevB
 // ---------------------------------------------------------------------------------------------
 // Fixed-point scale exponent for masses summing to at most `total_mass`.
 int fixed_point_shift(double total_mass);
-// CIC deposit of `mass` per particle into the u64 fixed-point mesh (zeroed inside).
+// CIC deposit of `mass` per particle into the u64 fixed-point mesh (zeroed inside); tiles of
+// 256 * ppt sorted particles per CTA (ppt 2, 4 or 8).
 void launch_deposit_fixed(const float* x3, size_t n, float mass, int mesh_n, float h, int shift,
-                          unsigned long long* mesh_fx, cudaStream_t s);
+                          unsigned long long* mesh_fx, cudaStream_t s, int ppt = 4);
 // cells = (float)fx * 2^-shift, or delta = cells / mean - 1 when to_delta.
 void launch_fixed_to_f32(const unsigned long long* fx, size_t m, int shift, int to_delta, float mean, float* out,
                          cudaStream_t s);
@@ -165,6 +166,7 @@ bool poisson_supported(int n);
 const char* fft_sizes_text();  // the list of supported sizes, for error messages
 struct FftPlan {
   int n = 0;
+  int max_radix = 8;  // radix plan of the Poisson passes: 8 (8.8.8 for 512) or 4 (4.4.4.4.2); autotuned
   DevBuf twiddle;  // exp(-2 pi i m / n), m < n, float2 built from double
   DevBuf deconv;   // per-axis 1 / sinc^4(pi m / n): CIC window of deposit and gather, squared
 };
@@ -231,6 +233,7 @@ struct TreeNodes {
   DevBuf x4;        // float4 copy of the sorted positions for the walk
   DevBuf quad;      // per node 2 float4: second moments about the centre of mass (quadrupole mode)
   bool has_quad = false;  // the last build computed `quad`; the walk then adds quadrupole terms
+  int walk_warps = 4;     // warps (groups of 32 particles) per walk block: 2, 4 or 8 (autotuned)
   size_t capacity = 0;
   void* walk_fit = nullptr;  // fitted pair-force coefficients of the last split (walk.cu)
 };

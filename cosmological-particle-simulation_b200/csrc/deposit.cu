@@ -15,9 +15,9 @@
 namespace cpm {
 
 constexpr int DEP_THREADS = 256;
-constexpr int DEP_PPT = 4;                          // particles per thread
-constexpr int DEP_CHUNK = DEP_THREADS * DEP_PPT;    // 1024 particles per CTA
 constexpr int DEP_SMEM_CELLS = 12288;               // 96 KB of u64 per CTA
+// Particles per thread PPT (tile of 256 * PPT consecutive sorted particles per CTA): 2, 4 or 8,
+// picked per workload by the autotuner (4 by default).
 
 int fixed_point_shift(double total_mass) {
   // Largest k with total_mass * 2^k < 2^62, clamped so a unit weight keeps >= 24 fractional bits.
@@ -33,6 +33,7 @@ __device__ __forceinline__ unsigned long long to_fixed(float mass, float w, floa
   return __float2ull_rn(__fmul_rn(__fmul_rn(mass, w), scale));
 }
 
+template <int DEP_PPT>
 __global__ void __launch_bounds__(DEP_THREADS) k_deposit_fixed(const float* __restrict__ x3, size_t n, float mass,
                                                                int mesh_n, float h, float scale,
                                                                unsigned long long* __restrict__ mesh) {
@@ -42,6 +43,7 @@ __global__ void __launch_bounds__(DEP_THREADS) k_deposit_fixed(const float* __re
   else if (threadIdx.x < 6) bb[threadIdx.x] = -0x7fffffff;
   __syncthreads();
 
+  constexpr int DEP_CHUNK = DEP_THREADS * DEP_PPT;
   const size_t base = (size_t)blockIdx.x * DEP_CHUNK;
   CicBase cb[DEP_PPT];
   bool valid[DEP_PPT];
@@ -115,19 +117,31 @@ __global__ void __launch_bounds__(DEP_THREADS) k_deposit_fixed(const float* __re
   }
 }
 
+template <int PPT>
+static void deposit_ppt(const float* x3, size_t n, float mass, int mesh_n, float h, float scale,
+                        unsigned long long* mesh_fx, cudaStream_t s) {
+  // Per device (a cheap host call, so made on every launch): a failure shows up as the launch's error.
+  cudaFuncSetAttribute(k_deposit_fixed<PPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       DEP_SMEM_CELLS * (int)sizeof(unsigned long long));
+  constexpr size_t chunk = (size_t)DEP_THREADS * PPT;
+  const unsigned blocks = (unsigned)((n + chunk - 1) / chunk);
+  count_launch();
+  k_deposit_fixed<PPT><<<blocks, DEP_THREADS, DEP_SMEM_CELLS * sizeof(unsigned long long), s>>>(x3, n, mass, mesh_n, h,
+                                                                                              scale, mesh_fx);
+}
+
 void launch_deposit_fixed(const float* x3, size_t n, float mass, int mesh_n, float h, int shift,
-                          unsigned long long* mesh_fx, cudaStream_t s) {
+                          unsigned long long* mesh_fx, cudaStream_t s, int ppt) {
   const size_t m = (size_t)mesh_n * mesh_n * mesh_n;
   cudaMemsetAsync(mesh_fx, 0, m * sizeof(unsigned long long), s);
   if (n == 0) return;
-  // Per device (a cheap host call, so made on every launch): a failure shows up as the launch's error.
-  cudaFuncSetAttribute(k_deposit_fixed, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       DEP_SMEM_CELLS * (int)sizeof(unsigned long long));
   const float scale = std::ldexp(1.0f, shift);
-  const unsigned blocks = (unsigned)((n + DEP_CHUNK - 1) / DEP_CHUNK);
-  count_launch();
-  k_deposit_fixed<<<blocks, DEP_THREADS, DEP_SMEM_CELLS * sizeof(unsigned long long), s>>>(x3, n, mass, mesh_n, h,
-                                                                                         scale, mesh_fx);
+  if (ppt == 2)
+    deposit_ppt<2>(x3, n, mass, mesh_n, h, scale, mesh_fx, s);
+  else if (ppt == 8)
+    deposit_ppt<8>(x3, n, mass, mesh_n, h, scale, mesh_fx, s);
+  else
+    deposit_ppt<4>(x3, n, mass, mesh_n, h, scale, mesh_fx, s);
 }
 
 // integrator.rs:117-126: cell mass c = fixed * 2^-k rounded once to f32; delta = c / mean - 1.

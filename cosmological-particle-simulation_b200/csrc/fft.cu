@@ -188,11 +188,15 @@ __device__ __forceinline__ void stockham_stage(float2* sm, const float2* __restr
   __syncthreads();
 }
 
-// Radix of the next Stockham stage for a remaining length L = 2^a 3^b 5^c: 8 while it divides,
-// then 4 or 2, then 3s, then 5s (powers of two: 8..8 then one 4 or 2).
-template <int L>
+// Radix of the next Stockham stage for a remaining length L = 2^a 3^b 5^c under a plan whose
+// largest radix is MR: MR = 8 takes 8 while it divides, then 4 or 2, then 3s, then 5s (512 = 8.8.8);
+// MR = 4 takes 4 while it divides, then 2, 3s, 5s (512 = 4.4.4.4.2). The autotuner picks the plan.
+template <int L, int MR>
 constexpr int next_radix() {
-  return L % 8 == 0 ? 8 : (L % 4 == 0 ? 4 : (L % 2 == 0 ? 2 : (L % 3 == 0 ? 3 : 5)));
+  if constexpr (MR >= 8)
+    return L % 8 == 0 ? 8 : (L % 4 == 0 ? 4 : (L % 2 == 0 ? 2 : (L % 3 == 0 ? 3 : 5)));
+  else
+    return L % 4 == 0 ? 4 : (L % 2 == 0 ? 2 : (L % 3 == 0 ? 3 : 5));
 }
 constexpr bool smooth235(int n) {
   if (n <= 0) return false;
@@ -202,20 +206,20 @@ constexpr bool smooth235(int n) {
   return n == 1;
 }
 
-template <int N, int NS, bool INV, int T, int TS>
+template <int N, int NS, bool INV, int T, int TS, int MR>
 __device__ __forceinline__ void fft_stages(float2* sm, const float2* __restrict__ tw) {
   if constexpr (NS < N) {
-    constexpr int R = next_radix<N / NS>();
+    constexpr int R = next_radix<N / NS, MR>();
     stockham_stage<N, R, NS, INV, T, TS>(sm, tw);
-    fft_stages<N, NS * R, INV, T, TS>(sm, tw);
+    fft_stages<N, NS * R, INV, T, TS, MR>(sm, tw);
   }
 }
 
-// Full length-N transform of the tile (N = 2^a 3^b 5^c).
-template <int N, bool INV, int T, int TS = 1>
+// Full length-N transform of the tile (N = 2^a 3^b 5^c) with the radix plan MR.
+template <int N, bool INV, int T, int TS = 1, int MR = 8>
 __device__ __forceinline__ void fft_lines(float2* sm, const float2* __restrict__ tw) {
   static_assert(N >= 2 && N <= 1024 && smooth235(N), "lengths 2..1024 with prime factors 2, 3, 5");
-  fft_stages<N, 1, INV, T, TS>(sm, tw);
+  fft_stages<N, 1, INV, T, TS, MR>(sm, tw);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -316,7 +320,7 @@ __device__ __forceinline__ void pipeline(float2* smem, int tile_elems, int total
 }
 
 // c2c pass over a strided axis; tile -> (comp, outer, column tile).
-template <int N, bool INV, int NBUF, int T>
+template <int N, bool INV, int NBUF, int T, int MR = 8>
 __global__ void __launch_bounds__(T) k_fft_cols(float2* data, long long comp_stride, ColGeo g, int ncomp,
                                                 const float2* __restrict__ tw) {
   extern __shared__ float2 smem[];
@@ -342,13 +346,13 @@ __global__ void __launch_bounds__(T) k_fft_cols(float2* data, long long comp_str
         int valid;
         float2* d;
         locate(tile, base, valid, d);
-        fft_lines<N, INV, T>(cur, tw);
+        fft_lines<N, INV, T, 1, MR>(cur, tw);
         store_cols<N, T>(cur, d, base, g.elem_stride, valid);
       });
 }
 
 // c2c pass over contiguous rows (the z lines of a full complex n^3 array).
-template <int N, bool INV, int NBUF, int T>
+template <int N, bool INV, int NBUF, int T, int MR = 8>
 __global__ void __launch_bounds__(T) k_fft_rows(float2* data, int rows, const float2* __restrict__ tw) {
   extern __shared__ float2 smem[];
   pipeline<NBUF>(
@@ -362,7 +366,7 @@ __global__ void __launch_bounds__(T) k_fft_rows(float2* data, int rows, const fl
       },
       [&](float2* cur, int tile) {
         const int row0 = tile * TW, valid = min(TW, rows - row0);
-        fft_lines<N, INV, T>(cur, tw);
+        fft_lines<N, INV, T, 1, MR>(cur, tw);
 #pragma unroll 4
         for (int q = threadIdx.x; q < row_span<N>(N); q += T) {
           const int t = row_t<N>(q), l = row_l<N>(q);
@@ -376,7 +380,7 @@ __global__ void __launch_bounds__(T) k_fft_rows(float2* data, int rows, const fl
 // the u64 fixed-point mass mesh (c = fx * 2^-k in f32, delta = c / mean - 1). The raw pairs land
 // in 16-byte slots of a staging buffer and are converted into the complex tile.
 // Shared memory: NBUF staging buffers of M*TLD 16-byte slots, then the M*TLD complex tile.
-template <int N, int NBUF, int T>
+template <int N, int NBUF, int T, int MR = 8>
 __global__ void __launch_bounds__(T) k_r2c_z(const float* __restrict__ delta,
                                              const unsigned long long* __restrict__ fx, float inv_scale, float mean,
                                              float2* __restrict__ spec, int rows, const float2* __restrict__ tw) {
@@ -415,7 +419,7 @@ __global__ void __launch_bounds__(T) k_r2c_z(const float* __restrict__ delta,
           cplx[m * TLD + l] = v;
         }
         __syncthreads();
-        fft_lines<M, false, T, 2>(cplx, tw);
+        fft_lines<M, false, T, 2, MR>(cplx, tw);
         // X[k] = (Z[k] + conj(Z[M-k]))/2 + w^k (Z[k] - conj(Z[M-k]))/(2i), w = exp(-2 pi i / N)
         for (int q = threadIdx.x; q < row_span<M>(NH); q += T) {
           const int k = row_t<M>(q), l = row_l<M>(q);
@@ -433,7 +437,7 @@ __global__ void __launch_bounds__(T) k_r2c_z(const float* __restrict__ delta,
 // z pass, inverse: N/2+1 complex per row -> N real values times scale, as an N/2-point complex
 // inverse transform of Z'[k] = (X[k] + conj(X[M-k])) + i (X[k] - conj(X[M-k])) conj(w^k), whose
 // output is x[2m] + i x[2m+1]. tile -> (comp, row tile). Shared memory: NBUF tiles of (M+1)*TLD.
-template <int N, int NBUF, int T>
+template <int N, int NBUF, int T, int MR = 8>
 __global__ void __launch_bounds__(T) k_c2r_z(const float2* __restrict__ spec, long long comp_stride,
                                              float* __restrict__ out0, float* __restrict__ out1,
                                              float* __restrict__ out2, float scale, int rows,
@@ -472,7 +476,7 @@ __global__ void __launch_bounds__(T) k_c2r_z(const float2* __restrict__ spec, lo
           }
         }
         __syncthreads();
-        fft_lines<M, true, T, 2>(cur, tw);
+        fft_lines<M, true, T, 2, MR>(cur, tw);
 #pragma unroll 4
         for (int q = threadIdx.x; q < row_span<M>(M); q += T) {
           const int m = row_t<M>(q), l = row_l<M>(q);
@@ -493,7 +497,7 @@ __global__ void __launch_bounds__(T) k_c2r_z(const float2* __restrict__ spec, lo
 // The gradient factor is the reference's (phi * (0 - i k_a), poisson.rs:70); for y and z it
 // multiplies the transformed phi instead, which differs only in round-off.
 // Shared memory: NBUF input tiles, then one work tile for -i k_x phi.
-template <int N, int NBUF, int T>
+template <int N, int NBUF, int T, int MR = 8>
 __global__ void __launch_bounds__(T) k_poisson_x(const float2* __restrict__ spec_in, float2* spec_out,
                                                  long long comp_stride, ColGeo g, PoissonParams pp,
                                                  const float* __restrict__ deconv, const float2* __restrict__ tw) {
@@ -512,7 +516,7 @@ __global__ void __launch_bounds__(T) k_poisson_x(const float2* __restrict__ spec
         const long long base = (long long)iy * g.outer_stride + (long long)ct * TW;
         const int z0 = ct * TW;
         const float prefactor = pp.prefactor_dev ? *pp.prefactor_dev : pp.prefactor;
-        fft_lines<N, false, T>(phi, tw);
+        fft_lines<N, false, T, 1, MR>(phi, tw);
         const float ky = wavenumber(iy, N, pp.two_pi_over_l);
         for (int q = threadIdx.x; q < N * TW; q += T) {
           const int l = q % TW, t = q / TW;
@@ -539,8 +543,8 @@ __global__ void __launch_bounds__(T) k_poisson_x(const float2* __restrict__ spec
                                          __fadd_rn(__fmul_rn(v.x, nk), __fmul_rn(v.y, 0.0f)));
         }
         __syncthreads();
-        fft_lines<N, true, T>(gxb, tw);
-        fft_lines<N, true, T>(phi, tw);
+        fft_lines<N, true, T, 1, MR>(gxb, tw);
+        fft_lines<N, true, T, 1, MR>(phi, tw);
         // -i k_x phi to slot 0; the x-transformed phi to slot 1, from which the y pass forms the
         // y and z components (k_y and k_z are constant along an x line)
         store_cols<N, T>(gxb, spec_out, base, g.elem_stride, valid);
@@ -551,7 +555,7 @@ __global__ void __launch_bounds__(T) k_poisson_x(const float2* __restrict__ spec
 // Inverse y pass of the y and z gradient components: reads the x-transformed potential of slot 1
 // once, forms -i k_y phi and -i k_z phi (the f32 operations of k_green_grad) and writes their
 // inverse y transforms to slots 1 and 2; tile -> (x, column tile), lines along y.
-template <int N, int NBUF, int T>
+template <int N, int NBUF, int T, int MR = 8>
 __global__ void __launch_bounds__(T) k_grad_yz(float2* spec, long long comp_stride, ColGeo g, PoissonParams pp,
                                                const float2* __restrict__ tw) {
   extern __shared__ float2 smem[];
@@ -580,8 +584,8 @@ __global__ void __launch_bounds__(T) k_grad_yz(float2* spec, long long comp_stri
                                          __fadd_rn(__fmul_rn(p.x, nkz), __fmul_rn(p.y, 0.0f)));
         }
         __syncthreads();
-        fft_lines<N, true, T>(cur, tw);
-        fft_lines<N, true, T>(gzb, tw);
+        fft_lines<N, true, T, 1, MR>(cur, tw);
+        fft_lines<N, true, T, 1, MR>(gzb, tw);
         store_cols<N, T>(cur, phi_slot, base, g.elem_stride, valid);
         store_cols<N, T>(gzb, spec + 2 * comp_stride, base, g.elem_stride, valid);
       });
@@ -703,7 +707,7 @@ static void launch_persistent(K kernel, int threads, size_t smem, int total, cud
 
 constexpr size_t c_tile(int rows_of_tile) { return (size_t)rows_of_tile * TLD * sizeof(float2); }
 
-template <int N>
+template <int N, int MR = 8>
 static void cols_pass(float2* data, long long comp_stride, int ncomp, ColGeo g, int inverse, const float2* tw,
                       cudaStream_t s) {
   constexpr int T = threads_for<N>();
@@ -712,9 +716,9 @@ static void cols_pass(float2* data, long long comp_stride, int ncomp, ColGeo g, 
   g.col_tiles = (g.cols + TW - 1) / TW;
   const int total = ncomp * g.outer * g.col_tiles;
   if (inverse)
-    launch_persistent(k_fft_cols<N, true, NB, T>, T, smem, total, s, data, comp_stride, g, ncomp, tw);
+    launch_persistent(k_fft_cols<N, true, NB, T, MR>, T, smem, total, s, data, comp_stride, g, ncomp, tw);
   else
-    launch_persistent(k_fft_cols<N, false, NB, T>, T, smem, total, s, data, comp_stride, g, ncomp, tw);
+    launch_persistent(k_fft_cols<N, false, NB, T, MR>, T, smem, total, s, data, comp_stride, g, ncomp, tw);
 }
 
 template <int N>
@@ -766,7 +770,7 @@ static void r2c3_n(const FftPlan& p, const float* delta, const unsigned long lon
   cols_pass<N>(spec, 0, 1, ColGeo{NHP, n * NHP, NH, 0, N}, 0, tw, s);  // x lines, outer = y
 }
 
-template <int N>
+template <int N, int MR>
 static void poisson_n(const FftPlan& p, const PoissonParams& pp, const float* delta, const unsigned long long* fx,
                       int fx_shift, float mean, float2* spec, float* gx, float* gy, float* gz, cudaStream_t s) {
   const float2* tw = static_cast<const float2*>(p.twiddle.p);
@@ -784,7 +788,7 @@ static void poisson_n(const FftPlan& p, const PoissonParams& pp, const float* de
     const int grid = (int)std::min<long long>((total + 255) / 256, 16LL * num_sms());
     count_launch();
     k_green_grad<<<grid, 256, 0, s>>>(spec, comp, N, pp, deconv);
-    cols_pass<N>(spec, comp, 3, ColGeo{NHP, n * NHP, NH, 0, N}, 1, tw, s);  // x lines, outer = y
+    cols_pass<N, MR>(spec, comp, 3, ColGeo{NHP, n * NHP, NH, 0, N}, 1, tw, s);  // x lines, outer = y
   } else {
     // Slot 0 holds the forward spectrum; the x pass reads each tile of it before writing the
     // same tile of slots 0..2, and tiles are disjoint, so the update in place is safe.
@@ -793,37 +797,37 @@ static void poisson_n(const FftPlan& p, const PoissonParams& pp, const float* de
       constexpr int T = threads_for<M>();
       constexpr int NB = 2 * (4 * c_tile(M) + c_tile(M)) <= SMEM_LIMIT ? 2 : 1;  // two CTAs per SM
       const size_t smem = (2 * NB + 1) * c_tile(M);
-      launch_persistent(k_r2c_z<N, NB, T>, T, smem, row_tiles, s, delta, fx, std::ldexp(1.0f, -fx_shift), mean, s0,
+      launch_persistent(k_r2c_z<N, NB, T, MR>, T, smem, row_tiles, s, delta, fx, std::ldexp(1.0f, -fx_shift), mean, s0,
                         rows, tw);
     }
     // 2. y forward on slot 0: lines along y (stride NHP), columns along kz adjacent, outer = x
-    cols_pass<N>(s0, 0, 1, ColGeo{n * NHP, NHP, NH, 0, N}, 0, tw, s);
+    cols_pass<N, MR>(s0, 0, 1, ColGeo{n * NHP, NHP, NH, 0, N}, 0, tw, s);
     {  // 3. x forward + Green + gradient + x inverse -> slots 0 (-i k_x phi) and 1 (phi); outer = y
       constexpr int T = threads_for<N>();
       constexpr int NBX = 3 * c_tile(N) <= SMEM_LIMIT ? 2 : 1;
       const size_t smem = (NBX + 1) * c_tile(N);
       ColGeo g{NHP, n * NHP, NH, (NH + TW - 1) / TW, N};
-      launch_persistent(k_poisson_x<N, NBX, T>, T, smem, g.outer * g.col_tiles, s, s0, spec, comp, g, pp, deconv, tw);
+      launch_persistent(k_poisson_x<N, NBX, T, MR>, T, smem, g.outer * g.col_tiles, s, s0, spec, comp, g, pp, deconv, tw);
     }
     // 4. y inverse: slot 0 (x component), then slots 1, 2 (y, z components) from the potential
-    cols_pass<N>(spec, comp, 1, ColGeo{n * NHP, NHP, NH, 0, N}, 1, tw, s);
+    cols_pass<N, MR>(spec, comp, 1, ColGeo{n * NHP, NHP, NH, 0, N}, 1, tw, s);
     {
       constexpr int T = threads_for<N>();
       constexpr int NBY = 3 * c_tile(N) <= SMEM_LIMIT ? 2 : 1;
       const size_t smem = (NBY + 1) * c_tile(N);
       ColGeo g{n * NHP, NHP, NH, (NH + TW - 1) / TW, N};
-      launch_persistent(k_grad_yz<N, NBY, T>, T, smem, g.outer * g.col_tiles, s, spec, comp, g, pp, tw);
+      launch_persistent(k_grad_yz<N, NBY, T, MR>, T, smem, g.outer * g.col_tiles, s, spec, comp, g, pp, tw);
     }
   }
   if constexpr (2 * c_tile(N) > SMEM_LIMIT) {
     // 4. y inverse on the three component spectra
-    cols_pass<N>(spec, comp, 3, ColGeo{n * NHP, NHP, NH, 0, N}, 1, tw, s);
+    cols_pass<N, MR>(spec, comp, 3, ColGeo{n * NHP, NHP, NH, 0, N}, 1, tw, s);
   }
   {  // 5. z: C2R with 1/n^3
     constexpr int T = threads_for<M>();
     constexpr int NB = 2 * c_tile(M + 1) <= SMEM_LIMIT ? 2 : 1;
     const size_t smem = NB * c_tile(M + 1);
-    launch_persistent(k_c2r_z<N, NB, T>, T, smem, 3 * row_tiles, s, spec, comp, gx, gy, gz, pp.scale, rows, tw);
+    launch_persistent(k_c2r_z<N, NB, T, MR>, T, smem, 3 * row_tiles, s, spec, comp, gx, gy, gz, pp.scale, rows, tw);
   }
 }
 
@@ -841,8 +845,13 @@ void launch_r2c3(const FftPlan& p, const float* delta, const unsigned long long*
 void launch_poisson(const FftPlan& p, const PoissonParams& pp, const float* delta, const unsigned long long* fx,
                     int fx_shift, float mean, float2* spec, float* gx, float* gy, float* gz, cudaStream_t s) {
   switch (p.n) {
-#define CPM_CASE(N) \
-  case N: poisson_n<N>(p, pp, delta, fx, fx_shift, mean, spec, gx, gy, gz, s); break;
+#define CPM_CASE(N)                                                          \
+  case N:                                                                    \
+    if (p.max_radix == 4)                                                    \
+      poisson_n<N, 4>(p, pp, delta, fx, fx_shift, mean, spec, gx, gy, gz, s); \
+    else                                                                     \
+      poisson_n<N, 8>(p, pp, delta, fx, fx_shift, mean, spec, gx, gy, gz, s); \
+    break;
     CPM_FFT_SIZES(CPM_CASE)
 #undef CPM_CASE
     default: break;

@@ -27,7 +27,10 @@
 // resolution is L / 2^32 everywhere in the box; x (f32, what every force kernel reads) is
 // rewritten from q after each drift. Positions given by the caller are rounded to the grid.
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -82,6 +85,10 @@ struct cpm_sim {
   float net_threshold = 50.0f;
   float net_in_scale = 1.0f;
   DevBuf flag, offset, list, list_n, scan_tmp;
+  // Autotuned launch choices (FFT radix plan in `plan`, walk warps in `tree`) and the timings.
+  int dep_ppt = 4;
+  float tune_ms[8] = {};
+  bool tuned = false;
 };
 
 #define SIM_CU(s, call)                                                                                      \
@@ -188,7 +195,8 @@ static int sim_accelerations(cpm_sim* s, float a, const StepScalars* dev = nullp
     s->x_out = nullptr;
   }
   mark(s, 2);
-  launch_deposit_fixed(as<float>(s->x), n, 1.0f, mn, s->h, s->shift, as<unsigned long long>(s->fx), s->stream);
+  launch_deposit_fixed(as<float>(s->x), n, 1.0f, mn, s->h, s->shift, as<unsigned long long>(s->fx), s->stream,
+                       s->dep_ppt);
   mark(s, 3);
   const float r_split = s->P.use_tree ? s->P.split.r_split : 0.0f;
   PoissonParams pp =
@@ -227,6 +235,154 @@ static int sim_accelerations(cpm_sim* s, float a, const StepScalars* dev = nullp
     mark(s, 6);
   }
   return CPM_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Autotuner. The compiled alternatives of three launch parameters are timed on the simulation's
+// own first state (after its first force evaluation, so the mesh, the sorted particles and the tree
+// are real), and the fastest is kept:
+//   FFT radix plan of the Poisson passes  largest radix 8 (512 = 8.8.8) or 4 (4.4.4.4.2)
+//   deposit tile                          256 x {2, 4, 8} sorted particles per CTA
+//   walk group                            {2, 4, 8} warps of 32 particles per block
+// Each candidate runs once untimed and twice timed with CUDA events on the simulation's stream;
+// the work repeats what the force evaluation did (deposit, Poisson solve) or writes to scratch
+// (walk), so the state is unchanged. Choices are cached per workload (particles, mesh, tree,
+// quadrupoles) for the process, and in the file named by CPM_TUNE_CACHE when it is set (one line
+// per workload: key, radix, tile, warps). CPM_SIM_NO_AUTOTUNE keeps 8, 4 and 4.
+namespace {
+struct TuneChoice {
+  int radix = 8, ppt = 4, warps = 4;
+  float ms[8] = {};
+};
+std::mutex g_tune_mu;
+std::map<std::string, TuneChoice> g_tune_cache;
+bool g_tune_file_read = false;
+
+std::string tune_key(const cpm_sim* s) {
+  char buf[160];
+  std::snprintf(buf, sizeof(buf), "n=%zu mesh=%d tree=%d quad=%d", s->n, s->P.mesh_n, s->P.use_tree,
+                (s->P.flags & CPM_SIM_QUADRUPOLE) ? 1 : 0);
+  return buf;
+}
+
+void tune_file_load() {
+  g_tune_file_read = true;
+  const char* path = std::getenv("CPM_TUNE_CACHE");
+  if (!path) return;
+  FILE* f = std::fopen(path, "r");
+  if (!f) return;
+  char line[256];
+  while (std::fgets(line, sizeof(line), f)) {
+    const char* bar = std::strchr(line, '|');
+    if (!bar) continue;
+    TuneChoice c;
+    if (std::sscanf(bar + 1, "%d %d %d", &c.radix, &c.ppt, &c.warps) == 3)
+      g_tune_cache[std::string(line, (size_t)(bar - line))] = c;
+  }
+  std::fclose(f);
+}
+
+void tune_file_append(const std::string& key, const TuneChoice& c) {
+  const char* path = std::getenv("CPM_TUNE_CACHE");
+  if (!path) return;
+  FILE* f = std::fopen(path, "a");
+  if (!f) return;
+  std::fprintf(f, "%s|%d %d %d\n", key.c_str(), c.radix, c.ppt, c.warps);
+  std::fclose(f);
+}
+
+template <typename F>
+float time_ms(cudaStream_t st, cudaEvent_t e0, cudaEvent_t e1, F&& f) {
+  f();
+  cudaEventRecord(e0, st);
+  f();
+  f();
+  cudaEventRecord(e1, st);
+  cudaEventSynchronize(e1);
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  return 0.5f * ms;
+}
+}  // namespace
+
+static void apply_tuning(cpm_sim* s, const TuneChoice& c) {
+  s->plan.max_radix = c.radix;
+  s->dep_ppt = c.ppt;
+  s->tree.walk_warps = c.warps;
+  for (int i = 0; i < 8; ++i) s->tune_ms[i] = c.ms[i];
+  s->tuned = true;
+}
+
+// A workload tuned before (this process or the cache file) takes its choices before its first
+// force evaluation, so that its arithmetic (the radix plan rounds differently) is that of the plan
+// it keeps.
+static void sim_apply_cached_tuning(cpm_sim* s) {
+  if (s->P.flags & CPM_SIM_NO_AUTOTUNE) return;
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  if (!g_tune_file_read) tune_file_load();
+  auto it = g_tune_cache.find(tune_key(s));
+  if (it != g_tune_cache.end()) apply_tuning(s, it->second);
+}
+
+static int sim_autotune(cpm_sim* s) {
+  if ((s->P.flags & CPM_SIM_NO_AUTOTUNE) || s->tuned) return CPM_OK;
+  const std::string key = tune_key(s);
+  const int radix_used = s->plan.max_radix;
+  SIM_CU(s, cudaStreamSynchronize(s->stream));
+  cudaEvent_t e0, e1;
+  SIM_CU(s, cudaEventCreate(&e0));
+  SIM_CU(s, cudaEventCreate(&e1));
+  TuneChoice c;
+  const int mn = s->P.mesh_n;
+  const float r_split = s->P.use_tree ? s->P.split.r_split : 0.0f;
+  const PoissonParams pp =
+      make_poisson_params(mn, s->box, s->P.cosmo.omega_m, s->a, r_split, (s->P.flags & CPM_SIM_DECONVOLVE) ? 1 : 0);
+  const int radices[2] = {8, 4};
+  float best = 1e30f;
+  for (int k = 0; k < 2; ++k) {
+    s->plan.max_radix = radices[k];
+    c.ms[k] = time_ms(s->stream, e0, e1, [&] {
+      launch_poisson(s->plan, pp, nullptr, as<unsigned long long>(s->fx), s->shift, s->mean, as<float2>(s->spec),
+                     as<float>(s->gx), as<float>(s->gy), as<float>(s->gz), s->stream);
+    });
+    if (c.ms[k] < best) best = c.ms[k], c.radix = radices[k];
+  }
+  const int tiles[3] = {2, 4, 8};
+  best = 1e30f;
+  for (int k = 0; k < 3; ++k) {
+    c.ms[2 + k] = time_ms(s->stream, e0, e1, [&] {
+      launch_deposit_fixed(as<float>(s->x), s->n, 1.0f, mn, s->h, s->shift, as<unsigned long long>(s->fx), s->stream,
+                           tiles[k]);
+    });
+    if (c.ms[2 + k] < best) best = c.ms[2 + k], c.ppt = tiles[k];
+  }
+  if (s->P.use_tree && s->tree.geo.p && !(s->P.flags & CPM_SIM_QUADRUPOLE)) {
+    int rc = ensure(s->host_tmp, 3 * s->n * sizeof(float)) == cudaSuccess ? CPM_OK : CPM_E_NOMEM;
+    if (rc) return set_error(&s->err, rc, "autotune: scratch allocation failed");
+    const float kk = tree_coupling(s->P.cosmo.omega_m, s->box, s->a, s->n);
+    const int warps[3] = {2, 4, 8};
+    best = 1e30f;
+    for (int k = 0; k < 3; ++k) {
+      s->tree.walk_warps = warps[k];
+      c.ms[5 + k] = time_ms(s->stream, e0, e1, [&] {
+        launch_tree_walk(s->tree, as<float>(s->x), s->n, s->box, s->P.split, kk, as<float>(s->host_tmp), 0, nullptr,
+                         as<DevStatus>(s->status), s->stream);
+      });
+      if (c.ms[5 + k] < best) best = c.ms[5 + k], c.warps = warps[k];
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  apply_tuning(s, c);
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune_cache[key] = c;
+    tune_file_append(key, c);
+  }
+  int rc = sim_check(s);
+  // the first force evaluation ran with another radix plan: repeat it with the one kept
+  if (!rc && c.radix != radix_used && (rc = sim_accelerations(s, s->a, nullptr)) == CPM_OK) rc = sim_check(s);
+  return rc;
 }
 
 // Validates the parameters and allocates every device buffer of a simulation.
@@ -280,6 +436,7 @@ static int sim_new(const cpm_sim_params* params, float a0, cpm_sim** out) {
   }
   cudaMemsetAsync(s->status.p, 0, sizeof(DevStatus), s->stream);
   cudaMemsetAsync(s->counters.p, 0, sizeof(TreeCounters), s->stream);
+  sim_apply_cached_tuning(s);
   *out = s;
   return CPM_OK;
 }
@@ -293,7 +450,7 @@ int cpm_sim_create(const cpm_sim_params* params, const float* x3, const float* p
   cpm_sim* s = nullptr;
   int rc = sim_new(params, a0, &s);
   if (rc) return rc;
-  if ((rc = cpm_sim_set_state(s, x3, p3)) != CPM_OK) {
+  if ((rc = cpm_sim_set_state(s, x3, p3)) != CPM_OK || (rc = sim_autotune(s)) != CPM_OK) {
     g_last_error = s->err;
     cpm_sim_destroy(s);
     return rc;
@@ -332,6 +489,7 @@ int cpm_sim_create_zeldovich(const cpm_sim_params* params, int n_side, float n_s
   if (fixed_point(s)) launch_to_fixed(as<float>(s->x), as<uint32_t>(s->q), s->n, s->box, s->stream);
   rc = sim_accelerations(s, s->a);
   if (rc == CPM_OK) rc = sim_check(s);
+  if (rc == CPM_OK) rc = sim_autotune(s);
   if (rc) {
     g_last_error = s->err;
     cpm_sim_destroy(s);
@@ -776,6 +934,36 @@ int cpm_sim_short_range(cpm_sim* s, float* sr3) {
   launch_scatter3(as<float>(s->host_tmp), as<uint32_t>(s->id), n, as<float>(s->x2), s->stream);
   SIM_CU(s, cudaMemcpyAsync(sr3, s->x2.p, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
   return sim_check(s);
+}
+
+int cpm_sim_autotune_report(cpm_sim* s, int* fft_radix, int* deposit_tile, int* walk_warps, float* ms8) {
+  if (!s) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_autotune_report: sim is NULL");
+  if (fft_radix) *fft_radix = s->plan.max_radix;
+  if (deposit_tile) *deposit_tile = 256 * s->dep_ppt;
+  if (walk_warps) *walk_warps = s->tree.walk_warps;
+  if (ms8)
+    for (int i = 0; i < 8; ++i) ms8[i] = s->tune_ms[i];
+  return CPM_OK;
+}
+
+int cpm_sim_set_tuning(cpm_sim* s, int fft_radix, int deposit_tile, int walk_warps) {
+  if (!s) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_set_tuning: sim is NULL");
+  if ((fft_radix != 4 && fft_radix != 8) || (deposit_tile != 512 && deposit_tile != 1024 && deposit_tile != 2048) ||
+      (walk_warps != 2 && walk_warps != 4 && walk_warps != 8))
+    return set_error(&s->err, CPM_E_INVALID,
+                     "cpm_sim_set_tuning: radix 4 or 8, tile 512, 1024 or 2048, warps 2, 4 or 8");
+  SIM_CU(s, cudaStreamSynchronize(s->stream));
+  s->plan.max_radix = fft_radix;
+  s->dep_ppt = deposit_tile / 256;
+  s->tree.walk_warps = walk_warps;
+  s->tuned = true;
+  for (int q = 0; q < 2; ++q) {  // the captured graphs hold the old launches
+    if (s->graph[q]) cudaGraphExecDestroy(s->graph[q]);
+    s->graph[q] = nullptr;
+    s->warm[q] = false;
+    s->no_graph[q] = false;
+  }
+  return CPM_OK;
 }
 
 int cpm_sim_learned_walked(cpm_sim* s, uint64_t* walked) {

@@ -386,8 +386,8 @@ __device__ __forceinline__ void quad_term(float d0, float d1, float d2, const fl
   A2.y += a * d2 + b * (tr * d2 + 2.0f * td2);
 }
 
-template <bool QUAD, bool LIST>
-__global__ void __launch_bounds__(WALK_THREADS) k_tree_walk(const uint4* __restrict__ link,
+template <bool QUAD, bool LIST, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) k_tree_walk(const uint4* __restrict__ link,
                                                             const float4* __restrict__ geo,
                                                             const float4* __restrict__ mass,
                                                             const float4* __restrict__ x4, size_t n, WalkParams w,
@@ -397,12 +397,12 @@ __global__ void __launch_bounds__(WALK_THREADS) k_tree_walk(const uint4* __restr
                                                             const uint32_t* __restrict__ list,
                                                             const uint32_t* __restrict__ list_n,
                                                             const float4* __restrict__ quad) {
-  __shared__ WalkShared shared[WALK_WARPS];
+  __shared__ WalkShared shared[WARPS];
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   // Lane t of the grid walks for sorted particle t, or, with a list, for particle list[t] (t below
   // *list_n): the list keeps the sorted order, so a warp's particles stay spatially coherent.
-  const size_t t = ((size_t)blockIdx.x * WALK_WARPS + warp) * 32 + lane;
+  const size_t t = ((size_t)blockIdx.x * WARPS + warp) * 32 + lane;
   const bool valid = LIST ? t < (size_t)*list_n : t < n;
   const size_t i = LIST ? (valid ? (size_t)list[t] : 0) : t;
   const unsigned group = __ballot_sync(FULL, valid);
@@ -742,11 +742,15 @@ void launch_tree_walk(const TreeNodes& t, const float* sorted_x3, size_t n, floa
   w.p2.eps2 = dup(w.eps2);
   w.p2.neg_m = dup(-1.0f);
   const size_t groups = (n + 31) / 32;
-  const unsigned blocks = (unsigned)((groups + WALK_WARPS - 1) / WALK_WARPS);
+  // warps per block: the autotuned group count for the plain and list walks; 4 with quadrupoles
+  const int warps = t.has_quad ? 4 : (t.walk_warps == 2 || t.walk_warps == 8 ? t.walk_warps : 4);
+  const unsigned blocks = (unsigned)((groups + warps - 1) / warps);
   count_launch();
-  auto kernel = t.has_quad ? (list ? k_tree_walk<true, true> : k_tree_walk<true, false>)
-                            : (list ? k_tree_walk<false, true> : k_tree_walk<false, false>);
-  kernel<<<blocks, WALK_THREADS, 0, s>>>(static_cast<const uint4*>(t.link.p), static_cast<const float4*>(t.geo.p),
+  auto kernel = t.has_quad ? (list ? k_tree_walk<true, true, 4> : k_tree_walk<true, false, 4>)
+              : warps == 2 ? (list ? k_tree_walk<false, true, 2> : k_tree_walk<false, false, 2>)
+              : warps == 8 ? (list ? k_tree_walk<false, true, 8> : k_tree_walk<false, false, 8>)
+                           : (list ? k_tree_walk<false, true, 4> : k_tree_walk<false, false, 4>);
+  kernel<<<blocks, warps * 32, 0, s>>>(static_cast<const uint4*>(t.link.p), static_cast<const float4*>(t.geo.p),
                                          static_cast<const float4*>(t.mass.p), as<float4>(tm.x4), n, w,
                                          static_cast<const float*>(fc.far_dev.p), acc3, accumulate,
                                          reinterpret_cast<unsigned long long*>(counters), st, k_dev, list, list_n,

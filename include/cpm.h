@@ -251,6 +251,8 @@ typedef struct {
  * short-range kernel to its monopole force. Precision mode (use with CPM_SIM_FIXED_POINT); it
  * changes the forces, so plain parity with the reference holds without it. */
 #define CPM_SIM_QUADRUPOLE 0x10u
+/* Skip the autotuner (see cpm_sim_autotune_report) and keep the default launch choices. */
+#define CPM_SIM_NO_AUTOTUNE 0x20u
 
 /* integrator.rs:54-79 `Simulation::new`: uploads x3, p3 (AoS [n][3]) and computes the initial
  * acceleration at a0. */
@@ -330,6 +332,17 @@ int cpm_sim_load(const char* path, uint32_t extra_flags, cpm_sim** out);
  * uses); fp64 = 1: the FP64 device computation of CPM_SIM_FIXED_POINT steps (256 Simpson
  * intervals; d is returned unrounded, k1 and k2 as the f32 values the kicks use). */
 int cpm_step_factors(const cpm_cosmology* cosmo, double a0, double a1, int fp64, double* k1, double* d, double* k2);
+/* No counterpart in the reference. The launch choices the autotuner made when the simulation was
+ * created (each candidate timed on the simulation's own first state; cached per workload, and in the
+ * file named by the environment variable CPM_TUNE_CACHE when set): the largest radix of the Poisson
+ * FFT passes (8 or 4), the deposit tile (512, 1024 or 2048 sorted particles per CTA) and the walk
+ * group (2, 4 or 8 warps of 32 particles per block). ms8 (may be NULL) receives the measured ms per
+ * call: radix 8, 4; tile 512, 1024, 2048; warps 2, 4, 8 (0 where not timed). */
+int cpm_sim_autotune_report(cpm_sim* sim, int* fft_radix, int* deposit_tile, int* walk_warps, float* ms8);
+/* Overrides the autotuner's choices (radix 4 or 8, tile 512, 1024 or 2048, warps 2, 4 or 8); the next
+ * force evaluation uses them. Deposit tile and walk group do not change any result bit; the radix
+ * plan changes FFT rounding only. */
+int cpm_sim_set_tuning(cpm_sim* sim, int fft_radix, int deposit_tile, int walk_warps);
 /* Particles the last step walked the tree for (all of them without a net). */
 int cpm_sim_learned_walked(cpm_sim* sim, uint64_t* walked);
 /* The CUDA stream the simulation launches on (cudaStream_t), for callers that time with events. */

@@ -59,6 +59,7 @@ pub const CPM_SIM_DECONVOLVE: u32 = 0x2;
 pub const CPM_SIM_TIMING: u32 = 0x4;
 pub const CPM_SIM_NO_GRAPH: u32 = 0x8;
 pub const CPM_SIM_QUADRUPOLE: u32 = 0x10;
+pub const CPM_SIM_NO_AUTOTUNE: u32 = 0x20;
 
 /// The reference panics where the C ABI returns an error (e.g. poisson.rs:35); keep that.
 pub fn check(rc: c_int, ctx: *const CpmCtx) {

@@ -363,3 +363,29 @@ def test_step_factors_fp64_and_reference(cpm, orc):
         assert abs(d / simpson(drift, a0, a1) - 1.0) < 1e-12
         assert abs(k1 / simpson(kick, a0, am64) - 1.0) < 2e-7
         assert abs(k2 / simpson(kick, am64, a1) - 1.0) < 2e-7
+
+
+def test_autotuned_variants_give_the_same_forces(cpm):
+    """The autotuner's alternatives: every deposit tile and walk group gives bit-identical forces;
+    the radix-4 plan of the Poisson FFT agrees with the radix-8 plan to FFT rounding."""
+    cc = cpm.Cosmology(0.0, 0.3, 0.7, 70.0)
+    split = cpm.ForceSplit.with_(64.0, 64, 32, 1.0 / 30.0, 0.5)
+    sim = cpm.Simulation.from_zeldovich(cc, 64.0, 64, 32, 0.96, 0.8, 0.02, 5, split)
+    for a1 in cpm.ln_a_schedule(0.02, 1.0, 64)[:48]:
+        sim.step_to(a1)
+    t = sim.tuning()
+    assert t["fft_radix"] in (4, 8) and t["deposit_tile"] in (512, 1024, 2048) and t["walk_warps"] in (2, 4, 8)
+    assert all(v > 0.0 for v in t["ms"].values())
+    st = sim.state()
+    accs = {}
+    for radix in (8, 4):
+        for tile in (512, 1024, 2048):
+            for warps in (2, 4, 8):
+                sim.set_tuning(radix, tile, warps)
+                sim.set_state(st["x"], st["p"])
+                accs[(radix, tile, warps)] = sim.state()["acc"]
+    for key, acc in accs.items():
+        same_radix = accs[(key[0], 1024, 4)]
+        assert np.array_equal(acc, same_radix), key
+    assert rel_rms(accs[(4, 1024, 4)], accs[(8, 1024, 4)]) < 1e-6
+    sim.close()
