@@ -182,8 +182,10 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
     torch.cuda.set_device(dev)
 
     if args.load_state:
-        # continue the schedule from a saved state (profiling of a given epoch, e.g. z = 0)
-        st0 = np.load(args.load_state)
+        # continue the schedule from a saved state file (cpm_sim_save; profiling of a given epoch, e.g. z = 0)
+        loaded = cpm.Simulation.load(args.load_state)
+        st0 = loaded.state()
+        loaded.close()
         a_saved = float(st0["a"])
         full = schedule(wl["steps_total"], wl["steps_total"] + args.warmup + args.steps + 1)
         i0 = int(np.searchsorted(np.asarray(full, np.float32), np.float32(a_saved), side="right"))
@@ -234,9 +236,9 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
     counters = sim.counters()
     graphs = sim.graphs()
     walked = sim.walked()
+    tuning = sim.tuning()
     if args.save_state and rank == 0:
-        st = sim.state()
-        np.savez(args.save_state, x=st["x"], p=st["p"], a=np.float32(st["a"]))
+        sim.save(args.save_state)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         st = sim.state()
         snapshots["end"] = (st["x"], st["p"], st["acc"], sched[-1])
@@ -328,6 +330,7 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
                  "candidates_last_step": counters["candidates"]},
         "tree_walk_end_state": walk,
         "walked_last_step": walked,
+        "autotune": tuning,
         "learned": ({"net": "3-layer 3^3 conv, 16 channels, BF16 tcgen05 kernels", "weights": str(NET_WEIGHTS.name),
                      "delta_threshold": net_threshold,
                      "note": "phase gather_ms includes the net inference; walk only for particles at or above "
@@ -442,8 +445,8 @@ def main() -> int:
     ap.add_argument("--no-phases", action="store_true", help="skip the second, per-phase timed run")
     ap.add_argument("--cpu-walk-fraction", type=float, default=1.0 / 64.0)
     ap.add_argument("--ref-budget-s", type=float, default=120.0)
-    ap.add_argument("--save-state", default="", help="write the state after the timed steps (npz: x, p, a)")
-    ap.add_argument("--load-state", default="", help="start from a saved state and continue its schedule")
+    ap.add_argument("--save-state", default="", help="write the state file (cpm_sim_save) after the timed steps")
+    ap.add_argument("--load-state", default="", help="start from a state file (cpm_sim_save) and continue its schedule")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         ap.error("--warmup must be >= 3")
