@@ -129,6 +129,15 @@ def lib() -> C.CDLL:
         "cpm_step_factors": (i, [C.POINTER(Cosmology), C.c_double, C.c_double, i, C.POINTER(C.c_double),
                                  C.POINTER(C.c_double), C.POINTER(C.c_double)]),
         "cpm_sim_load": (i, [C.c_char_p, u32, C.POINTER(vp)]),
+        "cpm_sim_tree_depth": (i, [vp, C.POINTER(u32), C.POINTER(u64)]),
+        "cpm_ensemble_create": (i, [C.POINTER(Cosmology), fl, fl, fl, fl, i, vp, u32, C.POINTER(vp)]),
+        "cpm_ensemble_step_to": (i, [vp, fl]),
+        "cpm_ensemble_get_state": (i, [vp, i, i, vp, vp, vp]),
+        "cpm_ensemble_power_spectrum": (i, [vp, i, i, i, vp, vp, vp]),
+        "cpm_ensemble_graphs": (i, [vp]),
+        "cpm_ensemble_stream": (vp, [vp]),
+        "cpm_ensemble_last_error": (C.c_char_p, [vp]),
+        "cpm_ensemble_destroy": (i, [vp]),
         "cpm_net_weight_count": (i, []),
         "cpm_net_create": (i, [i, C.POINTER(vp)]),
         "cpm_net_destroy": (i, [vp]),

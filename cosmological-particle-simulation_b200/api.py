@@ -441,6 +441,13 @@ class Simulation:
     def set_tuning(self, fft_radix: int, deposit_tile: int, walk_warps: int) -> None:
         check(nat.lib().cpm_sim_set_tuning(self.h, int(fft_radix), int(deposit_tile), int(walk_warps)), sim=True)
 
+    def tree_depth(self) -> dict:
+        """The last tree build's deepest split level and the nodes kept as leaves at the key depth
+        (the reference keeps splitting those to depth 40, tree.rs:13)."""
+        d, k = C.c_uint32(), C.c_uint64()
+        check(nat.lib().cpm_sim_tree_depth(self.h, C.byref(d), C.byref(k)), sim=True)
+        return {"max_depth": int(d.value), "key_depth_leaves": int(k.value)}
+
     def walked(self) -> int:
         """Particles the last step walked the tree for."""
         v = C.c_uint64()
@@ -453,6 +460,73 @@ class Simulation:
     def close(self):
         if getattr(self, "h", None):
             nat.lib().cpm_sim_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class EnsembleClass(C.Structure):
+    _fields_ = [("n_side", C.c_int), ("mesh_n", C.c_int), ("n_boxes", C.c_int), ("first_seed", C.c_uint64),
+                ("split", nat.ForceSplitC)]
+
+
+class Ensemble:
+    """Many independent realisations of uneven sizes (cpm_ensemble_*): classes of equal-size boxes,
+    every box a Simulation of integrator.rs:174-186 from Zel'dovich ICs (ics.rs:119-182) with seed
+    first_seed + b; every box of a class shares each launch, and one step of the ensemble is one CUDA
+    graph with a branch per class. `classes` is a list of (n_side, mesh_n, n_boxes, first_seed, split)."""
+
+    def __init__(self, cosmo: Cosmology, box_size: float, n_s: float, sigma8: float, a_init: float, classes,
+                 flags: int = 0):
+        arr = (EnsembleClass * len(classes))()
+        for i, (n_side, mesh_n, n_boxes, first_seed, split) in enumerate(classes):
+            arr[i] = EnsembleClass(int(n_side), int(mesh_n), int(n_boxes), int(first_seed), split.as_c())
+        h = C.c_void_p()
+        rc = nat.lib().cpm_ensemble_create(C.byref(cosmo), float(box_size), float(n_s), float(sigma8), float(a_init),
+                                           len(classes), arr, int(flags), C.byref(h))
+        check(rc, sim=True)
+        self.h = h
+        self.classes = [tuple(c) for c in classes]
+        self.a = float(a_init)
+
+    def _check(self, rc):
+        if rc != nat.CPM_OK:
+            msg = nat.lib().cpm_ensemble_last_error(self.h)
+            raise CpmError(rc, msg.decode() if msg else "")
+
+    def step_to(self, a1: float) -> None:
+        self._check(nat.lib().cpm_ensemble_step_to(self.h, float(a1)))
+        self.a = float(a1)
+
+    def state(self, cls: int, box: int) -> dict:
+        n = int(self.classes[cls][0]) ** 3
+        x = np.empty((n, 3), np.float32)
+        p = np.empty((n, 3), np.float32)
+        acc = np.empty((n, 3), np.float32)
+        self._check(nat.lib().cpm_ensemble_get_state(self.h, int(cls), int(box), ptr(x), ptr(p), ptr(acc)))
+        return dict(x=x, p=p, acc=acc, a=self.a)
+
+    def power_spectrum(self, cls: int, box: int, n_shells: int):
+        k = np.empty(n_shells, np.float64)
+        pk = np.empty(n_shells, np.float64)
+        cnt = np.empty(n_shells, np.uint64)
+        self._check(nat.lib().cpm_ensemble_power_spectrum(self.h, int(cls), int(box), int(n_shells), ptr(k), ptr(pk),
+                                                          ptr(cnt)))
+        return k, pk, cnt
+
+    def graphs(self) -> int:
+        return int(nat.lib().cpm_ensemble_graphs(self.h))
+
+    def stream(self) -> int:
+        return nat.lib().cpm_ensemble_stream(self.h) or 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            nat.lib().cpm_ensemble_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -136,8 +136,10 @@ struct SortScratch {
 };
 
 // Octant keys (tree.rs descent) of positions (AoS f32 or float4), values = 0..n-1.
+// With n_box > 0 (a batch of boxes of n_box particles each, in box order), the box index is placed
+// above the 3 * levels octant bits.
 void launch_octant_keys(const float* x3, size_t n, float box, int levels, uint64_t* keys, uint32_t* vals,
-                        DevStatus* st, cudaStream_t s);
+                        DevStatus* st, cudaStream_t s, size_t n_box = 0);
 // Stable LSD sort of the low `bits` bits of keys; result in keys/vals (ping-pong handled inside).
 cudaError_t radix_sort_pairs(uint64_t* keys, uint32_t* vals, size_t n, int bits, SortScratch& sc,
                              cudaStream_t s);
@@ -152,7 +154,7 @@ int fixed_point_shift(double total_mass);
 // CIC deposit of `mass` per particle into the u64 fixed-point mesh (zeroed inside); tiles of
 // 256 * ppt sorted particles per CTA (ppt 2, 4 or 8).
 void launch_deposit_fixed(const float* x3, size_t n, float mass, int mesh_n, float h, int shift,
-                          unsigned long long* mesh_fx, cudaStream_t s, int ppt = 4);
+                          unsigned long long* mesh_fx, cudaStream_t s, int ppt = 4, size_t n_box = 0);
 // cells = (float)fx * 2^-shift, or delta = cells / mean - 1 when to_delta.
 void launch_fixed_to_f32(const unsigned long long* fx, size_t m, int shift, int to_delta, float mean, float* out,
                          cudaStream_t s);
@@ -185,6 +187,7 @@ struct PoissonParams {
   float scale;      // 1 / n^3 (f32)
   int deconvolve;
   const float* prefactor_dev = nullptr;  // when set, the prefactor is read from device memory
+  int boxes = 1;  // a batch of meshes of the same size, one after another (meshes up to 512)
 };
 // Input: either f32 delta (delta != nullptr) or the u64 fixed-point mass mesh (fx != nullptr,
 // converted to delta = c/mean - 1 on load). Output: three f32 meshes. spec: 3 half spectra
@@ -218,7 +221,7 @@ void launch_interpolate(const float* cells, const float* x3, size_t n, int mesh_
                         cudaStream_t s);
 // out3[i] = (interp gx, gy, gz)[i]; when `add` != 0, out3 += that instead (f32 add in reference order).
 void launch_interpolate3(const float* gx, const float* gy, const float* gz, const float* x3, size_t n, int mesh_n,
-                         float h, float* out3, cudaStream_t s);
+                         float h, float* out3, cudaStream_t s, size_t n_box = 0);
 
 // ---------------------------------------------------------------------------------------------
 // Tree — tree.cu
@@ -234,6 +237,7 @@ struct TreeNodes {
   DevBuf quad;      // per node 2 float4: second moments about the centre of mass (quadrupole mode)
   bool has_quad = false;  // the last build computed `quad`; the walk then adds quadrupole terms
   int walk_warps = 4;     // warps (groups of 32 particles) per walk block: 2, 4 or 8 (autotuned)
+  uint32_t n_box = 0;     // batch of boxes: particles per box (a multiple of 32), root of group = box
   size_t capacity = 0;
   void* walk_fit = nullptr;  // fitted pair-force coefficients of the last split (walk.cu)
 };
@@ -246,8 +250,12 @@ struct TreeCounters {
 // Builds the octree over sorted keys/positions (sorted x as AoS f32). Returns the node count
 // through the counters buffer (read by tree_node_count). quad_half_max > 0 also computes the second
 // moments of every node with half < quad_half_max (the walk then adds quadrupole terms).
+// With n_box > 0 the keys hold a batch of boxes (box index above `levels` octant digits, boxes of
+// n_box particles in order): one root per box (nodes 0 .. boxes - 1), and the walk starts each
+// group of 32 particles at its box's root.
 cudaError_t tree_build(TreeNodes& t, const uint64_t* sorted_keys, const float* sorted_x3, size_t n, float box,
-                       DevStatus* st, cudaStream_t s, float quad_half_max = 0.0f);
+                       DevStatus* st, cudaStream_t s, float quad_half_max = 0.0f, int levels = KEY_LEVELS,
+                       size_t n_box = 0);
 // Half size from which a node can never be accepted by the walk (prune radius r_cut + sqrt(3) half
 // from the centre, centre of mass inside the cube, 2 half < theta r): +inf when theta >= 1/sqrt(3).
 float quad_half_bound(const cpm_force_split& split);

@@ -33,10 +33,12 @@ __device__ __forceinline__ unsigned long long to_fixed(float mass, float w, floa
   return __float2ull_rn(__fmul_rn(__fmul_rn(mass, w), scale));
 }
 
+// With n_box > 0 the particles form a batch of boxes (box i / n_box, each with its own mesh of
+// mesh_n^3 cells, one after another); a tile that spans two boxes takes the global-atomic path.
 template <int DEP_PPT>
 __global__ void __launch_bounds__(DEP_THREADS) k_deposit_fixed(const float* __restrict__ x3, size_t n, float mass,
                                                                int mesh_n, float h, float scale,
-                                                               unsigned long long* __restrict__ mesh) {
+                                                               unsigned long long* __restrict__ mesh, size_t n_box) {
   extern __shared__ unsigned long long sm_cells[];
   __shared__ int bb[6];  // min x,y,z then max x,y,z of the stencil base
   if (threadIdx.x < 3) bb[threadIdx.x] = 0x7fffffff;
@@ -45,6 +47,13 @@ __global__ void __launch_bounds__(DEP_THREADS) k_deposit_fixed(const float* __re
 
   constexpr int DEP_CHUNK = DEP_THREADS * DEP_PPT;
   const size_t base = (size_t)blockIdx.x * DEP_CHUNK;
+  const size_t cells_per_box = (size_t)mesh_n * mesh_n * mesh_n;
+  bool one_box = true;
+  if (n_box) {
+    const size_t last = min(base + DEP_CHUNK, n) - 1;
+    one_box = base / n_box == last / n_box;
+    mesh += (base / n_box) * cells_per_box;  // the tile's box (the global path re-bases per particle)
+  }
   CicBase cb[DEP_PPT];
   bool valid[DEP_PPT];
   int lo[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff}, hi[3] = {-0x7fffffff, -0x7fffffff, -0x7fffffff};
@@ -82,7 +91,7 @@ __global__ void __launch_bounds__(DEP_THREADS) k_deposit_fixed(const float* __re
   const long long cells = (long long)e0 * e1 * e2;
   if (bb[0] > bb[3]) return;  // empty chunk
 
-  if (cells <= DEP_SMEM_CELLS && e0 > 0 && e1 > 0 && e2 > 0) {
+  if (one_box && cells <= DEP_SMEM_CELLS && e0 > 0 && e1 > 0 && e2 > 0) {
     for (int t = threadIdx.x; t < (int)cells; t += DEP_THREADS) sm_cells[t] = 0ull;
     __syncthreads();
 #pragma unroll
@@ -110,16 +119,21 @@ __global__ void __launch_bounds__(DEP_THREADS) k_deposit_fixed(const float* __re
 #pragma unroll
     for (int q = 0; q < DEP_PPT; ++q) {
       if (!valid[q]) continue;
+      unsigned long long* m = mesh;
+      if (n_box && !one_box) {
+        const size_t i = base + (size_t)q * DEP_THREADS + threadIdx.x;
+        m = mesh + ((i / n_box) - (base / n_box)) * cells_per_box;
+      }
 #pragma unroll
       for (int c = 0; c < 8; ++c)
-        atomicAdd(&mesh[cic_index(cb[q], c, mesh_n)], to_fixed(mass, cic_weight(cb[q], c), scale));
+        atomicAdd(&m[cic_index(cb[q], c, mesh_n)], to_fixed(mass, cic_weight(cb[q], c), scale));
     }
   }
 }
 
 template <int PPT>
 static void deposit_ppt(const float* x3, size_t n, float mass, int mesh_n, float h, float scale,
-                        unsigned long long* mesh_fx, cudaStream_t s) {
+                        unsigned long long* mesh_fx, cudaStream_t s, size_t n_box) {
   // Per device (a cheap host call, so made on every launch): a failure shows up as the launch's error.
   cudaFuncSetAttribute(k_deposit_fixed<PPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        DEP_SMEM_CELLS * (int)sizeof(unsigned long long));
@@ -127,21 +141,22 @@ static void deposit_ppt(const float* x3, size_t n, float mass, int mesh_n, float
   const unsigned blocks = (unsigned)((n + chunk - 1) / chunk);
   count_launch();
   k_deposit_fixed<PPT><<<blocks, DEP_THREADS, DEP_SMEM_CELLS * sizeof(unsigned long long), s>>>(x3, n, mass, mesh_n, h,
-                                                                                              scale, mesh_fx);
+                                                                                              scale, mesh_fx, n_box);
 }
 
 void launch_deposit_fixed(const float* x3, size_t n, float mass, int mesh_n, float h, int shift,
-                          unsigned long long* mesh_fx, cudaStream_t s, int ppt) {
-  const size_t m = (size_t)mesh_n * mesh_n * mesh_n;
+                          unsigned long long* mesh_fx, cudaStream_t s, int ppt, size_t n_box) {
+  const size_t boxes = n_box ? (n + n_box - 1) / n_box : 1;
+  const size_t m = (size_t)mesh_n * mesh_n * mesh_n * boxes;
   cudaMemsetAsync(mesh_fx, 0, m * sizeof(unsigned long long), s);
   if (n == 0) return;
   const float scale = std::ldexp(1.0f, shift);
   if (ppt == 2)
-    deposit_ppt<2>(x3, n, mass, mesh_n, h, scale, mesh_fx, s);
+    deposit_ppt<2>(x3, n, mass, mesh_n, h, scale, mesh_fx, s, n_box);
   else if (ppt == 8)
-    deposit_ppt<8>(x3, n, mass, mesh_n, h, scale, mesh_fx, s);
+    deposit_ppt<8>(x3, n, mass, mesh_n, h, scale, mesh_fx, s, n_box);
   else
-    deposit_ppt<4>(x3, n, mass, mesh_n, h, scale, mesh_fx, s);
+    deposit_ppt<4>(x3, n, mass, mesh_n, h, scale, mesh_fx, s, n_box);
 }
 
 // integrator.rs:117-126: cell mass c = fixed * 2^-k rounded once to f32; delta = c / mean - 1.

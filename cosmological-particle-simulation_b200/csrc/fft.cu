@@ -249,7 +249,14 @@ struct ColGeo {
   long long elem_stride;
   int cols;       // valid columns along the contiguous axis
   int col_tiles;  // ceil(cols / TW)
-  int outer;      // number of outer indices
+  int outer;      // number of outer indices (over every box of a batch)
+  int per_box = 0;            // outer indices per box when a batch's boxes are not one linear run
+  long long box_stride = 0;   // elements between the boxes of such a batch
+  __host__ __device__ long long offset(int o) const {
+    return per_box ? (long long)(o / per_box) * box_stride + (long long)(o % per_box) * outer_stride
+                   : (long long)o * outer_stride;
+  }
+  __host__ __device__ int in_box(int o) const { return per_box ? o % per_box : o; }
 };
 
 // Row transfers: chunks of TT = min(L, 16) consecutive t go to consecutive lanes, chunk-major
@@ -329,7 +336,7 @@ __global__ void __launch_bounds__(T) k_fft_cols(float2* data, long long comp_str
     const int comp = tile / per_comp, rest = tile % per_comp;
     const int o = rest / g.col_tiles, ct = rest % g.col_tiles;
     d = data + (long long)comp * comp_stride;
-    base = (long long)o * g.outer_stride + (long long)ct * TW;
+    base = g.offset(o) + (long long)ct * TW;
     valid = min(TW, g.cols - ct * TW);
   };
   pipeline<NBUF>(
@@ -507,17 +514,17 @@ __global__ void __launch_bounds__(T) k_poisson_x(const float2* __restrict__ spec
       smem, N * TLD, g.outer * g.col_tiles,
       [&](float2* buf, int tile) {
         const int iy = tile / g.col_tiles, ct = tile % g.col_tiles;
-        const long long base = (long long)iy * g.outer_stride + (long long)ct * TW;
+        const long long base = g.offset(iy) + (long long)ct * TW;
         async_load_cols<N, T>(buf, spec_in, base, g.elem_stride, min(TW, g.cols - ct * TW));
       },
       [&](float2* phi, int tile) {
         const int iy = tile / g.col_tiles, ct = tile % g.col_tiles;
         const int valid = min(TW, g.cols - ct * TW);
-        const long long base = (long long)iy * g.outer_stride + (long long)ct * TW;
+        const long long base = g.offset(iy) + (long long)ct * TW;
         const int z0 = ct * TW;
         const float prefactor = pp.prefactor_dev ? *pp.prefactor_dev : pp.prefactor;
         fft_lines<N, false, T, 1, MR>(phi, tw);
-        const float ky = wavenumber(iy, N, pp.two_pi_over_l);
+        const float ky = wavenumber(g.in_box(iy), N, pp.two_pi_over_l);
         for (int q = threadIdx.x; q < N * TW; q += T) {
           const int l = q % TW, t = q / TW;
           const float kx = wavenumber(t, N, pp.two_pi_over_l);
@@ -533,7 +540,7 @@ __global__ void __launch_bounds__(T) k_poisson_x(const float2* __restrict__ spec
             // phi_k = delta_k * (-prefactor / k^2 * exp(-k^2 r_s^2)), k = 0 skipped (left zero)
             const float filter = expf(__fmul_rn(__fmul_rn(-k2, pp.r_split), pp.r_split));
             float sc = __fmul_rn(__fdiv_rn(-prefactor, k2), filter);
-            if (deconv) sc = __fmul_rn(sc, __fmul_rn(__fmul_rn(deconv[t], deconv[iy]), deconv[z0 + l]));
+            if (deconv) sc = __fmul_rn(sc, __fmul_rn(__fmul_rn(deconv[t], deconv[g.in_box(iy)]), deconv[z0 + l]));
             v = make_float2(__fmul_rn(v.x, sc), __fmul_rn(v.y, sc));
           }
           phi[t * TLD + l] = v;
@@ -565,13 +572,13 @@ __global__ void __launch_bounds__(T) k_grad_yz(float2* spec, long long comp_stri
       smem, N * TLD, g.outer * g.col_tiles,
       [&](float2* buf, int tile) {
         const int o = tile / g.col_tiles, ct = tile % g.col_tiles;
-        const long long base = (long long)o * g.outer_stride + (long long)ct * TW;
+        const long long base = g.offset(o) + (long long)ct * TW;
         async_load_cols<N, T>(buf, phi_slot, base, g.elem_stride, min(TW, g.cols - ct * TW));
       },
       [&](float2* cur, int tile) {
         const int o = tile / g.col_tiles, ct = tile % g.col_tiles;
         const int valid = min(TW, g.cols - ct * TW);
-        const long long base = (long long)o * g.outer_stride + (long long)ct * TW;
+        const long long base = g.offset(o) + (long long)ct * TW;
         const int z0 = ct * TW;
         for (int q = threadIdx.x; q < N * TW; q += T) {
           const int l = q % TW, t = q / TW;
@@ -777,8 +784,9 @@ static void poisson_n(const FftPlan& p, const PoissonParams& pp, const float* de
   const float* deconv = pp.deconvolve ? static_cast<const float*>(p.deconv.p) : nullptr;
   constexpr int M = N / 2, NH = N / 2 + 1, NHP = N / 2 + 2;
   const long long n = N;
-  const long long comp = n * n * NHP;  // elements per half spectrum
-  const int rows = N * N;
+  const int nb = pp.boxes > 1 ? pp.boxes : 1;  // a batch of nb meshes, one after another
+  const long long comp = nb * n * n * NHP;     // elements per half spectrum (every box)
+  const int rows = nb * N * N;
   const int row_tiles = (rows + TW - 1) / TW;
   if constexpr (2 * c_tile(N) > SMEM_LIMIT) {
     // The fused x pass needs two N-point tiles: not on one SM at this size. Forward R2C, the
@@ -801,21 +809,22 @@ static void poisson_n(const FftPlan& p, const PoissonParams& pp, const float* de
                         rows, tw);
     }
     // 2. y forward on slot 0: lines along y (stride NHP), columns along kz adjacent, outer = x
-    cols_pass<N, MR>(s0, 0, 1, ColGeo{n * NHP, NHP, NH, 0, N}, 0, tw, s);
+    //    (the x planes of a batch's boxes form one run)
+    cols_pass<N, MR>(s0, 0, 1, ColGeo{n * NHP, NHP, NH, 0, nb * N}, 0, tw, s);
     {  // 3. x forward + Green + gradient + x inverse -> slots 0 (-i k_x phi) and 1 (phi); outer = y
       constexpr int T = threads_for<N>();
       constexpr int NBX = 3 * c_tile(N) <= SMEM_LIMIT ? 2 : 1;
       const size_t smem = (NBX + 1) * c_tile(N);
-      ColGeo g{NHP, n * NHP, NH, (NH + TW - 1) / TW, N};
+      ColGeo g{NHP, n * NHP, NH, (NH + TW - 1) / TW, nb * N, nb > 1 ? N : 0, n * n * NHP};
       launch_persistent(k_poisson_x<N, NBX, T, MR>, T, smem, g.outer * g.col_tiles, s, s0, spec, comp, g, pp, deconv, tw);
     }
     // 4. y inverse: slot 0 (x component), then slots 1, 2 (y, z components) from the potential
-    cols_pass<N, MR>(spec, comp, 1, ColGeo{n * NHP, NHP, NH, 0, N}, 1, tw, s);
+    cols_pass<N, MR>(spec, comp, 1, ColGeo{n * NHP, NHP, NH, 0, nb * N}, 1, tw, s);
     {
       constexpr int T = threads_for<N>();
       constexpr int NBY = 3 * c_tile(N) <= SMEM_LIMIT ? 2 : 1;
       const size_t smem = (NBY + 1) * c_tile(N);
-      ColGeo g{n * NHP, NHP, NH, (NH + TW - 1) / TW, N};
+      ColGeo g{n * NHP, NHP, NH, (NH + TW - 1) / TW, nb * N};
       launch_persistent(k_grad_yz<N, NBY, T, MR>, T, smem, g.outer * g.col_tiles, s, spec, comp, g, pp, tw);
     }
   }

@@ -20,11 +20,18 @@ __global__ void k_interpolate(const float* __restrict__ cells, const float* __re
   out[i] = sum;
 }
 
+// n_box > 0: a batch of boxes (box i / n_box reads its own meshes, mesh_n^3 cells each, in order).
 __global__ void k_interpolate3(const float* __restrict__ gx, const float* __restrict__ gy,
                                const float* __restrict__ gz, const float* __restrict__ x3, size_t n, int mesh_n,
-                               float h, float* __restrict__ out3) {
+                               float h, float* __restrict__ out3, size_t n_box) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  if (n_box) {
+    const size_t off = (i / n_box) * ((size_t)mesh_n * mesh_n * mesh_n);
+    gx += off;
+    gy += off;
+    gz += off;
+  }
   const float x[3] = {x3[3 * i], x3[3 * i + 1], x3[3 * i + 2]};
   CicBase c;
   cic_base(x, h, mesh_n, c);
@@ -50,10 +57,10 @@ void launch_interpolate(const float* cells, const float* x3, size_t n, int mesh_
 }
 
 void launch_interpolate3(const float* gx, const float* gy, const float* gz, const float* x3, size_t n, int mesh_n,
-                         float h, float* out3, cudaStream_t s) {
+                         float h, float* out3, cudaStream_t s, size_t n_box) {
   if (n == 0) return;
   count_launch();
-  k_interpolate3<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(gx, gy, gz, x3, n, mesh_n, h, out3);
+  k_interpolate3<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(gx, gy, gz, x3, n, mesh_n, h, out3, n_box);
 }
 
 }  // namespace cpm

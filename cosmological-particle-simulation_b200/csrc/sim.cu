@@ -85,6 +85,11 @@ struct cpm_sim {
   float net_threshold = 50.0f;
   float net_in_scale = 1.0f;
   DevBuf flag, offset, list, list_n, scan_tmp;
+  // A batch of nb boxes of n_box particles each (the ensemble): particles box by box, nb meshes one
+  // after another, the box index above `levels` octant digits in the sort keys. nb = 1: one box.
+  int nb = 1;
+  size_t n_box = 0;
+  int levels = KEY_LEVELS;
   // Autotuned launch choices (FFT radix plan in `plan`, walk warps in `tree`) and the timings.
   int dep_ppt = 4;
   float tune_ms[8] = {};
@@ -165,11 +170,17 @@ static void swap_sorted(cpm_sim* s) {
 
 static bool fixed_point(const cpm_sim* s) { return (s->P.flags & CPM_SIM_FIXED_POINT) != 0; }
 
+// Particles of one box (the N of the reference's formulas, integrator.rs:120, :152).
+static size_t per_box(const cpm_sim* s) { return s->nb > 1 ? s->n_box : s->n; }
+// Particles per box of a batch, 0 for a single box (the batched kernels' parameter).
+static size_t batch_box(const cpm_sim* s) { return s->nb > 1 ? s->n_box : 0; }
+static size_t mesh_cells(const cpm_sim* s) { return (size_t)s->P.mesh_n * s->P.mesh_n * s->P.mesh_n; }
+
 // Output scale of the learned short-range field: the tree coupling K(a) (integrator.rs:150-152) times
 // the mean particles per cell over the cell size, which makes the net's output dimensionless.
 static float net_field_scale(const cpm_sim* s, float a) {
   const float m = (float)((double)s->P.mesh_n * s->P.mesh_n * s->P.mesh_n);
-  return tree_coupling(s->P.cosmo.omega_m, s->box, a, s->n) * ((float)s->n / m) / s->h;
+  return tree_coupling(s->P.cosmo.omega_m, s->box, a, per_box(s)) * ((float)per_box(s) / m) / s->h;
 }
 
 // Sort into key order, then the force: deposit, FFT-Poisson, gather, tree. Phases 1..6. With
@@ -178,9 +189,9 @@ static int sim_accelerations(cpm_sim* s, float a, const StepScalars* dev = nullp
   const size_t n = s->n;
   const int mn = s->P.mesh_n;
   mark(s, 1);
-  launch_octant_keys(as<float>(s->x), n, s->box, KEY_LEVELS, as<uint64_t>(s->keys), as<uint32_t>(s->vals),
-                     as<DevStatus>(s->status), s->stream);
-  SIM_CU(s, radix_sort_pairs(as<uint64_t>(s->keys), as<uint32_t>(s->vals), n, 3 * KEY_LEVELS, s->sort, s->stream));
+  launch_octant_keys(as<float>(s->x), n, s->box, s->levels, as<uint64_t>(s->keys), as<uint32_t>(s->vals),
+                     as<DevStatus>(s->status), s->stream, batch_box(s));
+  SIM_CU(s, radix_sort_pairs(as<uint64_t>(s->keys), as<uint32_t>(s->vals), n, 63, s->sort, s->stream));
   launch_permute3(as<float>(s->x), as<uint32_t>(s->vals), n, as<float>(s->x2), s->stream);
   launch_permute3(as<float>(s->p), as<uint32_t>(s->vals), n, as<float>(s->p2), s->stream);
   launch_permute_u32(as<uint32_t>(s->id), as<uint32_t>(s->vals), n, as<uint32_t>(s->id2), s->stream);
@@ -196,12 +207,13 @@ static int sim_accelerations(cpm_sim* s, float a, const StepScalars* dev = nullp
   }
   mark(s, 2);
   launch_deposit_fixed(as<float>(s->x), n, 1.0f, mn, s->h, s->shift, as<unsigned long long>(s->fx), s->stream,
-                       s->dep_ppt);
+                       s->dep_ppt, batch_box(s));
   mark(s, 3);
   const float r_split = s->P.use_tree ? s->P.split.r_split : 0.0f;
   PoissonParams pp =
       make_poisson_params(mn, s->box, s->P.cosmo.omega_m, a, r_split, (s->P.flags & CPM_SIM_DECONVOLVE) ? 1 : 0);
   if (dev) pp.prefactor_dev = &dev->prefactor;
+  pp.boxes = s->nb;
   launch_poisson(s->plan, pp, nullptr, as<unsigned long long>(s->fx), s->shift, s->mean, as<float2>(s->spec),
                  as<float>(s->gx), as<float>(s->gy), as<float>(s->gz), s->stream);
   mark(s, 4);
@@ -217,16 +229,16 @@ static int sim_accelerations(cpm_sim* s, float a, const StepScalars* dev = nullp
                              as<uint32_t>(s->list_n), s->scan_tmp, s->stream));
   } else {
     launch_interpolate3(as<float>(s->gx), as<float>(s->gy), as<float>(s->gz), as<float>(s->x), n, mn, s->h,
-                        as<float>(s->acc), s->stream);
+                        as<float>(s->acc), s->stream, batch_box(s));
   }
   mark(s, 5);
   if (s->P.use_tree) {
     const float quad_half = (s->P.flags & CPM_SIM_QUADRUPOLE) ? quad_half_bound(s->P.split) : 0.0f;
     SIM_CU(s, tree_build(s->tree, as<uint64_t>(s->keys), as<float>(s->x), n, s->box, as<DevStatus>(s->status),
-                         s->stream, quad_half));
+                         s->stream, quad_half, s->levels, batch_box(s)));
     mark(s, 6);
     SIM_CU(s, cudaMemsetAsync(s->counters.p, 0, sizeof(TreeCounters), s->stream));
-    const float k = tree_coupling(s->P.cosmo.omega_m, s->box, a, n);
+    const float k = tree_coupling(s->P.cosmo.omega_m, s->box, a, per_box(s));
     launch_tree_walk(s->tree, as<float>(s->x), n, s->box, s->P.split, k, as<float>(s->acc), 1,
                      as<TreeCounters>(s->counters), as<DevStatus>(s->status), s->stream,
                      dev ? &dev->tree_k : nullptr, learned ? as<uint32_t>(s->list) : nullptr,
@@ -260,8 +272,8 @@ bool g_tune_file_read = false;
 
 std::string tune_key(const cpm_sim* s) {
   char buf[160];
-  std::snprintf(buf, sizeof(buf), "n=%zu mesh=%d tree=%d quad=%d", s->n, s->P.mesh_n, s->P.use_tree,
-                (s->P.flags & CPM_SIM_QUADRUPOLE) ? 1 : 0);
+  std::snprintf(buf, sizeof(buf), "n=%zu mesh=%d boxes=%d tree=%d quad=%d", per_box(s), s->P.mesh_n, s->nb,
+                s->P.use_tree, (s->P.flags & CPM_SIM_QUADRUPOLE) ? 1 : 0);
   return buf;
 }
 
@@ -335,8 +347,9 @@ static int sim_autotune(cpm_sim* s) {
   TuneChoice c;
   const int mn = s->P.mesh_n;
   const float r_split = s->P.use_tree ? s->P.split.r_split : 0.0f;
-  const PoissonParams pp =
+  PoissonParams pp =
       make_poisson_params(mn, s->box, s->P.cosmo.omega_m, s->a, r_split, (s->P.flags & CPM_SIM_DECONVOLVE) ? 1 : 0);
+  pp.boxes = s->nb;
   const int radices[2] = {8, 4};
   float best = 1e30f;
   for (int k = 0; k < 2; ++k) {
@@ -352,14 +365,14 @@ static int sim_autotune(cpm_sim* s) {
   for (int k = 0; k < 3; ++k) {
     c.ms[2 + k] = time_ms(s->stream, e0, e1, [&] {
       launch_deposit_fixed(as<float>(s->x), s->n, 1.0f, mn, s->h, s->shift, as<unsigned long long>(s->fx), s->stream,
-                           tiles[k]);
+                           tiles[k], batch_box(s));
     });
     if (c.ms[2 + k] < best) best = c.ms[2 + k], c.ppt = tiles[k];
   }
   if (s->P.use_tree && s->tree.geo.p && !(s->P.flags & CPM_SIM_QUADRUPOLE)) {
     int rc = ensure(s->host_tmp, 3 * s->n * sizeof(float)) == cudaSuccess ? CPM_OK : CPM_E_NOMEM;
     if (rc) return set_error(&s->err, rc, "autotune: scratch allocation failed");
-    const float kk = tree_coupling(s->P.cosmo.omega_m, s->box, s->a, s->n);
+    const float kk = tree_coupling(s->P.cosmo.omega_m, s->box, s->a, per_box(s));
     const int warps[3] = {2, 4, 8};
     best = 1e30f;
     for (int k = 0; k < 3; ++k) {
@@ -386,10 +399,13 @@ static int sim_autotune(cpm_sim* s) {
 }
 
 // Validates the parameters and allocates every device buffer of a simulation.
-static int sim_new(const cpm_sim_params* params, float a0, cpm_sim** out) {
+static int sim_new(const cpm_sim_params* params, float a0, cpm_sim** out, int nb = 1) {
   const cpm_sim_params& P = *params;
-  if (P.n_particles == 0 || P.n_particles > 0x7FFFFFFFull)
+  if (P.n_particles == 0 || P.n_particles * (size_t)(nb > 0 ? nb : 1) > 0x7FFFFFFFull)
     return set_error(nullptr, CPM_E_INVALID, "cpm_sim_create: n_particles must be in [1, 2^31)");
+  if (nb < 1 || nb > 64 || (nb > 1 && (P.n_particles % 2048 != 0 || P.mesh_n > 512)))
+    return set_error(nullptr, CPM_E_INVALID,
+                     "batch: 1..64 boxes of a multiple of 2048 particles each, meshes up to 512");
   if (!(P.box_size > 0.0f) || !(a0 > 0.0f)) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_create: box and a0 must be > 0");
   if (!poisson_supported(P.mesh_n))
     return set_error(nullptr, CPM_E_UNSUPPORTED,
@@ -398,12 +414,16 @@ static int sim_new(const cpm_sim_params* params, float a0, cpm_sim** out) {
   if (rc) return rc;
   cpm_sim* s = new cpm_sim();
   s->P = P;
-  s->n = P.n_particles;
+  s->nb = nb;
+  s->n_box = P.n_particles;
+  s->levels = nb > 1 ? KEY_LEVELS - 2 : KEY_LEVELS;  // 19 octant digits under 6 bits of box index
+  s->tree.n_box = nb > 1 ? (uint32_t)P.n_particles : 0u;
+  s->n = P.n_particles * (size_t)nb;
   s->box = P.box_size;
   s->h = P.box_size / (float)P.mesh_n;
-  const size_t m = (size_t)P.mesh_n * P.mesh_n * P.mesh_n;
-  s->mean = (float)s->n / (float)m;  // integrator.rs:120-121
-  s->shift = fixed_point_shift((double)s->n + 1.0);
+  const size_t m = (size_t)P.mesh_n * P.mesh_n * P.mesh_n * (size_t)nb;
+  s->mean = (float)P.n_particles / (float)((size_t)P.mesh_n * P.mesh_n * P.mesh_n);  // integrator.rs:120-121
+  s->shift = fixed_point_shift((double)P.n_particles + 1.0);
   s->a = a0;
   auto fail = [&](int code) {
     g_last_error = s->err;
@@ -423,7 +443,7 @@ static int sim_new(const cpm_sim_params* params, float a0, cpm_sim** out) {
   ok = ok && ensure(s->keys, n * sizeof(uint64_t)) == cudaSuccess;
   ok = ok && ensure(s->fx, m * sizeof(unsigned long long)) == cudaSuccess;
   for (DevBuf* b : {&s->gx, &s->gy, &s->gz}) ok = ok && ensure(*b, m * sizeof(float)) == cudaSuccess;
-  ok = ok && ensure(s->spec, 3 * half * sizeof(float2)) == cudaSuccess;
+  ok = ok && ensure(s->spec, 3 * half * (size_t)nb * sizeof(float2)) == cudaSuccess;
   ok = ok && ensure(s->status, sizeof(DevStatus)) == cudaSuccess;
   ok = ok && ensure(s->counters, sizeof(TreeCounters)) == cudaSuccess;
   ok = ok && ensure(s->stepv, sizeof(StepScalars)) == cudaSuccess;
@@ -554,31 +574,37 @@ static int step_captured(cpm_sim* s, int q, float a1) {
   return CPM_OK;
 }
 
-int cpm_sim_step_to(cpm_sim* s, float a1) {
-  if (!s) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_step_to: sim is NULL");
-  if (!(a1 > 0.0f) || !std::isfinite(a1)) return set_error(&s->err, CPM_E_INVALID, "cpm_sim_step_to: a1 must be > 0");
+// Writes the scalars of the step a -> a1 into the device step block, on stream `st`: the reference's
+// f32 factors (integrator.rs:263-297) from the host, or in precision mode the FP64 device factors.
+static void sim_write_step_scalars(cpm_sim* s, float a1, cudaStream_t st) {
   const cpm_cosmology& c = s->P.cosmo;
   const float a0 = s->a;
+  if (fixed_point(s)) {
+    const double m = (double)s->P.mesh_n * s->P.mesh_n * s->P.mesh_n;
+    launch_step_factors64(as<StepScalars>(s->stepv), c, (double)a0, (double)a1, (double)s->box, (double)per_box(s),
+                          ((double)per_box(s) / m) / (double)s->h, st);
+    return;
+  }
   const float am = midpoint(c, a0, a1);
   StepScalars sc;
   sc.k1 = kick_factor(c, a0, am);
   sc.d = drift_factor(c, a0, a1);
   sc.k2 = kick_factor(c, am, a1);
   sc.prefactor = make_poisson_params(s->P.mesh_n, s->box, c.omega_m, a1, 0.0f, 0).prefactor;
-  sc.tree_k = tree_coupling(c.omega_m, s->box, a1, s->n);
+  sc.tree_k = tree_coupling(c.omega_m, s->box, a1, per_box(s));
   sc.net_scale = net_field_scale(s, a1);
+  sc.pad_ = 0.0f;
+  sc.d64 = (double)sc.d;
+  launch_set_step_scalars(as<StepScalars>(s->stepv), sc, st);
+}
+
+int cpm_sim_step_to(cpm_sim* s, float a1) {
+  if (!s) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_step_to: sim is NULL");
+  if (!(a1 > 0.0f) || !std::isfinite(a1)) return set_error(&s->err, CPM_E_INVALID, "cpm_sim_step_to: a1 must be > 0");
   const int q = s->parity;
   int rc;
   if ((s->P.flags & CPM_SIM_TIMING) && (rc = flush_set(s, q))) return rc;
-  sc.pad_ = 0.0f;
-  sc.d64 = (double)sc.d;
-  if (fixed_point(s)) {  // precision mode: the step's scalars in FP64 on the device
-    const double m = (double)s->P.mesh_n * s->P.mesh_n * s->P.mesh_n;
-    launch_step_factors64(as<StepScalars>(s->stepv), s->P.cosmo, (double)a0, (double)a1, (double)s->box,
-                          (double)s->n, ((double)s->n / m) / (double)s->h, s->stream);
-  } else {
-    launch_set_step_scalars(as<StepScalars>(s->stepv), sc, s->stream);
-  }
+  sim_write_step_scalars(s, a1, s->stream);
   const unsigned long long l0 = launch_count();
   s->ev_set = q;
   const bool graphs =
@@ -661,7 +687,7 @@ int cpm_sim_get_state(cpm_sim* s, float* x3, float* p3, float* acc3, float* delt
     SIM_CU(s, cudaMemcpyAsync(dsts[q], s->x2.p, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
   }
   if (delta) {
-    const size_t m = (size_t)s->P.mesh_n * s->P.mesh_n * s->P.mesh_n;
+    const size_t m = mesh_cells(s) * (size_t)s->nb;
     launch_fixed_to_f32(as<unsigned long long>(s->fx), m, s->shift, 1, s->mean, as<float>(s->gx), s->stream);
     SIM_CU(s, cudaMemcpyAsync(delta, s->gx.p, m * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
   }
@@ -674,6 +700,7 @@ int cpm_sim_power_spectrum(cpm_sim* s, int n_shells, double* k_mean, double* p_m
   if (!k_mean || !p_mean || !counts) return set_error(&s->err, CPM_E_INVALID, "cpm_sim_power_spectrum: null pointer");
   if (n_shells < 1 || n_shells > PK_MAX_SHELLS)
     return set_error(&s->err, CPM_E_INVALID, "cpm_sim_power_spectrum: n_shells must be in [1, 2048]");
+  if (s->nb > 1) return set_error(&s->err, CPM_E_INVALID, "cpm_sim_power_spectrum: a batch (use the ensemble's)");
   const int mn = s->P.mesh_n;
   // The deposit of the current positions (the mesh of the last force evaluation may predate a
   // set_state); the next step deposits again before it uses the mesh.
@@ -692,6 +719,7 @@ int cpm_sim_power_spectrum(cpm_sim* s, int n_shells, double* k_mean, double* p_m
 int cpm_sim_snapshot(cpm_sim* s, float* speeds, float* densities, float* rsd3, float* grid, int* grid_n,
                      float* max_speed) {
   if (!s) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_snapshot: sim is NULL");
+  if (s->nb > 1) return set_error(&s->err, CPM_E_INVALID, "cpm_sim_snapshot: not for a batch of boxes");
   const size_t n = s->n;
   const int mn = s->P.mesh_n;
   const size_t m3 = (size_t)mn * mn * mn;
@@ -764,6 +792,16 @@ int cpm_sim_counters(cpm_sim* s, uint64_t* nodes, uint64_t* leaf_pairs, uint64_t
   if (leaf_pairs) *leaf_pairs = tc[0];
   if (node_accepts) *node_accepts = tc[1];
   if (launches_per_step) *launches_per_step = s->launches;
+  return CPM_OK;
+}
+
+int cpm_sim_tree_depth(cpm_sim* s, uint32_t* max_depth, uint64_t* key_depth_leaves) {
+  if (!s) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_tree_depth: sim is NULL");
+  SIM_CU(s, cudaStreamSynchronize(s->stream));
+  uint32_t cnt[64] = {};
+  if (s->tree.counters.p) SIM_CU(s, cudaMemcpy(cnt, s->tree.counters.p, sizeof(cnt), cudaMemcpyDeviceToHost));
+  if (max_depth) *max_depth = cnt[33];         // deepest level that split
+  if (key_depth_leaves) *key_depth_leaves = cnt[32];  // nodes kept as leaves at the key depth
   return CPM_OK;
 }
 
@@ -899,6 +937,7 @@ int cpm_sim_set_learned(cpm_sim* s, cpm_net* net, float delta_threshold, float i
     return set_error(&s->err, CPM_E_MESH_MISMATCH, "cpm_sim_set_learned: the net's mesh differs from the simulation's");
   if (net && !s->P.use_tree)
     return set_error(&s->err, CPM_E_INVALID, "cpm_sim_set_learned: a pure PM simulation has no short-range force");
+  if (net && s->nb > 1) return set_error(&s->err, CPM_E_INVALID, "cpm_sim_set_learned: not for a batch of boxes");
   if (net && (!std::isfinite(delta_threshold) || !(in_scale > 0.0f) || !std::isfinite(in_scale)))
     return set_error(&s->err, CPM_E_INVALID, "cpm_sim_set_learned: threshold must be finite and in_scale > 0");
   if (net) {
@@ -928,7 +967,7 @@ int cpm_sim_short_range(cpm_sim* s, float* sr3) {
   SIM_CU(s, ensure(s->host_tmp, 3 * n * sizeof(float)));
   // the tree of the last force evaluation was built on the current positions (the kick that ends a
   // step changes the momenta only)
-  const float k = tree_coupling(s->P.cosmo.omega_m, s->box, s->a, n);
+  const float k = tree_coupling(s->P.cosmo.omega_m, s->box, s->a, per_box(s));
   launch_tree_walk(s->tree, as<float>(s->x), n, s->box, s->P.split, k, as<float>(s->host_tmp), 0, nullptr,
                    as<DevStatus>(s->status), s->stream);
   launch_scatter3(as<float>(s->host_tmp), as<uint32_t>(s->id), n, as<float>(s->x2), s->stream);
@@ -1005,5 +1044,236 @@ int cpm_sim_destroy(cpm_sim* s) {
   delete s;
   return CPM_OK;
 }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// Ensemble: many independent realisations of uneven sizes (no counterpart in the reference, which
+// runs one realisation per run, runner.rs:228-260). Each size class is one batched simulation
+// (its boxes share every launch: keys, sort, deposit, the batched FFT passes, gather, tree build
+// with one root per box, walk), and a step of the whole ensemble is one CUDA graph: the classes
+// run as parallel branches forked from the ensemble's stream and joined back.
+// ---------------------------------------------------------------------------------------------
+struct cpm_ensemble {
+  std::vector<cpm_sim*> classes;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> join;
+  cudaGraphExec_t graph[2] = {};
+  bool warm[2] = {false, false};
+  bool no_graph[2] = {false, false};
+  std::string err;
+  float a = 0.0f;
+};
+
+namespace {
+
+// Forks every class off the ensemble's stream, runs its step body on its own stream, joins back.
+int ensemble_branches(cpm_ensemble* e, float a1) {
+  cudaError_t ce = cudaEventRecord(e->fork, e->stream);
+  for (size_t c = 0; c < e->classes.size() && ce == cudaSuccess; ++c) {
+    cpm_sim* s = e->classes[c];
+    ce = cudaStreamWaitEvent(s->stream, e->fork, 0);
+    if (ce != cudaSuccess) break;
+    const int rc = step_body(s, a1);
+    if (rc) {
+      e->err = s->err;
+      return rc;
+    }
+    ce = cudaEventRecord(e->join[c], s->stream);
+    if (ce == cudaSuccess) ce = cudaStreamWaitEvent(e->stream, e->join[c], 0);
+  }
+  if (ce != cudaSuccess) return set_error(&e->err, CPM_E_CUDA, std::string("ensemble step: ") + cudaGetErrorString(ce));
+  return CPM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cpm_ensemble_destroy(cpm_ensemble* e) {
+  if (!e) return CPM_OK;
+  if (e->stream) cudaStreamSynchronize(e->stream);
+  for (cudaGraphExec_t& g : e->graph)
+    if (g) cudaGraphExecDestroy(g);
+  for (cpm_sim* s : e->classes) cpm_sim_destroy(s);
+  for (cudaEvent_t ev : e->join)
+    if (ev) cudaEventDestroy(ev);
+  if (e->fork) cudaEventDestroy(e->fork);
+  if (e->stream) cudaStreamDestroy(e->stream);
+  delete e;
+  return CPM_OK;
+}
+
+int cpm_ensemble_create(const cpm_cosmology* cosmo, float box_size, float n_s, float sigma8, float a0, int n_classes,
+                        const cpm_ensemble_class* classes, uint32_t flags, cpm_ensemble** out) {
+  if (!out) return set_error(nullptr, CPM_E_INVALID, "cpm_ensemble_create: out is NULL");
+  *out = nullptr;
+  if (!cosmo || !classes || n_classes < 1 || n_classes > 16)
+    return set_error(nullptr, CPM_E_INVALID, "cpm_ensemble_create: 1..16 classes and a cosmology are required");
+  if (!(box_size > 0.0f) || !(a0 > 0.0f) || !(sigma8 > 0.0f))
+    return set_error(nullptr, CPM_E_INVALID, "cpm_ensemble_create: box, a0 and sigma8 must be > 0");
+  if (flags & (CPM_SIM_TIMING | CPM_SIM_QUADRUPOLE))
+    return set_error(nullptr, CPM_E_INVALID, "cpm_ensemble_create: CPM_SIM_TIMING and CPM_SIM_QUADRUPOLE are per simulation");
+  for (int c = 0; c < n_classes; ++c) {
+    const cpm_ensemble_class& k = classes[c];
+    const size_t nbox = (size_t)k.n_side * k.n_side * k.n_side;
+    if (!fft_supported(k.n_side) || k.n_boxes < 1 || k.n_boxes > 64 || nbox % 2048 != 0 || k.mesh_n > 512 ||
+        !poisson_supported(k.mesh_n))
+      return set_error(nullptr, CPM_E_INVALID,
+                       "cpm_ensemble_create: class " + std::to_string(c) +
+                           ": 1..64 boxes, n_side a supported FFT length with n_side^3 a multiple of 2048, "
+                           "mesh a supported length up to 512");
+  }
+  int rc = check_device_once(nullptr);
+  if (rc) return rc;
+  cpm_ensemble* e = new cpm_ensemble();
+  e->a = a0;
+  auto fail = [&](int code, const std::string& msg) {
+    set_error(nullptr, code, msg);
+    cpm_ensemble_destroy(e);
+    return code;
+  };
+  if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) != cudaSuccess)
+    return fail(CPM_E_CUDA, "cpm_ensemble_create: stream or event creation failed");
+  e->join.assign((size_t)n_classes, nullptr);
+  for (auto& ev : e->join)
+    if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess)
+      return fail(CPM_E_CUDA, "cpm_ensemble_create: event creation failed");
+  for (int c = 0; c < n_classes; ++c) {
+    const cpm_ensemble_class& k = classes[c];
+    cpm_sim_params P{};
+    P.cosmo = *cosmo;
+    P.box_size = box_size;
+    P.mesh_n = k.mesh_n;
+    P.n_particles = (size_t)k.n_side * k.n_side * k.n_side;
+    P.use_tree = 1;
+    P.split = k.split;
+    P.flags = flags;
+    cpm_sim* s = nullptr;
+    rc = sim_new(&P, a0, &s, k.n_boxes);
+    if (rc) return fail(rc, g_last_error);
+    e->classes.push_back(s);
+    // ics.rs:119-182 for every box of the class, seeds first_seed + b, into the box's slice
+    DevBuf modes, work;
+    FftPlan plan;
+    cudaError_t ce = cudaSuccess;
+    for (int b = 0; b < k.n_boxes && ce == cudaSuccess; ++b)
+      ce = generate_zeldovich(k.n_side, box_size, *cosmo, n_s, sigma8, a0, k.first_seed + (uint64_t)b,
+                              as<float>(s->x) + 3 * P.n_particles * (size_t)b,
+                              as<float>(s->p) + 3 * P.n_particles * (size_t)b, modes, work, plan, s->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s->stream);
+    release(modes);
+    release(work);
+    fft_plan_free(plan);
+    if (ce != cudaSuccess)
+      return fail(ce == cudaErrorMemoryAllocation ? CPM_E_NOMEM : CPM_E_CUDA,
+                  std::string("cpm_ensemble_create: initial conditions: ") + cudaGetErrorString(ce));
+    launch_iota(as<uint32_t>(s->id), s->n, s->stream);
+    if (fixed_point(s)) launch_to_fixed(as<float>(s->x), as<uint32_t>(s->q), s->n, s->box, s->stream);
+    rc = sim_accelerations(s, s->a);
+    if (rc == CPM_OK) rc = sim_check(s);
+    if (rc == CPM_OK) rc = sim_autotune(s);
+    if (rc) return fail(rc, s->err);
+  }
+  *out = e;
+  return CPM_OK;
+}
+
+int cpm_ensemble_step_to(cpm_ensemble* e, float a1) {
+  if (!e) return set_error(nullptr, CPM_E_INVALID, "cpm_ensemble_step_to: ensemble is NULL");
+  if (!(a1 > 0.0f) || !std::isfinite(a1)) return set_error(&e->err, CPM_E_INVALID, "cpm_ensemble_step_to: a1 must be > 0");
+  // every class's step scalars, on the ensemble's stream ahead of the branches
+  for (cpm_sim* s : e->classes) sim_write_step_scalars(s, a1, e->stream);
+  const int q = e->classes[0]->parity;  // the classes' sorted buffers alternate together
+  const bool graphs = !(e->classes[0]->P.flags & CPM_SIM_NO_GRAPH) && e->warm[q] && !e->no_graph[q];
+  int rc = CPM_OK;
+  if (graphs && e->graph[q]) {
+    const cudaError_t ce = cudaGraphLaunch(e->graph[q], e->stream);
+    if (ce != cudaSuccess) return set_error(&e->err, CPM_E_CUDA, std::string("cudaGraphLaunch: ") + cudaGetErrorString(ce));
+    for (cpm_sim* s : e->classes) swap_sorted(s);  // the host side of the replayed sorts
+  } else if (graphs) {
+    cudaError_t ce = cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal);
+    rc = ce == cudaSuccess ? ensemble_branches(e, a1) : CPM_E_CUDA;
+    cudaGraph_t g = nullptr;
+    if (ce == cudaSuccess) ce = cudaStreamEndCapture(e->stream, &g);
+    if (rc == CPM_OK && ce == cudaSuccess && g) ce = cudaGraphInstantiate(&e->graph[q], g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (rc != CPM_OK || ce != cudaSuccess || !e->graph[q]) {
+      // capture failed: undo the host-side swaps of the captured step and run it directly
+      cudaGetLastError();
+      if (e->graph[q]) cudaGraphExecDestroy(e->graph[q]);
+      e->graph[q] = nullptr;
+      e->no_graph[q] = true;
+      for (cpm_sim* s : e->classes)
+        if (s->parity != q) swap_sorted(s);
+      rc = ensemble_branches(e, a1);
+    } else {
+      ce = cudaGraphLaunch(e->graph[q], e->stream);
+      if (ce != cudaSuccess)
+        return set_error(&e->err, CPM_E_CUDA, std::string("cudaGraphLaunch: ") + cudaGetErrorString(ce));
+    }
+  } else {
+    rc = ensemble_branches(e, a1);
+    e->warm[q] = true;
+  }
+  if (rc) return rc;
+  for (cpm_sim* s : e->classes) s->a = a1;
+  e->a = a1;
+  return CPM_OK;
+}
+
+int cpm_ensemble_get_state(cpm_ensemble* e, int cls, int box, float* x3, float* p3, float* acc3) {
+  if (!e || cls < 0 || cls >= (int)e->classes.size())
+    return set_error(e ? &e->err : nullptr, CPM_E_INVALID, "cpm_ensemble_get_state: bad ensemble or class");
+  cpm_sim* s = e->classes[(size_t)cls];
+  if (box < 0 || box >= s->nb) return set_error(&e->err, CPM_E_INVALID, "cpm_ensemble_get_state: bad box");
+  SIM_CU(s, cudaStreamSynchronize(e->stream));
+  const size_t nb = s->n_box, off = (size_t)box * nb;
+  const float* srcs[3] = {as<float>(s->x), as<float>(s->p), as<float>(s->acc)};
+  float* dsts[3] = {x3, p3, acc3};
+  for (int k = 0; k < 3; ++k) {
+    if (!dsts[k]) continue;
+    launch_scatter3(srcs[k], as<uint32_t>(s->id), s->n, as<float>(s->x2), s->stream);
+    SIM_CU(s, cudaMemcpyAsync(dsts[k], as<float>(s->x2) + 3 * off, 3 * nb * sizeof(float), cudaMemcpyDeviceToHost,
+                              s->stream));
+  }
+  const int rc = sim_check(s);
+  if (rc) e->err = s->err;
+  return rc;
+}
+
+int cpm_ensemble_power_spectrum(cpm_ensemble* e, int cls, int box, int n_shells, double* k_mean, double* p_mean,
+                                uint64_t* counts) {
+  if (!e || cls < 0 || cls >= (int)e->classes.size() || !k_mean || !p_mean || !counts)
+    return set_error(e ? &e->err : nullptr, CPM_E_INVALID, "cpm_ensemble_power_spectrum: bad arguments");
+  cpm_sim* s = e->classes[(size_t)cls];
+  if (box < 0 || box >= s->nb || n_shells < 1 || n_shells > PK_MAX_SHELLS)
+    return set_error(&e->err, CPM_E_INVALID, "cpm_ensemble_power_spectrum: bad box or n_shells");
+  SIM_CU(s, cudaStreamSynchronize(e->stream));
+  const int mn = s->P.mesh_n;
+  launch_deposit_fixed(as<float>(s->x), s->n, 1.0f, mn, s->h, s->shift, as<unsigned long long>(s->fx), s->stream,
+                       s->dep_ppt, batch_box(s));
+  launch_r2c3(s->plan, nullptr, as<unsigned long long>(s->fx) + mesh_cells(s) * (size_t)box, s->shift, s->mean,
+              as<float2>(s->spec), s->stream);
+  SIM_CU(s, ensure(s->pk, sizeof(PkSums)));
+  launch_pk_bin(as<float2>(s->spec), mn, n_shells, as<PkSums>(s->pk), s->stream);
+  std::vector<PkSums> host(1);
+  SIM_CU(s, cudaMemcpyAsync(host.data(), s->pk.p, sizeof(PkSums), cudaMemcpyDeviceToHost, s->stream));
+  const int rc = sim_check(s);
+  if (rc) {
+    e->err = s->err;
+    return rc;
+  }
+  pk_finish(host[0], mn, s->box, n_shells, k_mean, p_mean, counts);
+  return CPM_OK;
+}
+
+int cpm_ensemble_graphs(cpm_ensemble* e) { return e ? (e->graph[0] ? 1 : 0) + (e->graph[1] ? 1 : 0) : 0; }
+
+void* cpm_ensemble_stream(cpm_ensemble* e) { return e ? (void*)e->stream : nullptr; }
+
+const char* cpm_ensemble_last_error(const cpm_ensemble* e) { return e ? e->err.c_str() : g_last_error.c_str(); }
 
 }  // extern "C"

@@ -37,8 +37,12 @@ void release(DevBuf& b) {
 // against the node centre; the child centre is centre +- half/2, in f32. The first digit is the
 // most significant. Comparisons and additions only, so the digits are bit-exact.
 // ---------------------------------------------------------------------------------------------
+// With a batch of boxes (n_box > 0: particle i belongs to box i / n_box, boxes one after another),
+// the box index goes above the octant digits (bit `box_shift` up), so sorting keeps every box's
+// particles together and in box order.
 __global__ void k_octant_keys(const float* __restrict__ x3, size_t n, float half0, int levels,
-                              uint64_t* __restrict__ keys, uint32_t* __restrict__ vals, DevStatus* st) {
+                              uint64_t* __restrict__ keys, uint32_t* __restrict__ vals, DevStatus* st,
+                              size_t n_box, int box_shift) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float p0 = x3[3 * i], p1 = x3[3 * i + 1], p2 = x3[3 * i + 2];
@@ -54,16 +58,18 @@ __global__ void k_octant_keys(const float* __restrict__ x3, size_t n, float half
     c2 = __fadd_rn(c2, (o & 4u) ? q : -q);
     half = q;
   }
+  if (n_box) key |= (uint64_t)(i / n_box) << box_shift;
   keys[i] = key;
   if (vals) vals[i] = (uint32_t)i;
 }
 
 void launch_octant_keys(const float* x3, size_t n, float box, int levels, uint64_t* keys, uint32_t* vals,
-                        DevStatus* st, cudaStream_t s) {
+                        DevStatus* st, cudaStream_t s, size_t n_box) {
   if (n == 0) return;
   const int T = 256;
   count_launch();
-  k_octant_keys<<<(unsigned)((n + T - 1) / T), T, 0, s>>>(x3, n, box / 2.0f, levels, keys, vals, st);
+  k_octant_keys<<<(unsigned)((n + T - 1) / T), T, 0, s>>>(x3, n, box / 2.0f, levels, keys, vals, st, n_box,
+                                                          3 * levels);
 }
 
 // ---------------------------------------------------------------------------------------------

@@ -54,12 +54,16 @@ __device__ __forceinline__ uint32_t warp_lower_bound(const uint64_t* __restrict_
   return lo + (uint32_t)(__ffs(ge) - 1);  // lane hi - lo (< 32) always votes
 }
 
-__global__ void k_tree_root(uint4* link, float4* geo, uint32_t* counters, uint32_t n, float half0) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) {
-    link[0] = make_uint4(0u, n, 0u, 0u);
-    geo[0] = make_float4(half0, half0, half0, half0);
+// The root of every box (one box, or a batch of `roots` boxes of n_box particles each, sorted box by
+// box): node b covers the particles of box b, the cube [0, L]^3 of its own box.
+__global__ void k_tree_root(uint4* link, float4* geo, uint32_t* counters, uint32_t n, float half0, uint32_t roots,
+                            uint32_t n_box) {
+  for (uint32_t b = threadIdx.x; b < roots; b += blockDim.x) {
+    const uint32_t s0 = roots > 1 ? b * n_box : 0u, e0 = roots > 1 ? min(n, (b + 1) * n_box) : n;
+    link[b] = make_uint4(s0, e0, 0u, 0u);
+    geo[b] = make_float4(half0, half0, half0, half0);
   }
-  if (blockIdx.x == 0 && threadIdx.x < CNT_WORDS) counters[threadIdx.x] = threadIdx.x == 0 ? 1u : 0u;
+  if (threadIdx.x < CNT_WORDS) counters[threadIdx.x] = threadIdx.x == 0 ? roots : 0u;
 }
 
 // first index in [lo, hi) whose digit is >= o (digits non-decreasing in the range)
@@ -85,9 +89,9 @@ __device__ __forceinline__ uint32_t lower_bound_digit(const uint64_t* __restrict
 constexpr uint32_t SMALL_NODE = 256;
 constexpr uint32_t SCAN_NODE = 64;  // thread path: nodes up to this size count their digits
 
-__global__ void __launch_bounds__(BUILD_THREADS) k_tree_level(int d, const uint64_t* __restrict__ keys, uint4* link,
-                                                              float4* geo, uint32_t* counters, uint32_t capacity,
-                                                              DevStatus* st) {
+__global__ void __launch_bounds__(BUILD_THREADS) k_tree_level(int d, int levels, const uint64_t* __restrict__ keys,
+                                                              uint4* link, float4* geo, uint32_t* counters,
+                                                              uint32_t capacity, DevStatus* st) {
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   uint32_t lb = 0;
@@ -96,7 +100,7 @@ __global__ void __launch_bounds__(BUILD_THREADS) k_tree_level(int d, const uint6
   const uint32_t next_base = lb + cnt;
   // After a capacity failure the counters overshoot; never touch nodes past the arrays.
   const uint32_t level_end = min(next_base, capacity);
-  const int shift = 3 * (KEY_LEVELS - 1 - d);
+  const int shift = 3 * (levels - 1 - d);
   const uint32_t warps = gridDim.x * (BUILD_THREADS / 32);
   if (cnt > warps) {
     // Thread per node; each warp allocates the children of its 32 nodes with one atomic (an
@@ -111,7 +115,7 @@ __global__ void __launch_bounds__(BUILD_THREADS) k_tree_level(int d, const uint6
       if (valid) {
         if (c <= (uint32_t)LEAF_SIZE || d >= MAX_DEPTH) {
           link[node] = make_uint4(s, e, 0u, (uint32_t)d << 8);
-        } else if (d >= KEY_LEVELS) {
+        } else if (d >= levels) {
           atomicAdd(&counters[CNT_DEPTH_LIMIT], 1u);
           link[node] = make_uint4(s, e, 0u, (uint32_t)d << 8);
         } else {
@@ -185,7 +189,7 @@ __global__ void __launch_bounds__(BUILD_THREADS) k_tree_level(int d, const uint6
       if (lane == 0) link[node] = make_uint4(s, e, 0u, (uint32_t)d << 8);
       continue;
     }
-    if (d >= KEY_LEVELS) {
+    if (d >= levels) {
       if (lane == 0) {
         atomicAdd(&counters[CNT_DEPTH_LIMIT], 1u);
         link[node] = make_uint4(s, e, 0u, (uint32_t)d << 8);
@@ -396,7 +400,7 @@ __global__ void k_tree_quad(const uint4* __restrict__ link, const float4* __rest
 }
 
 cudaError_t tree_build(TreeNodes& t, const uint64_t* sorted_keys, const float* sorted_x3, size_t n, float box,
-                       DevStatus* st, cudaStream_t s, float quad_half_max) {
+                       DevStatus* st, cudaStream_t s, float quad_half_max, int levels, size_t n_box) {
   if (n == 0) return cudaSuccess;
   const size_t cap = 2 * n + 64;
   cudaError_t e;
@@ -415,10 +419,12 @@ cudaError_t tree_build(TreeNodes& t, const uint64_t* sorted_keys, const float* s
   float4* geo = as<float4>(t.geo);
   uint32_t* counters = as<uint32_t>(t.counters);
   count_launch();
-  k_tree_root<<<1, CNT_WORDS, 0, s>>>(link, geo, counters, (uint32_t)n, box / 2.0f);
-  for (int d = 0; d <= KEY_LEVELS; ++d) {
+  const uint32_t roots = n_box ? (uint32_t)((n + n_box - 1) / n_box) : 1u;
+  k_tree_root<<<1, 256, 0, s>>>(link, geo, counters, (uint32_t)n, box / 2.0f, roots, (uint32_t)n_box);
+  for (int d = 0; d <= levels; ++d) {
     count_launch();
-    k_tree_level<<<BUILD_BLOCKS, BUILD_THREADS, 0, s>>>(d, sorted_keys, link, geo, counters, (uint32_t)t.capacity, st);
+    k_tree_level<<<BUILD_BLOCKS, BUILD_THREADS, 0, s>>>(d, levels, sorted_keys, link, geo, counters,
+                                                        (uint32_t)t.capacity, st);
   }
 
   D3* partial = as<D3>(t.scan_tmp);

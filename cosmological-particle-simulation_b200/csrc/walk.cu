@@ -48,7 +48,6 @@
 namespace cpm {
 
 constexpr int WALK_WARPS = 4;
-constexpr int WALK_THREADS = WALK_WARPS * 32;
 constexpr int STACK_CAP = 8 * (KEY_LEVELS + 2);
 constexpr int FIT_DEG = 12;
 constexpr int FAR_PIECES_MAX = 8;
@@ -83,6 +82,7 @@ struct WalkParams {
   float inv_two_rs;
   float eps2;   // softening^2
   float k;      // Newtonian coupling
+  uint32_t n_box;  // batch of boxes: particles per box (multiple of 32); a warp starts at root i / n_box
   SFit fit;
   PairConst2 p2;
 };
@@ -438,12 +438,15 @@ __global__ void __launch_bounds__(WARPS * 32) k_tree_walk(const uint4* __restric
   // The current batch: sibling nodes first .. first + count - 1, walked by the lanes in mask.
   // Lane c < count copies node first + c into shared buffer `cur` asynchronously; the next batch
   // is copied into the other buffer while the current one is summed.
-  uint32_t b_count = 1, b_mask = group, b_first = 0;
+  // The walk starts at the root: node 0, or in a batch of boxes the root of the warp's box (nodes
+  // 0 .. boxes - 1; a box's particles fill whole warps).
+  const uint32_t root = (!LIST && w.n_box) ? (uint32_t)(t / w.n_box) : 0u;
+  uint32_t b_count = 1, b_mask = group, b_first = root;
   int cur = 0;
   if (lane == 0) {
-    cp_async16(&sh.geo[0][0], geo);
-    cp_async16(&sh.mass[0][0], mass);
-    cp_async16(&sh.link[0][0], link);
+    cp_async16(&sh.geo[0][0], geo + root);
+    cp_async16(&sh.mass[0][0], mass + root);
+    cp_async16(&sh.link[0][0], link + root);
   }
   int sp = 0;
   for (;;) {
@@ -731,6 +734,7 @@ void launch_tree_walk(const TreeNodes& t, const float* sorted_x3, size_t n, floa
   w.inv_two_rs = (float)(1.0 / (2.0 * (double)split.r_split));
   w.eps2 = split.softening * split.softening;
   w.k = k;
+  w.n_box = t.n_box;
   w.fit = fc.fit;
   auto dup = [](float v) { return make_float2(v, v); };
   w.p2.tiny = dup(1e-30f);

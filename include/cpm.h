@@ -343,11 +343,50 @@ int cpm_sim_autotune_report(cpm_sim* sim, int* fft_radix, int* deposit_tile, int
  * force evaluation uses them. Deposit tile and walk group do not change any result bit; the radix
  * plan changes FFT rounding only. */
 int cpm_sim_set_tuning(cpm_sim* sim, int fft_radix, int deposit_tile, int walk_warps);
+/* The last tree build's deepest split level, and the number of nodes with more than 8 particles
+ * kept as leaves because their particles share every key digit (21 digits; 19 in an ensemble's
+ * batch). The reference splits such nodes down to MAX_DEPTH = 40 (tree.rs:13, :211), so a non-zero
+ * count marks states where the GPU's tree departs from the reference's. */
+int cpm_sim_tree_depth(cpm_sim* sim, uint32_t* max_depth, uint64_t* key_depth_leaves);
 /* Particles the last step walked the tree for (all of them without a net). */
 int cpm_sim_learned_walked(cpm_sim* sim, uint64_t* walked);
 /* The CUDA stream the simulation launches on (cudaStream_t), for callers that time with events. */
 void* cpm_sim_stream(cpm_sim* sim);
 int cpm_sim_destroy(cpm_sim* sim);
+
+/* ------------------------------------------------------------------ ensembles of realisations */
+/* No counterpart in the reference, which runs one realisation per run (runner.rs:228-260). An
+ * ensemble holds many independent realisations of uneven sizes, grouped in classes of equal size.
+ * Every box of a class shares one launch per phase (keys with the box index above the octant digits,
+ * one sort, one deposit into the boxes' meshes, batched FFT passes, one gather, one tree build with a
+ * root per box, one walk), and one ensemble step is one CUDA graph in which the classes run as
+ * parallel branches. Each box is a Simulation of the reference's step (integrator.rs:174-186) with
+ * the class's mesh and split, Zel'dovich ICs (ics.rs:119-182, as cpm_sim_create_zeldovich) from seed
+ * first_seed + b, and the common box size, cosmology and schedule; steps are autotuned per class. */
+typedef struct cpm_ensemble cpm_ensemble;
+typedef struct {
+  int n_side;           /* particles per side of every box of the class; n_side^3 a multiple of 2048 */
+  int mesh_n;           /* mesh cells per side (a supported FFT length up to 512) */
+  int n_boxes;          /* realisations of the class, 1..64 */
+  uint64_t first_seed;  /* box b uses seed first_seed + b */
+  cpm_force_split split;
+} cpm_ensemble_class;
+/* 1..16 classes; flags: CPM_SIM_FIXED_POINT, CPM_SIM_DECONVOLVE, CPM_SIM_NO_GRAPH, CPM_SIM_NO_AUTOTUNE. */
+int cpm_ensemble_create(const cpm_cosmology* cosmo, float box_size, float n_s, float sigma8, float a0, int n_classes,
+                        const cpm_ensemble_class* classes, uint32_t flags, cpm_ensemble** out);
+/* One KDK step of every realisation to a1 (the third and later steps replay a captured graph). */
+int cpm_ensemble_step_to(cpm_ensemble* ens, float a1);
+/* Positions, momenta and accelerations (any may be NULL) of box `box` of class `cls`, in the box's
+ * lattice order (AoS [n_side^3][3]). Synchronous. */
+int cpm_ensemble_get_state(cpm_ensemble* ens, int cls, int box, float* x3, float* p3, float* acc3);
+/* cpm_sim_power_spectrum of one box. */
+int cpm_ensemble_power_spectrum(cpm_ensemble* ens, int cls, int box, int n_shells, double* k_mean, double* p_mean,
+                                uint64_t* counts);
+/* Captured step graphs (0, 1 or 2) and the stream the steps run on (cudaStream_t). */
+int cpm_ensemble_graphs(cpm_ensemble* ens);
+void* cpm_ensemble_stream(cpm_ensemble* ens);
+const char* cpm_ensemble_last_error(const cpm_ensemble* ens);
+int cpm_ensemble_destroy(cpm_ensemble* ens);
 
 #ifdef __cplusplus
 }

