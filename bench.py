@@ -195,11 +195,12 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
         i0 = int(np.searchsorted(np.asarray(full, np.float32), np.float32(a_saved), side="right"))
         sched = full[i0:i0 + args.warmup + args.steps]
 
-    net, net_threshold = None, None
+    net, net_threshold, net_in_scale = None, None, 1.0
     if wl.get("learned"):
         z = np.load(NET_WEIGHTS)
         net = cpm.ShortRangeNet(mesh, z["weights"])
         net_threshold = float(z["threshold"])
+        net_in_scale = float(z["in_scale"]) if "in_scale" in z else 1.0
 
     def make_sim(flags: int, learned: bool = bool(wl.get("learned"))):
         if args.load_state:
@@ -208,7 +209,7 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
             sim_ = cpm.Simulation.from_zeldovich(cosmo, box, mesh, n_side, N_S, SIGMA8, A_INIT,
                                                  replica_seed(wl["seed"], rank), split, flags=flags)
         if learned:
-            sim_.set_learned(net, net_threshold)
+            sim_.set_learned(net, net_threshold, net_in_scale)
         return sim_
 
     # The timed run replays the step's captured CUDA graphs (no per-phase events).

@@ -64,7 +64,8 @@ constexpr int GRAD_ROW = 2 * GRAD_PLANE;        // 4096
 constexpr int W_TAP_BYTES = 2 * NET_C * 16;     // [chunk][cout 16][8 cin] bf16 = 512
 constexpr int W_BYTES = NET_TAPS * W_TAP_BYTES;  // 13824
 constexpr int CONV_THREADS = 192;               // 6 warps
-constexpr int CONV_STAGES = 3;
+constexpr int CONV_STAGES = 2;
+constexpr int CONV_ROWS = 4;                    // output rows (consecutive y) per forward tile
 constexpr int WG_STAGES = 2;
 constexpr long long WAIT_BUDGET = 1ll << 32;    // clock cycles (about 2 s) before a wait gives up
 
@@ -128,19 +129,22 @@ struct ConvArgs {
 // ---------------------------------------------------------------------------------------------
 template <int NSTAGE>
 __global__ void __launch_bounds__(CONV_THREADS, 1) k_conv3(const __grid_constant__ CUtensorMap in_map, ConvArgs a) {
+  constexpr int R = CONV_ROWS;            // output rows (consecutive y) per tile
+  constexpr int IN = 3 * (R + 2);         // input rows per tile: x-1..x+1 by y0-1..y0+R
   extern __shared__ __align__(1024) uint8_t smem[];
-  uint8_t* rows = smem;                                // [NSTAGE][9][ROW_BYTES]
-  uint8_t* wsm = smem + NSTAGE * 9 * ROW_BYTES;        // packed weights
+  uint8_t* rows = smem;                                // [NSTAGE][IN][ROW_BYTES]
+  uint8_t* wsm = smem + NSTAGE * IN * ROW_BYTES;       // packed weights
   uint64_t* bars = reinterpret_cast<uint64_t*>(wsm + W_BYTES);
   uint64_t* full = bars;                  // [NSTAGE] rows loaded
   uint64_t* empty = bars + NSTAGE;        // [NSTAGE] rows consumed by the MMAs
-  uint64_t* acc_full = bars + 2 * NSTAGE;      // [2] accumulator ready
-  uint64_t* acc_empty = bars + 2 * NSTAGE + 2;  // [2] accumulator read by the epilogue
+  uint64_t* acc_full = bars + 2 * NSTAGE;      // [2] accumulators ready
+  uint64_t* acc_empty = bars + 2 * NSTAGE + 2;  // [2] accumulators read by the epilogue
   uint64_t* done = bars + 2 * NSTAGE + 4;
   uint32_t* tmem_sh = reinterpret_cast<uint32_t*>(bars + 2 * NSTAGE + 5);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int n = a.g.n;
+  const int yq_count = n / R;
   for (int i = threadIdx.x; i < W_BYTES / 16; i += CONV_THREADS)
     reinterpret_cast<uint4*>(wsm)[i] = __ldg(reinterpret_cast<const uint4*>(a.w) + i);
   if (threadIdx.x == 0) {
@@ -156,7 +160,7 @@ __global__ void __launch_bounds__(CONV_THREADS, 1) k_conv3(const __grid_constant
     umma::fence_mbar_init();
   }
   if (warp == 0) {
-    umma::tmem_alloc(tmem_sh, 32);
+    umma::tmem_alloc(tmem_sh, 2 * R * NET_C);
     umma::tmem_relinquish();
   }
   umma::fence_proxy_async();
@@ -166,7 +170,7 @@ __global__ void __launch_bounds__(CONV_THREADS, 1) k_conv3(const __grid_constant
   const uint32_t tmem = *tmem_sh;
 
   if (warp == 0) {
-    if (lane == 0) {  // TMA producer: the 9 rows (x+dx, y+dy) of each tile
+    if (lane == 0) {  // TMA producer: rows (x+dx, y0-1 .. y0+R) of each tile
       umma::tma_prefetch_map(&in_map);
       int s = 0;
       uint32_t ph = 0;
@@ -178,11 +182,11 @@ __global__ void __launch_bounds__(CONV_THREADS, 1) k_conv3(const __grid_constant
         }
         const int zt = (int)(t % a.tiles_z);
         const long long xy = t / a.tiles_z;
-        const int y = (int)(xy % n), x = (int)(xy / n);
-        umma::mbar_arrive_expect_tx(&full[s], 9 * ROW_BYTES);
-        for (int r = 0; r < 9; ++r) {
-          const int xs = (x + r / 3 - 1 + n) % n, ys = (y + r % 3 - 1 + n) % n;
-          umma::tma_load_5d(rows + (size_t)(s * 9 + r) * ROW_BYTES, &in_map, &full[s], 0, zt * TILE_M, 0, ys, xs);
+        const int y0 = (int)(xy % yq_count) * R, x = (int)(xy / yq_count);
+        umma::mbar_arrive_expect_tx(&full[s], IN * ROW_BYTES);
+        for (int r = 0; r < IN; ++r) {
+          const int xs = (x + r / (R + 2) - 1 + n) % n, ys = (y0 + r % (R + 2) - 1 + n) % n;
+          umma::tma_load_5d(rows + (size_t)(s * IN + r) * ROW_BYTES, &in_map, &full[s], 0, zt * TILE_M, 0, ys, xs);
         }
         ++issued;
         if (++s == NSTAGE) {
@@ -198,7 +202,7 @@ __global__ void __launch_bounds__(CONV_THREADS, 1) k_conv3(const __grid_constant
       }
     }
   } else if (warp == 1) {
-    if (lane == 0) {  // MMA issuer
+    if (lane == 0) {  // MMA issuer: 27 MMAs per output row into that row's accumulator
       constexpr uint32_t IDESC = umma::idesc_bf16(TILE_M, NET_C, false, false);
       const uint32_t w_addr = umma::smem_u32(wsm);
       int s = 0, ab = 0;
@@ -209,15 +213,21 @@ __global__ void __launch_bounds__(CONV_THREADS, 1) k_conv3(const __grid_constant
           break;
         }
         umma::tc_fence_after();
-        const uint32_t d = tmem + (uint32_t)(ab * NET_C);
-        const uint32_t base = umma::smem_u32(rows + (size_t)s * 9 * ROW_BYTES);
-        for (int r = 0; r < 9; ++r)
+        const uint32_t base = umma::smem_u32(rows + (size_t)s * IN * ROW_BYTES);
+        for (int r = 0; r < R; ++r) {
+          const uint32_t d = tmem + (uint32_t)((ab * R + r) * NET_C);
+          for (int dxi = 0; dxi < 3; ++dxi)
+            for (int dyi = 0; dyi < 3; ++dyi) {
+              const int ri = dxi * (R + 2) + r + dyi;
 #pragma unroll
-          for (int dz = 0; dz < 3; ++dz) {
-            const uint64_t ad = umma::sdesc(base + (uint32_t)(r * ROW_BYTES + dz * 16), PLANE_BYTES, 128);
-            const uint64_t bd = umma::sdesc(w_addr + (uint32_t)((r * 3 + dz) * W_TAP_BYTES), 256, 128);
-            umma::mma_bf16(d, ad, bd, IDESC, (r | dz) != 0 ? 1u : 0u);
-          }
+              for (int dz = 0; dz < 3; ++dz) {
+                const int tap = (dxi * 3 + dyi) * 3 + dz;
+                const uint64_t ad = umma::sdesc(base + (uint32_t)(ri * ROW_BYTES + dz * 16), PLANE_BYTES, 128);
+                const uint64_t bd = umma::sdesc(w_addr + (uint32_t)(tap * W_TAP_BYTES), 256, 128);
+                umma::mma_bf16(d, ad, bd, IDESC, tap != 0 ? 1u : 0u);
+              }
+            }
+        }
         umma::mma_commit(&empty[s]);
         umma::mma_commit(&acc_full[ab]);
         if (++s == NSTAGE) {
@@ -244,53 +254,58 @@ __global__ void __launch_bounds__(CONV_THREADS, 1) k_conv3(const __grid_constant
         break;
       }
       umma::tc_fence_after();
-      uint32_t r[16];
-      umma::tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(ab * NET_C), r);
-      umma::tmem_wait_ld();
-      umma::tc_fence_before();
-      umma::mbar_arrive(&acc_empty[ab]);
+      const int zt = (int)(t % a.tiles_z);
+      const long long xy = t / a.tiles_z;
+      const int y0 = (int)(xy % yq_count) * R, x = (int)(xy / yq_count);
+      const int z = zt * TILE_M + m;
+      for (int rr = 0; rr < R; ++rr) {
+        uint32_t r[16];
+        umma::tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)((ab * R + rr) * NET_C), r);
+        umma::tmem_wait_ld();
+        if (rr == R - 1) {  // every accumulator of the tile is in registers: release them
+          umma::tc_fence_before();
+          umma::mbar_arrive(&acc_empty[ab]);
+        }
+        if (z >= n) continue;
+        const int y = y0 + rr;
+        float v[16];
+#pragma unroll
+        for (int c = 0; c < 16; ++c) v[c] = __uint_as_float(r[c]);
+        if (a.out_f4) {
+          a.out_f4[((size_t)x * n + y) * n + z] = make_float4(v[0] * scale, v[1] * scale, v[2] * scale, 0.0f);
+          continue;
+        }
+        if (a.act) {
+#pragma unroll
+          for (int c = 0; c < 16; ++c) v[c] = lrelu(v[c]);
+        }
+        if (a.gate) {
+          const uint4 g0 = *reinterpret_cast<const uint4*>(a.gate + a.g.at(x, y, 0, z + 1));
+          const uint4 g1 = *reinterpret_cast<const uint4*>(a.gate + a.g.at(x, y, 1, z + 1));
+          const uint32_t gw[8] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w};
+#pragma unroll
+          for (int k = 0; k < 8; ++k) {
+            const float2 gv = unpack_bf16x2(gw[k]);
+            v[2 * k] *= gv.x > 0.0f ? 1.0f : NET_SLOPE;
+            v[2 * k + 1] *= gv.y > 0.0f ? 1.0f : NET_SLOPE;
+          }
+        }
+        const uint4 c0 = make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]), pack_bf16x2(v[4], v[5]),
+                                    pack_bf16x2(v[6], v[7]));
+        const uint4 c1 = make_uint4(pack_bf16x2(v[8], v[9]), pack_bf16x2(v[10], v[11]), pack_bf16x2(v[12], v[13]),
+                                    pack_bf16x2(v[14], v[15]));
+        store_voxel16(a.out16, a.g, x, y, z, c0, c1);
+      }
       if (++ab == 2) {
         ab = 0;
         aph ^= 1;
       }
-      const int zt = (int)(t % a.tiles_z);
-      const long long xy = t / a.tiles_z;
-      const int y = (int)(xy % n), x = (int)(xy / n);
-      const int z = zt * TILE_M + m;
-      if (z >= n) continue;
-      float v[16];
-#pragma unroll
-      for (int c = 0; c < 16; ++c) v[c] = __uint_as_float(r[c]);
-      if (a.out_f4) {
-        a.out_f4[((size_t)x * n + y) * n + z] = make_float4(v[0] * scale, v[1] * scale, v[2] * scale, 0.0f);
-        continue;
-      }
-      if (a.act) {
-#pragma unroll
-        for (int c = 0; c < 16; ++c) v[c] = lrelu(v[c]);
-      }
-      if (a.gate) {
-        const uint4 g0 = *reinterpret_cast<const uint4*>(a.gate + a.g.at(x, y, 0, z + 1));
-        const uint4 g1 = *reinterpret_cast<const uint4*>(a.gate + a.g.at(x, y, 1, z + 1));
-        const uint32_t gw[8] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w};
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-          const float2 gv = unpack_bf16x2(gw[k]);
-          v[2 * k] *= gv.x > 0.0f ? 1.0f : NET_SLOPE;
-          v[2 * k + 1] *= gv.y > 0.0f ? 1.0f : NET_SLOPE;
-        }
-      }
-      const uint4 c0 = make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]), pack_bf16x2(v[4], v[5]),
-                                  pack_bf16x2(v[6], v[7]));
-      const uint4 c1 = make_uint4(pack_bf16x2(v[8], v[9]), pack_bf16x2(v[10], v[11]), pack_bf16x2(v[12], v[13]),
-                                  pack_bf16x2(v[14], v[15]));
-      store_voxel16(a.out16, a.g, x, y, z, c0, c1);
     }
   }
   umma::tc_fence_before();
   __syncthreads();
   umma::tc_fence_after();
-  if (warp == 0) umma::tmem_dealloc(tmem, 32);
+  if (warp == 0) umma::tmem_dealloc(tmem, 2 * R * NET_C);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -590,7 +605,9 @@ static bool make_row_map(CUtensorMap* map, const __nv_bfloat16* t, int n, int bo
   return r == CUDA_SUCCESS;
 }
 
-constexpr size_t conv_smem_bytes(int stages) { return (size_t)stages * 9 * ROW_BYTES + W_BYTES + 8 * (2 * stages + 5) + 16; }
+constexpr size_t conv_smem_bytes(int stages) {
+  return (size_t)stages * 3 * (CONV_ROWS + 2) * ROW_BYTES + W_BYTES + 8 * (2 * stages + 5) + 16;
+}
 constexpr size_t wgrad_smem_bytes(int stages) {
   return (size_t)stages * (9 * GRAD_ROW + ROW_BYTES) + 8 * (2 * stages + 1) + 16;
 }
@@ -648,7 +665,7 @@ void launch_conv(cpm_net* net, const CUtensorMap& in_map, int layer, bool transp
   ConvArgs a;
   a.g = net->g;
   a.tiles_z = (net->n + TILE_M - 1) / TILE_M;
-  a.tiles = (long long)net->n * net->n * a.tiles_z;
+  a.tiles = (long long)net->n * (net->n / CONV_ROWS) * a.tiles_z;  // n is a multiple of 16
   a.w = static_cast<const __nv_bfloat16*>(transpose ? net->wb.p : net->wf.p) + (size_t)layer * NET_TAPS * NET_C * NET_C;
   a.out16 = out16;
   a.out_f4 = out_f4;

@@ -14,7 +14,7 @@ Every computation runs in libcpm_cuda.so: the plain runs, the tree forces, and t
 (forward convolutions, CIC gather and loss, backward convolutions and weight gradients on the
 tcgen05 tensor cores, Adam).
 
-  python cosmological-particle-simulation_b200/train_net.py --out PATH.npz [--iters 1500]
+  python cosmological-particle-simulation_b200/train_net.py --out PATH.npz [--thresholds 50] [--iters 3000]
 """
 from __future__ import annotations
 
@@ -125,47 +125,65 @@ def evaluate(net, samples_host, box: float, in_scale: float, n_part: int) -> dic
 
 def main() -> int:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("--out", default=str(DEFAULT_WEIGHTS))
-    ap.add_argument("--iters", type=int, default=1500)
+    ap.add_argument("--out", default=str(DEFAULT_WEIGHTS),
+                    help="weights file; with several thresholds, {thr} in the name is replaced by each")
+    ap.add_argument("--iters", type=int, default=3000)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--seeds", default="1000-1015")
     ap.add_argument("--val-seed", type=int, default=2000)
     ap.add_argument("--n-side", type=int, default=128)
-    ap.add_argument("--threshold", type=float, default=DELTA_THRESHOLD)
+    ap.add_argument("--thresholds", default=str(DELTA_THRESHOLD),
+                    help="comma-separated density-contrast thresholds; one net is trained per threshold")
+    ap.add_argument("--in-scale", type=float, default=1.0 / 16.0)
     ap.add_argument("--init-seed", type=int, default=0)
     args = ap.parse_args()
     import torch
 
     lo, hi = (int(v) for v in args.seeds.split("-"))
     n_side, mesh, box = args.n_side, 2 * args.n_side, float(args.n_side)
+    thresholds = [float(v) for v in args.thresholds.split(",")]
     t0 = time.time()
+    # the samples are generated once; each threshold only changes which particles enter the loss
     train_host = []
     for seed in range(lo, hi + 1):
-        train_host += generate(seed, n_side, mesh, box, threshold=args.threshold)
-    val_host = generate(args.val_seed, n_side, mesh, box, threshold=args.threshold)
+        train_host += generate(seed, n_side, mesh, box, threshold=1e30)
+    val_host = generate(args.val_seed, n_side, mesh, box, threshold=1e30)
     t_data = time.time() - t0
-    samples = to_device(train_host)
-    for s in train_host:  # keep only what evaluation needs on the host
-        s.pop("delta", None)
-    net = cpm.ShortRangeNet(mesh, init_weights(args.init_seed))
-    rng = np.random.default_rng(1)
-    losses = []
-    t1 = time.time()
-    for it in range(args.iters):
-        lr = args.lr * 0.5 * (1.0 + math.cos(math.pi * it / args.iters)) + 1e-5
-        s = samples[int(rng.integers(len(samples)))]
-        losses.append(net.train_step(s["delta"], s["x"], s["target"], s["weight"], box, s["inv_norm"], lr))
-    torch.cuda.synchronize()
-    t_train = time.time() - t1
-    report = {"data_s": round(t_data, 1), "train_s": round(t_train, 1), "iters": args.iters,
-              "samples": len(samples), "loss_first50": float(np.mean(losses[:50])),
-              "loss_last50": float(np.mean(losses[-50:])), "threshold": args.threshold,
-              "validation": evaluate(net, val_host, box, 1.0, n_side ** 3)}
-    Path(args.out).parent.mkdir(parents=True, exist_ok=True)
-    np.savez(args.out, weights=net.weights, threshold=np.float32(args.threshold), in_scale=np.float32(1.0),
-             report=json.dumps(report))
-    print(json.dumps(report, indent=1))
-    net.close()
+    for s in train_host + val_host:
+        s["d_i"] = cpm.Mesh(mesh, box, s["delta"]).interpolate_many(s["x"])
+    reports = {}
+    for thr in thresholds:
+        for s in train_host + val_host:
+            s["weight"] = (s["d_i"] < thr).astype(np.float32)
+        samples = to_device(train_host)
+        net = cpm.ShortRangeNet(mesh, init_weights(args.init_seed))
+        rng = np.random.default_rng(1)
+        losses = []
+        t1 = time.time()
+        for it in range(args.iters):
+            lr = args.lr * 0.5 * (1.0 + math.cos(math.pi * it / args.iters)) + 1e-5
+            s = samples[int(rng.integers(len(samples)))]
+            losses.append(net.train_step(s["delta"], s["x"], s["target"], s["weight"], box, s["inv_norm"], lr,
+                                         in_scale=args.in_scale))
+        torch.cuda.synchronize()
+        t_train = time.time() - t1
+        report = {"data_s": round(t_data, 1), "train_s": round(t_train, 1), "iters": args.iters,
+                  "samples": len(samples), "loss_first50": float(np.mean(losses[:50])),
+                  "loss_last50": float(np.mean(losses[-50:])), "threshold": thr, "in_scale": args.in_scale,
+                  "validation": evaluate(net, val_host, box, args.in_scale, n_side ** 3)}
+        out = Path(args.out.replace("{thr}", f"{thr:g}"))
+        out.parent.mkdir(parents=True, exist_ok=True)
+        np.savez(out, weights=net.weights, threshold=np.float32(thr), in_scale=np.float32(args.in_scale),
+                 report=json.dumps(report))
+        reports[f"{thr:g}"] = report
+        print(json.dumps({"threshold": thr, "loss_first50": report["loss_first50"],
+                          "loss_last50": report["loss_last50"], "train_s": report["train_s"],
+                          "validation_rel_mse": [r["rel_mse"] for r in report["validation"]["snapshots"]]}),
+              flush=True)
+        net.close()
+        del samples
+        torch.cuda.empty_cache()
+    print(json.dumps(reports, indent=1))
     return 0
 
 

@@ -5,8 +5,9 @@ that replay the ensemble's captured graph.
 A batch's particles share one sort (the box index above 19 octant digits instead of 21), one tree
 (a root per box) and FP64 prefix sums over the whole batch for the centres of mass, whose last f32
 bit can round differently from a single box's; deposit, FFT, gather and kick/drift are per box the
-same arithmetic. So positions must agree to 1e-5 L and forces to 1e-5 relative RMS (bit-equal in
-practice), and the boxes' P(k) to 1e-4."""
+same arithmetic. So the initial conditions must be equal, the initial forces within 1e-6 relative RMS; after 40 steps
+(the last ones replayed from the ensemble's graph, where the chaotic growth of last-bit differences
+shows) positions within 1e-5 L, forces within 1e-4 relative RMS and the boxes' P(k) within 1e-4."""
 import numpy as np
 import pytest
 
@@ -32,6 +33,14 @@ def test_every_box_of_a_mixed_ensemble_equals_its_single_run(cpm):
         split = cpm.ForceSplit.with_(box, mesh, n_side, 1.0 / 30.0, 0.5)
         classes.append((n_side, mesh, boxes, seed, split))
     ens = cpm.Ensemble(cc, box, 0.96, 0.8, 0.02, classes)
+    # the forces of the initial conditions: every box against its own single-box simulation
+    for ci, (n_side, mesh, boxes, seed, split) in enumerate(classes):
+        for b in range(boxes):
+            single = cpm.Simulation.from_zeldovich(cc, box, mesh, n_side, 0.96, 0.8, 0.02, seed + b, split)
+            s, e = single.state(), ens.state(ci, b)
+            assert np.array_equal(e["x"], s["x"]) and np.array_equal(e["p"], s["p"]), (ci, b)
+            assert rel_rms(e["acc"], s["acc"]) < 1e-6, (ci, b)
+            single.close()
     sched = cpm.ln_a_schedule(0.02, 1.0, 64)[:40]
     for a1 in sched:
         ens.step_to(a1)
@@ -43,7 +52,7 @@ def test_every_box_of_a_mixed_ensemble_equals_its_single_run(cpm):
                 single.step_to(a1)
             s, e = single.state(), ens.state(ci, b)
             assert periodic_max_diff(e["x"], s["x"], box) < 1e-5 * box, (ci, b)
-            assert rel_rms(e["acc"], s["acc"]) < 1e-5, (ci, b)
+            assert rel_rms(e["acc"], s["acc"]) < 1e-4, (ci, b)
             _, p_s, c_s = single.power_spectrum(mesh // 4)
             _, p_e, c_e = ens.power_spectrum(ci, b, mesh // 4)
             np.testing.assert_array_equal(c_s, c_e)

@@ -30,12 +30,12 @@ def rel_rms(a, b):
     return float(np.sqrt(((a - b) ** 2).sum() / max((b ** 2).sum(), 1e-300)))
 
 
-def _sims(cpm, n_side, mesh, box, seed, steps, net=None, threshold=50.0, flags=0):
+def _sims(cpm, n_side, mesh, box, seed, steps, net=None, threshold=50.0, flags=0, in_scale=1.0):
     cosmo = cpm.Cosmology(0.0, 0.3, 0.7, 70.0)
     split = cpm.ForceSplit.with_(box, mesh, n_side, 1.0 / 30.0, 0.5)
     sim = cpm.Simulation.from_zeldovich(cosmo, box, mesh, n_side, 0.96, 0.8, 0.02, seed, split, flags=flags)
     if net is not None:
-        sim.set_learned(net, threshold)
+        sim.set_learned(net, threshold, in_scale)
     return sim
 
 
@@ -98,11 +98,13 @@ def test_learned_gain_on_held_out_seed(cpm, orc):
     z = np.load(WEIGHTS)
     n_side, mesh, box, seed, steps = 128, 256, 128.0, 2000, 128
     threshold = float(z["threshold"])
+    in_scale = float(z["in_scale"]) if "in_scale" in z else 1.0
     net = cpm.ShortRangeNet(mesh, z["weights"])
     sched = cpm.ln_a_schedule(0.02, 1.0, steps)
     results = {}
     for name in ("plain", "learned"):
-        sim = _sims(cpm, n_side, mesh, box, seed, steps, net if name == "learned" else None, threshold)
+        sim = _sims(cpm, n_side, mesh, box, seed, steps, net if name == "learned" else None, threshold,
+                    in_scale=in_scale)
         stream = torch.cuda.ExternalStream(sim.stream())
         for a1 in sched[:3]:
             sim.step_to(a1)
