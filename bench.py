@@ -42,6 +42,9 @@ WORKLOADS = {
     "treepm-32": dict(n_side=32, mesh=64, box=64.0, seed=42, steps_total=64),
     # profiling case: same physics at 128^3 particles (a few GB on the device).
     "treepm-128": dict(n_side=128, mesh=256, box=128.0, seed=7, steps_total=128),
+    # profiling case for the PM traffic: the headline's 1/8 particle per cell at 192^3 / 384^3 (meshes
+    # and positions larger than L2, about 3 GB on the device); per-step bytes scale by (256/192)^3.
+    "treepm-192": dict(n_side=192, mesh=384, box=192.0, seed=7, steps_total=128),
     # profiling case for the PM kernels: full-size 512^3 mesh, 128^3 particles.
     "pm512-128": dict(n_side=128, mesh=512, box=128.0, seed=7, steps_total=128),
     # the headline workload with the learned short-range force (trained weights, tree walk kept for
@@ -203,6 +206,8 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
         net_in_scale = float(z["in_scale"]) if "in_scale" in z else 1.0
 
     def make_sim(flags: int, learned: bool = bool(wl.get("learned"))):
+        if args.no_autotune:
+            flags |= cpm._native.SIM_NO_AUTOTUNE
         if args.load_state:
             sim_ = cpm.Simulation(cosmo, box, mesh, st0["x"], st0["p"], a_saved, split, flags=flags)
         else:
@@ -326,7 +331,8 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
         "roofline": {"bound": "hbm", "kernels": "PM: deposit + FFT-Poisson + gather",
                      "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
                      "peak_kind": peak_kind, "algorithmic_bytes_per_step": pm_b,
-                     "traffic": traffic.get("pm_bytes_per_step") if traffic else None},
+                     "traffic": traffic.get("pm_bytes_per_step")
+                     if traffic and traffic.get("workload") == args.workload else None},
         "phase_ms": {k: round(float(v), 4) for k, v in zip(phase_names, phases)} if nsteps else None,
         "phase_steps": nsteps,
         "phase_note": "per-phase CUDA events on a second run of the same window (uncaptured steps)",
@@ -502,6 +508,9 @@ def main() -> int:
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-phases", action="store_true", help="skip the second, per-phase timed run")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="default launch parameters (FFT radix 8, deposit tile 1024, walk group 4 warps), no timing "
+                         "of alternatives: a fixed launch sequence for profiling")
     ap.add_argument("--cpu-walk-fraction", type=float, default=1.0 / 64.0)
     ap.add_argument("--ref-budget-s", type=float, default=120.0)
     ap.add_argument("--save-state", default="", help="write the state file (cpm_sim_save) after the timed steps")

@@ -431,9 +431,9 @@ class Simulation:
     def tuning(self) -> dict:
         """The autotuner's choices and the measured ms of every candidate (cpm_sim_autotune_report)."""
         r, t, wp = C.c_int(), C.c_int(), C.c_int()
-        ms = np.zeros(8, np.float32)
+        ms = np.zeros(9, np.float32)
         check(nat.lib().cpm_sim_autotune_report(self.h, C.byref(r), C.byref(t), C.byref(wp), ptr(ms)), sim=True)
-        names = ["fft_radix8", "fft_radix4", "deposit_tile512", "deposit_tile1024", "deposit_tile2048",
+        names = ["fft_radix8", "fft_radix4", "fft_warp", "deposit_tile512", "deposit_tile1024", "deposit_tile2048",
                  "walk_warps2", "walk_warps4", "walk_warps8"]
         return {"fft_radix": r.value, "deposit_tile": t.value, "walk_warps": wp.value,
                 "ms": {k: round(float(v), 4) for k, v in zip(names, ms)}}

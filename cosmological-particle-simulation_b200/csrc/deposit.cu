@@ -15,9 +15,13 @@
 namespace cpm {
 
 constexpr int DEP_THREADS = 256;
-constexpr int DEP_SMEM_CELLS = 12288;               // 96 KB of u64 per CTA
 // Particles per thread PPT (tile of 256 * PPT consecutive sorted particles per CTA): 2, 4 or 8,
-// picked per workload by the autotuner (4 by default).
+// picked per workload by the autotuner (4 by default). The shared-memory box grows with the tile:
+// 48 KB (four CTAs per SM), 96 KB (two) or 192 KB (one) of u64 cells.
+template <int PPT>
+__host__ __device__ constexpr int dep_smem_cells() {
+  return PPT <= 2 ? 6144 : (PPT <= 4 ? 12288 : 24576);
+}
 
 int fixed_point_shift(double total_mass) {
   // Largest k with total_mass * 2^k < 2^62, clamped so a unit weight keeps >= 24 fractional bits.
@@ -91,7 +95,7 @@ __global__ void __launch_bounds__(DEP_THREADS) k_deposit_fixed(const float* __re
   const long long cells = (long long)e0 * e1 * e2;
   if (bb[0] > bb[3]) return;  // empty chunk
 
-  if (one_box && cells <= DEP_SMEM_CELLS && e0 > 0 && e1 > 0 && e2 > 0) {
+  if (one_box && cells <= dep_smem_cells<DEP_PPT>() && e0 > 0 && e1 > 0 && e2 > 0) {
     for (int t = threadIdx.x; t < (int)cells; t += DEP_THREADS) sm_cells[t] = 0ull;
     __syncthreads();
 #pragma unroll
@@ -106,10 +110,15 @@ __global__ void __launch_bounds__(DEP_THREADS) k_deposit_fixed(const float* __re
       }
     }
     __syncthreads();
+    // floor(t / e) as floor((t + 1/2) * fl(1/e)): (t + 1/2) / e lies at least 1/(2e) from an
+    // integer, and for t < 2^15 the two f32 roundings move it by less than 2^-7 / e.
+    const float inv_e2 = 1.0f / (float)e2, inv_e1 = 1.0f / (float)e1;
     for (int t = threadIdx.x; t < (int)cells; t += DEP_THREADS) {
       const unsigned long long v = sm_cells[t];
       if (v == 0ull) continue;
-      const int lz = t % e2, ly = (t / e2) % e1, lx = t / (e1 * e2);
+      const int row = (int)(((float)t + 0.5f) * inv_e2);
+      const int lx = (int)(((float)row + 0.5f) * inv_e1);
+      const int lz = t - row * e2, ly = row - lx * e1;
       const size_t gx = (size_t)wrap_index(bb[0] + lx, mesh_n);
       const size_t gy = (size_t)wrap_index(bb[1] + ly, mesh_n);
       const size_t gz = (size_t)wrap_index(bb[2] + lz, mesh_n);
@@ -135,13 +144,12 @@ template <int PPT>
 static void deposit_ppt(const float* x3, size_t n, float mass, int mesh_n, float h, float scale,
                         unsigned long long* mesh_fx, cudaStream_t s, size_t n_box) {
   // Per device (a cheap host call, so made on every launch): a failure shows up as the launch's error.
-  cudaFuncSetAttribute(k_deposit_fixed<PPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       DEP_SMEM_CELLS * (int)sizeof(unsigned long long));
+  constexpr int smem = dep_smem_cells<PPT>() * (int)sizeof(unsigned long long);
+  cudaFuncSetAttribute(k_deposit_fixed<PPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   constexpr size_t chunk = (size_t)DEP_THREADS * PPT;
   const unsigned blocks = (unsigned)((n + chunk - 1) / chunk);
   count_launch();
-  k_deposit_fixed<PPT><<<blocks, DEP_THREADS, DEP_SMEM_CELLS * sizeof(unsigned long long), s>>>(x3, n, mass, mesh_n, h,
-                                                                                              scale, mesh_fx, n_box);
+  k_deposit_fixed<PPT><<<blocks, DEP_THREADS, smem, s>>>(x3, n, mass, mesh_n, h, scale, mesh_fx, n_box);
 }
 
 void launch_deposit_fixed(const float* x3, size_t n, float mass, int mesh_n, float h, int shift,

@@ -46,13 +46,8 @@ constexpr int TW = 16;       // lines per tile
 constexpr int TLD = TW + 1;  // shared-memory row pitch (elements)
 constexpr size_t SMEM_LIMIT = 227 * 1024;
 
-// Threads of a CTA that transforms TW lines of length L: about one radix-8 butterfly each,
-// a multiple of 32 in 256..1024.
-template <int L>
-constexpr int threads_for() {
-  constexpr int t = (TW * L / 8 + 31) / 32 * 32;
-  return t < 256 ? 256 : (t > 1024 ? 1024 : t);
-}
+template <int L, int MR = 8>
+constexpr int threads_for();
 
 // ---------------------------------------------------------------------------------------------
 // Complex helpers and small DFTs
@@ -215,11 +210,155 @@ __device__ __forceinline__ void fft_stages(float2* sm, const float2* __restrict_
   }
 }
 
-// Full length-N transform of the tile (N = 2^a 3^b 5^c) with the radix plan MR.
+// ---------------------------------------------------------------------------------------------
+// Warp-per-line plan (MR = 0) for N = 256 and 512: warp w transforms line w of the tile by itself,
+// with three register stages of radix R1, R2, R3 (N = R1 R2 R3; 8.8.8 and 4.8.8) and two exchanges
+// through the line's own shared-memory elements, synchronised with __syncwarp only. With
+// n = s + S1 r (S1 = N / R1), s = sa + R3 sb, k = k1 + R1 (k2 + R2 k3):
+//   A: Y[s][k1]   = w_N^(s k1)     sum_r  x[s + S1 r] w_R1^(r k1)        stored at s + S1 k1
+//   B: Z[sa][k2]  = w_S1^(sa k2)   sum_sb Y[sa + R3 sb][k1] w_R2^(sb k2)  stored at sa + R3 k2 + S1 k1
+//   C: X[k]       =                sum_sa Z[sa][k2] w_R3^(sa k3)         stored at k (natural order)
+// Element t of the line sits in bank pair (t + l) mod 16 (pitch TW + 1 = 17 float2), so an access is
+// conflict-free when the 16 lanes of each half-warp hold distinct t mod 16. The lanes of stages B
+// and C take their inputs in an order rotated per lane so that this holds (B: by k1 mod 2; C: by
+// k1 + 4 ((k2 / 2) mod 2), mod 8), and put the values back in place with register selects.
+template <int N>
+struct WarpPlan {
+  static constexpr bool ok = false;
+};
+template <>
+struct WarpPlan<512> {
+  static constexpr bool ok = true;
+  static constexpr int R1 = 8, R2 = 8, R3 = 8;
+};
+template <>
+struct WarpPlan<256> {
+  static constexpr bool ok = true;
+  static constexpr int R1 = 4, R2 = 8, R3 = 8;
+};
+
+// Threads of a CTA that transforms TW lines of length L: one warp per line for the warp plan, else
+// about one radix-8 butterfly each, a multiple of 32 in 256..1024.
+template <int L, int MR>
+constexpr int threads_for() {
+  if constexpr (MR == 0 && WarpPlan<L>::ok) {
+    return 32 * TW;
+  } else {
+    constexpr int t = (TW * L / 8 + 31) / 32 * 32;
+    return t < 256 ? 256 : (t > 1024 ? 1024 : t);
+  }
+}
+
+template <bool INV>
+__device__ __forceinline__ float2 twiddle(const float2* __restrict__ tw, int idx) {
+  float2 w = __ldg(tw + idx);
+  if (INV) w.y = -w.y;
+  return w;
+}
+
+// v[j] = u[(j - k) mod R] when `on` (a rotation of the array by k places), else unchanged
+template <int R, int K>
+__device__ __forceinline__ void rotate_if(float2 (&v)[R], bool on) {
+  float2 u[R];
+#pragma unroll
+  for (int j = 0; j < R; ++j) u[j] = v[j];
+#pragma unroll
+  for (int j = 0; j < R; ++j) {
+    const float2 a = u[(j - K + R) % R];
+    v[j].x = on ? a.x : u[j].x;
+    v[j].y = on ? a.y : u[j].y;
+  }
+}
+
+template <int N, bool INV, int TS>
+__device__ __forceinline__ void warp_fft_line(float2* sm, int l, const float2* __restrict__ tw) {
+  using P = WarpPlan<N>;
+  constexpr int R1 = P::R1, R2 = P::R2, R3 = P::R3, S1 = N / R1;
+  static_assert(R2 == 8 && R3 == 8 && S1 == 64, "plans with S1 = 64 = 8 x 8");
+  const int lane = threadIdx.x & 31;
+  float2* line = sm + l;
+  // A: columns s = lane + 32 q
+  {
+    constexpr int QA = S1 / 32;
+    float2 v[QA][R1];
+#pragma unroll
+    for (int q = 0; q < QA; ++q) {
+      const int s = lane + 32 * q;
+#pragma unroll
+      for (int r = 0; r < R1; ++r) v[q][r] = line[(s + S1 * r) * TLD];
+      dft<R1, INV>(v[q]);
+#pragma unroll
+      for (int k1 = 1; k1 < R1; ++k1) v[q][k1] = cmul(v[q][k1], twiddle<INV>(tw, s * k1 * TS));
+    }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < QA; ++q) {
+      const int s = lane + 32 * q;
+#pragma unroll
+      for (int k1 = 0; k1 < R1; ++k1) line[(s + S1 * k1) * TLD] = v[q][k1];
+    }
+    __syncwarp();
+  }
+  // B: pairs p = lane + 32 q -> (sa = p % R3, k1 = p / R3); lanes with odd k1 rotate sb by one
+  {
+    constexpr int QB = R3 * R1 / 32;
+    float2 v[QB][R2];
+#pragma unroll
+    for (int q = 0; q < QB; ++q) {
+      const int p = lane + 32 * q, sa = p % R3, k1 = p / R3, rho = k1 & 1;
+#pragma unroll
+      for (int i = 0; i < R2; ++i) v[q][i] = line[(sa + R3 * ((i + rho) % R2) + S1 * k1) * TLD];
+      rotate_if<R2, 1>(v[q], rho);  // v[sb]
+      dft<R2, INV>(v[q]);
+#pragma unroll
+      for (int k2 = 1; k2 < R2; ++k2) v[q][k2] = cmul(v[q][k2], twiddle<INV>(tw, R1 * sa * k2 * TS));
+      rotate_if<R2, R2 - 1>(v[q], rho);  // v[i] = Z[(i + rho) % R2]
+    }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < QB; ++q) {
+      const int p = lane + 32 * q, sa = p % R3, k1 = p / R3, rho = k1 & 1;
+#pragma unroll
+      for (int i = 0; i < R2; ++i) line[(sa + R3 * ((i + rho) % R2) + S1 * k1) * TLD] = v[q][i];
+    }
+    __syncwarp();
+  }
+  // C: pairs p = lane + 32 q -> (k1 = p % R1, k2 = p / R1); lane rotation rho of sa
+  {
+    constexpr int QC = R1 * R2 / 32;
+    float2 v[QC][R3];
+#pragma unroll
+    for (int q = 0; q < QC; ++q) {
+      const int p = lane + 32 * q, k1 = p % R1, k2 = p / R1, rho = (k1 + 4 * ((k2 >> 1) & 1)) & 7;
+#pragma unroll
+      for (int i = 0; i < R3; ++i) v[q][i] = line[(((i + rho) & 7) + R3 * k2 + S1 * k1) * TLD];
+      rotate_if<R3, 1>(v[q], rho & 1);
+      rotate_if<R3, 2>(v[q], rho & 2);
+      rotate_if<R3, 4>(v[q], rho & 4);  // v[sa]
+      dft<R3, INV>(v[q]);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < QC; ++q) {
+      const int p = lane + 32 * q, k1 = p % R1, k2 = p / R1;
+#pragma unroll
+      for (int k3 = 0; k3 < R3; ++k3) line[(k1 + R1 * k2 + R1 * R2 * k3) * TLD] = v[q][k3];
+    }
+  }
+}
+
+// Full length-N transform of the tile (N = 2^a 3^b 5^c) with the radix plan MR (MR = 0: the
+// warp-per-line plan where it exists, else the radix-8 Stockham plan).
 template <int N, bool INV, int T, int TS = 1, int MR = 8>
 __device__ __forceinline__ void fft_lines(float2* sm, const float2* __restrict__ tw) {
   static_assert(N >= 2 && N <= 1024 && smooth235(N), "lengths 2..1024 with prime factors 2, 3, 5");
-  fft_stages<N, 1, INV, T, TS, MR>(sm, tw);
+  if constexpr (MR == 0 && WarpPlan<N>::ok) {
+    static_assert(T == 32 * TW, "one warp per line");
+    warp_fft_line<N, INV, TS>(sm, threadIdx.x >> 5, tw);
+    __syncthreads();
+  } else {
+    fft_stages<N, 1, INV, T, TS, (MR == 0 ? 8 : MR)>(sm, tw);
+  }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -717,7 +856,7 @@ constexpr size_t c_tile(int rows_of_tile) { return (size_t)rows_of_tile * TLD * 
 template <int N, int MR = 8>
 static void cols_pass(float2* data, long long comp_stride, int ncomp, ColGeo g, int inverse, const float2* tw,
                       cudaStream_t s) {
-  constexpr int T = threads_for<N>();
+  constexpr int T = threads_for<N, MR>();
   constexpr int NB = 2 * c_tile(N) <= SMEM_LIMIT ? 2 : 1;
   const size_t smem = NB * c_tile(N);
   g.col_tiles = (g.cols + TW - 1) / TW;
@@ -802,7 +941,7 @@ static void poisson_n(const FftPlan& p, const PoissonParams& pp, const float* de
     // same tile of slots 0..2, and tiles are disjoint, so the update in place is safe.
     float2* s0 = spec;
     {  // 1. z: R2C into slot 0 (staging buffers of 16-byte slots + one complex tile)
-      constexpr int T = threads_for<M>();
+      constexpr int T = threads_for<M, MR>();
       constexpr int NB = 2 * (4 * c_tile(M) + c_tile(M)) <= SMEM_LIMIT ? 2 : 1;  // two CTAs per SM
       const size_t smem = (2 * NB + 1) * c_tile(M);
       launch_persistent(k_r2c_z<N, NB, T, MR>, T, smem, row_tiles, s, delta, fx, std::ldexp(1.0f, -fx_shift), mean, s0,
@@ -812,7 +951,7 @@ static void poisson_n(const FftPlan& p, const PoissonParams& pp, const float* de
     //    (the x planes of a batch's boxes form one run)
     cols_pass<N, MR>(s0, 0, 1, ColGeo{n * NHP, NHP, NH, 0, nb * N}, 0, tw, s);
     {  // 3. x forward + Green + gradient + x inverse -> slots 0 (-i k_x phi) and 1 (phi); outer = y
-      constexpr int T = threads_for<N>();
+      constexpr int T = threads_for<N, MR>();
       constexpr int NBX = 3 * c_tile(N) <= SMEM_LIMIT ? 2 : 1;
       const size_t smem = (NBX + 1) * c_tile(N);
       ColGeo g{NHP, n * NHP, NH, (NH + TW - 1) / TW, nb * N, nb > 1 ? N : 0, n * n * NHP};
@@ -821,7 +960,7 @@ static void poisson_n(const FftPlan& p, const PoissonParams& pp, const float* de
     // 4. y inverse: slot 0 (x component), then slots 1, 2 (y, z components) from the potential
     cols_pass<N, MR>(spec, comp, 1, ColGeo{n * NHP, NHP, NH, 0, nb * N}, 1, tw, s);
     {
-      constexpr int T = threads_for<N>();
+      constexpr int T = threads_for<N, MR>();
       constexpr int NBY = 3 * c_tile(N) <= SMEM_LIMIT ? 2 : 1;
       const size_t smem = (NBY + 1) * c_tile(N);
       ColGeo g{n * NHP, NHP, NH, (NH + TW - 1) / TW, nb * N};
@@ -833,7 +972,7 @@ static void poisson_n(const FftPlan& p, const PoissonParams& pp, const float* de
     cols_pass<N, MR>(spec, comp, 3, ColGeo{n * NHP, NHP, NH, 0, N}, 1, tw, s);
   }
   {  // 5. z: C2R with 1/n^3
-    constexpr int T = threads_for<M>();
+    constexpr int T = threads_for<M, MR>();
     constexpr int NB = 2 * c_tile(M + 1) <= SMEM_LIMIT ? 2 : 1;
     const size_t smem = NB * c_tile(M + 1);
     launch_persistent(k_c2r_z<N, NB, T, MR>, T, smem, 3 * row_tiles, s, spec, comp, gx, gy, gz, pp.scale, rows, tw);
@@ -858,6 +997,8 @@ void launch_poisson(const FftPlan& p, const PoissonParams& pp, const float* delt
   case N:                                                                    \
     if (p.max_radix == 4)                                                    \
       poisson_n<N, 4>(p, pp, delta, fx, fx_shift, mean, spec, gx, gy, gz, s); \
+    else if (p.max_radix == 0)                                               \
+      poisson_n<N, 0>(p, pp, delta, fx, fx_shift, mean, spec, gx, gy, gz, s); \
     else                                                                     \
       poisson_n<N, 8>(p, pp, delta, fx, fx_shift, mean, spec, gx, gy, gz, s); \
     break;

@@ -21,13 +21,18 @@
 // a row box lands as [chunk][136 voxels][8 channels]: the K-major canonical layout of an MMA A
 // operand (core matrix = 8 voxels x 8 channels, SBO = 128 B, LBO = one chunk plane), and a shift
 // of the tile by one voxel along z is a shift of the descriptor's start address by 16 bytes. So a
-// 3^3 convolution over a tile of 128 voxels is 9 row loads and 27 MMAs of 128 x 16 x 16 (implicit
-// GEMM: no im2col copy).
+// 3^3 convolution over a row of 128 voxels is 9 row loads and 27 MMAs of 128 x 16 x 16 (implicit
+// GEMM: no im2col copy); the forward kernel groups them per input row (below).
 //
-// Kernels (warp-specialised, persistent over tiles of 128 voxels of one row):
+// Kernels (warp-specialised, persistent over tiles of 128-voxel rows):
 //   k_conv3       forward convolution (also the data gradient, with transposed and flipped weights):
 //                 warp 0 = TMA producer, warp 1 = MMA issuer (one thread), warps 2-5 = epilogue
-//                 (TMEM -> registers, leaky ReLU or the activation-derivative gate, BF16 or FP32 out)
+//                 (TMEM -> registers, leaky ReLU or the activation-derivative gate, BF16 or FP32 out).
+//                 A tile is 16 output rows (consecutive y) of 128 voxels; each input row is loaded
+//                 once per tile and feeds the (up to) three output rows it touches through one MMA
+//                 of N = 48 whose weight operand stacks the three dy taps: 9 MMAs per input row
+//                 instead of 27 per output row, so each 4 KB activation operand read from shared
+//                 memory serves three times the arithmetic.
 //   k_conv3_wgrad weight gradient dW[t][co][ci] = sum_v dOut[v][co] In[v + t][ci]: 9 gradient rows
 //                 (x - dx, y - dy) and one input row per tile, both MN-major operands; M = 128 =
 //                 8 rows x 16 output channels, N = 32 = 4 z shifts x 8 input channels, K = voxels;
@@ -63,9 +68,12 @@ constexpr int GRAD_PLANE = TILE_M * 16;         // a gradient row (weight-gradie
 constexpr int GRAD_ROW = 2 * GRAD_PLANE;        // 4096
 constexpr int W_TAP_BYTES = 2 * NET_C * 16;     // [chunk][cout 16][8 cin] bf16 = 512
 constexpr int W_BYTES = NET_TAPS * W_TAP_BYTES;  // 13824
-constexpr int CONV_THREADS = 192;               // 6 warps
-constexpr int CONV_STAGES = 2;
-constexpr int CONV_ROWS = 4;                    // output rows (consecutive y) per forward tile
+constexpr int CONV_THREADS = 192;               // 6 warps (weight-gradient kernel)
+constexpr int FWD_THREADS = 320;                // 10 warps (forward kernel: 8 epilogue warps)
+constexpr int CONV_ROWS = 16;                   // output rows (consecutive y) per forward tile
+constexpr int CONV_SLOTS = 12;                  // input row triplets in flight (forward kernel)
+constexpr int SLOT_BYTES = 3 * ROW_BYTES;       // rows x-1, x, x+1 at one y
+constexpr int WS_BYTES = 2 * 3 * NET_C * 16;    // stacked weights of one (dx, dz): [chunk][48][8 cin] bf16
 constexpr int WG_STAGES = 2;
 constexpr long long WAIT_BUDGET = 1ll << 32;    // clock cycles (about 2 s) before a wait gives up
 
@@ -127,34 +135,46 @@ struct ConvArgs {
 // ---------------------------------------------------------------------------------------------
 // Forward convolution
 // ---------------------------------------------------------------------------------------------
-template <int NSTAGE>
-__global__ void __launch_bounds__(CONV_THREADS, 1) k_conv3(const __grid_constant__ CUtensorMap in_map, ConvArgs a) {
+// Instruction descriptor of a forward MMA: 128 voxels x (16 channels x rows) x 16 input channels.
+__device__ __forceinline__ uint32_t idesc_rows(int rows) {
+  return umma::idesc_bf16(TILE_M, NET_C * rows, false, false);
+}
+
+template <int NSLOT>
+__global__ void __launch_bounds__(FWD_THREADS, 1) k_conv3(const __grid_constant__ CUtensorMap in_map, ConvArgs a) {
   constexpr int R = CONV_ROWS;            // output rows (consecutive y) per tile
-  constexpr int IN = 3 * (R + 2);         // input rows per tile: x-1..x+1 by y0-1..y0+R
+  constexpr int NY = R + 2;               // input row triplets per tile: y0-1 .. y0+R
   extern __shared__ __align__(1024) uint8_t smem[];
-  uint8_t* rows = smem;                                // [NSTAGE][IN][ROW_BYTES]
-  uint8_t* wsm = smem + NSTAGE * IN * ROW_BYTES;       // packed weights
+  uint8_t* slots = smem;                               // [NSLOT][3 rows x-1, x, x+1][ROW_BYTES]
+  uint8_t* wsm = smem + NSLOT * SLOT_BYTES;            // weights stacked over dy, [dx][dz][chunk][48][8]
   uint64_t* bars = reinterpret_cast<uint64_t*>(wsm + W_BYTES);
-  uint64_t* full = bars;                  // [NSTAGE] rows loaded
-  uint64_t* empty = bars + NSTAGE;        // [NSTAGE] rows consumed by the MMAs
-  uint64_t* acc_full = bars + 2 * NSTAGE;      // [2] accumulators ready
-  uint64_t* acc_empty = bars + 2 * NSTAGE + 2;  // [2] accumulators read by the epilogue
-  uint64_t* done = bars + 2 * NSTAGE + 4;
-  uint32_t* tmem_sh = reinterpret_cast<uint32_t*>(bars + 2 * NSTAGE + 5);
+  uint64_t* full = bars;                  // [NSLOT] triplet loaded
+  uint64_t* empty = bars + NSLOT;         // [NSLOT] triplet consumed by the MMAs
+  uint64_t* acc_full = bars + 2 * NSLOT;      // [2] accumulators ready
+  uint64_t* acc_empty = bars + 2 * NSLOT + 2;  // [2] accumulators read by the epilogue
+  uint64_t* done = bars + 2 * NSLOT + 4;
+  uint32_t* tmem_sh = reinterpret_cast<uint32_t*>(bars + 2 * NSLOT + 5);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int n = a.g.n;
   const int yq_count = n / R;
-  for (int i = threadIdx.x; i < W_BYTES / 16; i += CONV_THREADS)
-    reinterpret_cast<uint4*>(wsm)[i] = __ldg(reinterpret_cast<const uint4*>(a.w) + i);
+  // Restack the weights [tap][chunk][cout][8 cin] as, per (dx, dz), one N = 48 operand whose rows
+  // are (dy = +1, 0, -1) x cout: the output rows fed by one input row, in increasing y.
+  for (int i = threadIdx.x; i < W_BYTES / 16; i += FWD_THREADS) {
+    const int co = i % 48, blk = i / 48;  // blk = (dxi * 3 + dz) * 2 + chunk
+    const int ch = blk & 1, dxz = blk >> 1, dxi = dxz / 3, dz = dxz % 3;
+    const int dyi = 2 - co / 16, c = co % 16;
+    const int tap = (dxi * 3 + dyi) * 3 + dz;
+    reinterpret_cast<uint4*>(wsm)[i] = __ldg(reinterpret_cast<const uint4*>(a.w) + (tap * 2 + ch) * 16 + c);
+  }
   if (threadIdx.x == 0) {
-    for (int s = 0; s < NSTAGE; ++s) {
+    for (int s = 0; s < NSLOT; ++s) {
       umma::mbar_init(&full[s], 1);
       umma::mbar_init(&empty[s], 1);
     }
     for (int b = 0; b < 2; ++b) {
       umma::mbar_init(&acc_full[b], 1);
-      umma::mbar_init(&acc_empty[b], 128);
+      umma::mbar_init(&acc_empty[b], 256);
     }
     umma::mbar_init(done, 1);
     umma::fence_mbar_init();
@@ -170,70 +190,95 @@ __global__ void __launch_bounds__(CONV_THREADS, 1) k_conv3(const __grid_constant
   const uint32_t tmem = *tmem_sh;
 
   if (warp == 0) {
-    if (lane == 0) {  // TMA producer: rows (x+dx, y0-1 .. y0+R) of each tile
+    if (lane == 0) {  // TMA producer: triplets (x-1..x+1, y) for y = y0-1 .. y0+R of each tile
       umma::tma_prefetch_map(&in_map);
       int s = 0;
       uint32_t ph = 0;
       long long issued = 0;
-      for (long long t = blockIdx.x; t < a.tiles; t += gridDim.x) {
-        if (!umma::mbar_wait(&empty[s], ph ^ 1, WAIT_BUDGET)) {
-          atomicCAS(a.status, 0, NET_TIMEOUT);
-          break;
-        }
+      bool ok = true;
+      for (long long t = blockIdx.x; t < a.tiles && ok; t += gridDim.x) {
         const int zt = (int)(t % a.tiles_z);
         const long long xy = t / a.tiles_z;
         const int y0 = (int)(xy % yq_count) * R, x = (int)(xy / yq_count);
-        umma::mbar_arrive_expect_tx(&full[s], IN * ROW_BYTES);
-        for (int r = 0; r < IN; ++r) {
-          const int xs = (x + r / (R + 2) - 1 + n) % n, ys = (y0 + r % (R + 2) - 1 + n) % n;
-          umma::tma_load_5d(rows + (size_t)(s * IN + r) * ROW_BYTES, &in_map, &full[s], 0, zt * TILE_M, 0, ys, xs);
-        }
-        ++issued;
-        if (++s == NSTAGE) {
-          s = 0;
-          ph ^= 1;
+        for (int yi = 0; yi < NY; ++yi) {
+          if (!umma::mbar_wait(&empty[s], ph ^ 1, WAIT_BUDGET)) {
+            atomicCAS(a.status, 0, NET_TIMEOUT);
+            ok = false;
+            break;
+          }
+          const int ys = (y0 + yi - 1 + n) % n;
+          umma::mbar_arrive_expect_tx(&full[s], 3 * ROW_BYTES);
+          for (int r = 0; r < 3; ++r) {
+            const int xs = (x + r - 1 + n) % n;
+            umma::tma_load_5d(slots + (size_t)(s * 3 + r) * ROW_BYTES, &in_map, &full[s], 0, zt * TILE_M, 0, ys, xs);
+          }
+          ++issued;
+          if (++s == NSLOT) {
+            s = 0;
+            ph ^= 1;
+          }
         }
       }
       // drain: wait until the loads still in flight have landed (they complete without a consumer)
-      for (int k = 0; k < NSTAGE && issued > 0; ++k, --issued) {
-        s = s == 0 ? NSTAGE - 1 : s - 1;
-        if (s == NSTAGE - 1) ph ^= 1;
+      for (int k = 0; k < NSLOT && issued > 0; ++k, --issued) {
+        s = s == 0 ? NSLOT - 1 : s - 1;
+        if (s == NSLOT - 1) ph ^= 1;
         umma::mbar_wait(&full[s], ph, WAIT_BUDGET);
       }
     }
   } else if (warp == 1) {
-    if (lane == 0) {  // MMA issuer: 27 MMAs per output row into that row's accumulator
-      constexpr uint32_t IDESC = umma::idesc_bf16(TILE_M, NET_C, false, false);
+    if (lane == 0) {
+      // MMA issuer. Input row (x + dx, y) feeds output rows y - dy, dy in {+1, 0, -1}, of the tile:
+      // one MMA of N = 16 x (rows in the tile) per (dx, dz) with the stacked weights, written to
+      // those rows' adjacent accumulators. An output row's accumulator starts on the first MMA of
+      // the triplet y = row - 1 (dx = -1, dz = -1), which is split so that the new row is
+      // written without accumulation.
       const uint32_t w_addr = umma::smem_u32(wsm);
       int s = 0, ab = 0;
       uint32_t ph = 0, aph = 0;
-      for (long long t = blockIdx.x; t < a.tiles; t += gridDim.x) {
-        if (!umma::mbar_wait(&full[s], ph, WAIT_BUDGET) || !umma::mbar_wait(&acc_empty[ab], aph ^ 1, WAIT_BUDGET)) {
+      bool ok = true;
+      for (long long t = blockIdx.x; t < a.tiles && ok; t += gridDim.x) {
+        if (!umma::mbar_wait(&acc_empty[ab], aph ^ 1, WAIT_BUDGET)) {
           atomicCAS(a.status, 0, NET_TIMEOUT);
           break;
         }
-        umma::tc_fence_after();
-        const uint32_t base = umma::smem_u32(rows + (size_t)s * IN * ROW_BYTES);
-        for (int r = 0; r < R; ++r) {
-          const uint32_t d = tmem + (uint32_t)((ab * R + r) * NET_C);
-          for (int dxi = 0; dxi < 3; ++dxi)
-            for (int dyi = 0; dyi < 3; ++dyi) {
-              const int ri = dxi * (R + 2) + r + dyi;
+        for (int yi = 0; yi < NY; ++yi) {
+          if (!umma::mbar_wait(&full[s], ph, WAIT_BUDGET)) {
+            atomicCAS(a.status, 0, NET_TIMEOUT);
+            ok = false;
+            break;
+          }
+          umma::tc_fence_after();
+          const uint32_t base = umma::smem_u32(slots + (size_t)s * SLOT_BYTES);
+          const int a_lo = yi - 2 > 0 ? yi - 2 : 0, a_hi = yi < R - 1 ? yi : R - 1;
+          const int j = a_lo - (yi - 2);  // first stacked block used
+#pragma unroll 1
+          for (int dxi = 0; dxi < 3; ++dxi) {
 #pragma unroll
-              for (int dz = 0; dz < 3; ++dz) {
-                const int tap = (dxi * 3 + dyi) * 3 + dz;
-                const uint64_t ad = umma::sdesc(base + (uint32_t)(ri * ROW_BYTES + dz * 16), PLANE_BYTES, 128);
-                const uint64_t bd = umma::sdesc(w_addr + (uint32_t)(tap * W_TAP_BYTES), 256, 128);
-                umma::mma_bf16(d, ad, bd, IDESC, tap != 0 ? 1u : 0u);
+            for (int dz = 0; dz < 3; ++dz) {
+              const uint64_t ad = umma::sdesc(base + (uint32_t)(dxi * ROW_BYTES + dz * 16), PLANE_BYTES, 128);
+              const uint32_t wb = w_addr + (uint32_t)((dxi * 3 + dz) * WS_BYTES + j * 256);
+              const uint32_t d = tmem + (uint32_t)((ab * R + a_lo) * NET_C);
+              if (dxi == 0 && dz == 0 && yi < R) {
+                // rows a_lo .. yi-1 accumulate, row yi starts here
+                const int old = yi - a_lo;
+                if (old > 0)
+                  umma::mma_bf16(d, ad, umma::sdesc(wb, WS_BYTES / 2, 128), idesc_rows(old), 1u);
+                umma::mma_bf16(d + (uint32_t)(old * NET_C), ad, umma::sdesc(wb + (uint32_t)(old * 256), WS_BYTES / 2, 128),
+                               idesc_rows(1), 0u);
+              } else {
+                umma::mma_bf16(d, ad, umma::sdesc(wb, WS_BYTES / 2, 128), idesc_rows(a_hi - a_lo + 1), 1u);
               }
             }
+          }
+          umma::mma_commit(&empty[s]);
+          if (++s == NSLOT) {
+            s = 0;
+            ph ^= 1;
+          }
         }
-        umma::mma_commit(&empty[s]);
+        if (!ok) break;
         umma::mma_commit(&acc_full[ab]);
-        if (++s == NSTAGE) {
-          s = 0;
-          ph ^= 1;
-        }
         if (++ab == 2) {
           ab = 0;
           aph ^= 1;
@@ -242,12 +287,16 @@ __global__ void __launch_bounds__(CONV_THREADS, 1) k_conv3(const __grid_constant
       umma::mma_commit(done);
       umma::mbar_wait(done, 0, WAIT_BUDGET);
     }
-  } else {  // epilogue: warps 2..5, TMEM lane quarter warp % 4
+  } else {
+    // epilogue: warps 2..9. Warp w reads TMEM lane quarter w % 4 (its voxels); warps 2-5 take
+    // output rows 0-7 of the tile, warps 6-9 rows 8-15, four rows per TMEM round trip.
     const int q = warp & 3;
+    const int half = (warp - 2) >> 2;
     const int m = q * 32 + lane;
     int ab = 0;
     uint32_t aph = 0;
     const float scale = a.out_scale_dev ? *a.out_scale_dev : a.out_scale;
+    constexpr int HR = R / 2, GR = 4;
     for (long long t = blockIdx.x; t < a.tiles; t += gridDim.x) {
       if (!umma::mbar_wait(&acc_full[ab], aph, WAIT_BUDGET)) {
         atomicCAS(a.status, 0, NET_TIMEOUT);
@@ -258,43 +307,48 @@ __global__ void __launch_bounds__(CONV_THREADS, 1) k_conv3(const __grid_constant
       const long long xy = t / a.tiles_z;
       const int y0 = (int)(xy % yq_count) * R, x = (int)(xy / yq_count);
       const int z = zt * TILE_M + m;
-      for (int rr = 0; rr < R; ++rr) {
-        uint32_t r[16];
-        umma::tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)((ab * R + rr) * NET_C), r);
+      for (int g = 0; g < HR; g += GR) {
+        uint32_t r4[GR][16];
+#pragma unroll
+        for (int j = 0; j < GR; ++j)
+          umma::tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)((ab * R + half * HR + g + j) * NET_C), r4[j]);
         umma::tmem_wait_ld();
-        if (rr == R - 1) {  // every accumulator of the tile is in registers: release them
+        if (g + GR == HR) {  // every accumulator of this warp is in registers: release them
           umma::tc_fence_before();
           umma::mbar_arrive(&acc_empty[ab]);
         }
         if (z >= n) continue;
-        const int y = y0 + rr;
-        float v[16];
 #pragma unroll
-        for (int c = 0; c < 16; ++c) v[c] = __uint_as_float(r[c]);
-        if (a.out_f4) {
-          a.out_f4[((size_t)x * n + y) * n + z] = make_float4(v[0] * scale, v[1] * scale, v[2] * scale, 0.0f);
-          continue;
-        }
-        if (a.act) {
+        for (int j = 0; j < GR; ++j) {
+          const int y = y0 + half * HR + g + j;
+          float v[16];
 #pragma unroll
-          for (int c = 0; c < 16; ++c) v[c] = lrelu(v[c]);
-        }
-        if (a.gate) {
-          const uint4 g0 = *reinterpret_cast<const uint4*>(a.gate + a.g.at(x, y, 0, z + 1));
-          const uint4 g1 = *reinterpret_cast<const uint4*>(a.gate + a.g.at(x, y, 1, z + 1));
-          const uint32_t gw[8] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w};
-#pragma unroll
-          for (int k = 0; k < 8; ++k) {
-            const float2 gv = unpack_bf16x2(gw[k]);
-            v[2 * k] *= gv.x > 0.0f ? 1.0f : NET_SLOPE;
-            v[2 * k + 1] *= gv.y > 0.0f ? 1.0f : NET_SLOPE;
+          for (int c = 0; c < 16; ++c) v[c] = __uint_as_float(r4[j][c]);
+          if (a.out_f4) {
+            a.out_f4[((size_t)x * n + y) * n + z] = make_float4(v[0] * scale, v[1] * scale, v[2] * scale, 0.0f);
+            continue;
           }
+          if (a.act) {
+#pragma unroll
+            for (int c = 0; c < 16; ++c) v[c] = lrelu(v[c]);
+          }
+          if (a.gate) {
+            const uint4 g0 = *reinterpret_cast<const uint4*>(a.gate + a.g.at(x, y, 0, z + 1));
+            const uint4 g1 = *reinterpret_cast<const uint4*>(a.gate + a.g.at(x, y, 1, z + 1));
+            const uint32_t gw[8] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w};
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+              const float2 gv = unpack_bf16x2(gw[k]);
+              v[2 * k] *= gv.x > 0.0f ? 1.0f : NET_SLOPE;
+              v[2 * k + 1] *= gv.y > 0.0f ? 1.0f : NET_SLOPE;
+            }
+          }
+          const uint4 c0 = make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]), pack_bf16x2(v[4], v[5]),
+                                      pack_bf16x2(v[6], v[7]));
+          const uint4 c1 = make_uint4(pack_bf16x2(v[8], v[9]), pack_bf16x2(v[10], v[11]), pack_bf16x2(v[12], v[13]),
+                                      pack_bf16x2(v[14], v[15]));
+          store_voxel16(a.out16, a.g, x, y, z, c0, c1);
         }
-        const uint4 c0 = make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]), pack_bf16x2(v[4], v[5]),
-                                    pack_bf16x2(v[6], v[7]));
-        const uint4 c1 = make_uint4(pack_bf16x2(v[8], v[9]), pack_bf16x2(v[10], v[11]), pack_bf16x2(v[12], v[13]),
-                                    pack_bf16x2(v[14], v[15]));
-        store_voxel16(a.out16, a.g, x, y, z, c0, c1);
       }
       if (++ab == 2) {
         ab = 0;
@@ -605,8 +659,8 @@ static bool make_row_map(CUtensorMap* map, const __nv_bfloat16* t, int n, int bo
   return r == CUDA_SUCCESS;
 }
 
-constexpr size_t conv_smem_bytes(int stages) {
-  return (size_t)stages * 3 * (CONV_ROWS + 2) * ROW_BYTES + W_BYTES + 8 * (2 * stages + 5) + 16;
+constexpr size_t conv_smem_bytes(int slots) {
+  return (size_t)slots * SLOT_BYTES + W_BYTES + 8 * (2 * slots + 5) + 16;
 }
 constexpr size_t wgrad_smem_bytes(int stages) {
   return (size_t)stages * (9 * GRAD_ROW + ROW_BYTES) + 8 * (2 * stages + 1) + 16;
@@ -674,11 +728,11 @@ void launch_conv(cpm_net* net, const CUtensorMap& in_map, int layer, bool transp
   a.out_scale = out_scale;
   a.out_scale_dev = out_scale_dev;
   a.status = net_status(net);
-  const size_t smem = conv_smem_bytes(CONV_STAGES);
-  cudaFuncSetAttribute(k_conv3<CONV_STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const size_t smem = conv_smem_bytes(CONV_SLOTS);
+  cudaFuncSetAttribute(k_conv3<CONV_SLOTS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const long long grid = std::min<long long>(a.tiles, sm_count());
   count_launch();
-  k_conv3<CONV_STAGES><<<(unsigned)grid, CONV_THREADS, smem, s>>>(in_map, a);
+  k_conv3<CONV_SLOTS><<<(unsigned)grid, FWD_THREADS, smem, s>>>(in_map, a);
 }
 
 void launch_wgrad(cpm_net* net, const CUtensorMap& grad_map, const CUtensorMap& in_map, int layer, cudaStream_t s) {

@@ -43,6 +43,8 @@ namespace {
 constexpr int N_PHASES = 8;
 }
 
+constexpr int N_TUNE = 9;  // autotuner candidates: 3 FFT plans, 3 deposit tiles, 3 walk groups
+
 struct cpm_sim {
   cpm_sim_params P{};
   cudaStream_t stream = nullptr;
@@ -90,9 +92,9 @@ struct cpm_sim {
   int nb = 1;
   size_t n_box = 0;
   int levels = KEY_LEVELS;
-  // Autotuned launch choices (FFT radix plan in `plan`, walk warps in `tree`) and the timings.
+  // Autotuned launch choices (FFT plan in `plan`, walk warps in `tree`) and the timings.
   int dep_ppt = 4;
-  float tune_ms[8] = {};
+  float tune_ms[N_TUNE] = {};
   bool tuned = false;
 };
 
@@ -253,18 +255,20 @@ static int sim_accelerations(cpm_sim* s, float a, const StepScalars* dev = nullp
 // Autotuner. The compiled alternatives of three launch parameters are timed on the simulation's
 // own first state (after its first force evaluation, so the mesh, the sorted particles and the tree
 // are real), and the fastest is kept:
-//   FFT radix plan of the Poisson passes  largest radix 8 (512 = 8.8.8) or 4 (4.4.4.4.2)
+//   FFT plan of the Poisson passes        Stockham stages of largest radix 8 (512 = 8.8.8) or 4
+//                                         (4.4.4.4.2) over the CTA, or (0) one warp per 256- or
+//                                         512-point line with register stages (radix 8 elsewhere)
 //   deposit tile                          256 x {2, 4, 8} sorted particles per CTA
 //   walk group                            {2, 4, 8} warps of 32 particles per block
 // Each candidate runs once untimed and twice timed with CUDA events on the simulation's stream;
 // the work repeats what the force evaluation did (deposit, Poisson solve) or writes to scratch
 // (walk), so the state is unchanged. Choices are cached per workload (particles, mesh, tree,
 // quadrupoles) for the process, and in the file named by CPM_TUNE_CACHE when it is set (one line
-// per workload: key, radix, tile, warps). CPM_SIM_NO_AUTOTUNE keeps 8, 4 and 4.
+// per workload: key, plan, tile, warps). CPM_SIM_NO_AUTOTUNE keeps 8, 4 and 4.
 namespace {
 struct TuneChoice {
   int radix = 8, ppt = 4, warps = 4;
-  float ms[8] = {};
+  float ms[N_TUNE] = {};  // plan 8, 4, 0; tile 512, 1024, 2048; warps 2, 4, 8
 };
 std::mutex g_tune_mu;
 std::map<std::string, TuneChoice> g_tune_cache;
@@ -321,7 +325,7 @@ static void apply_tuning(cpm_sim* s, const TuneChoice& c) {
   s->plan.max_radix = c.radix;
   s->dep_ppt = c.ppt;
   s->tree.walk_warps = c.warps;
-  for (int i = 0; i < 8; ++i) s->tune_ms[i] = c.ms[i];
+  for (int i = 0; i < N_TUNE; ++i) s->tune_ms[i] = c.ms[i];
   s->tuned = true;
 }
 
@@ -350,9 +354,9 @@ static int sim_autotune(cpm_sim* s) {
   PoissonParams pp =
       make_poisson_params(mn, s->box, s->P.cosmo.omega_m, s->a, r_split, (s->P.flags & CPM_SIM_DECONVOLVE) ? 1 : 0);
   pp.boxes = s->nb;
-  const int radices[2] = {8, 4};
+  const int radices[3] = {8, 4, 0};
   float best = 1e30f;
-  for (int k = 0; k < 2; ++k) {
+  for (int k = 0; k < 3; ++k) {
     s->plan.max_radix = radices[k];
     c.ms[k] = time_ms(s->stream, e0, e1, [&] {
       launch_poisson(s->plan, pp, nullptr, as<unsigned long long>(s->fx), s->shift, s->mean, as<float2>(s->spec),
@@ -363,11 +367,11 @@ static int sim_autotune(cpm_sim* s) {
   const int tiles[3] = {2, 4, 8};
   best = 1e30f;
   for (int k = 0; k < 3; ++k) {
-    c.ms[2 + k] = time_ms(s->stream, e0, e1, [&] {
+    c.ms[3 + k] = time_ms(s->stream, e0, e1, [&] {
       launch_deposit_fixed(as<float>(s->x), s->n, 1.0f, mn, s->h, s->shift, as<unsigned long long>(s->fx), s->stream,
                            tiles[k], batch_box(s));
     });
-    if (c.ms[2 + k] < best) best = c.ms[2 + k], c.ppt = tiles[k];
+    if (c.ms[3 + k] < best) best = c.ms[3 + k], c.ppt = tiles[k];
   }
   if (s->P.use_tree && s->tree.geo.p && !(s->P.flags & CPM_SIM_QUADRUPOLE)) {
     int rc = ensure(s->host_tmp, 3 * s->n * sizeof(float)) == cudaSuccess ? CPM_OK : CPM_E_NOMEM;
@@ -377,11 +381,11 @@ static int sim_autotune(cpm_sim* s) {
     best = 1e30f;
     for (int k = 0; k < 3; ++k) {
       s->tree.walk_warps = warps[k];
-      c.ms[5 + k] = time_ms(s->stream, e0, e1, [&] {
+      c.ms[6 + k] = time_ms(s->stream, e0, e1, [&] {
         launch_tree_walk(s->tree, as<float>(s->x), s->n, s->box, s->P.split, kk, as<float>(s->host_tmp), 0, nullptr,
                          as<DevStatus>(s->status), s->stream);
       });
-      if (c.ms[5 + k] < best) best = c.ms[5 + k], c.warps = warps[k];
+      if (c.ms[6 + k] < best) best = c.ms[6 + k], c.warps = warps[k];
     }
   }
   cudaEventDestroy(e0);
@@ -975,22 +979,23 @@ int cpm_sim_short_range(cpm_sim* s, float* sr3) {
   return sim_check(s);
 }
 
-int cpm_sim_autotune_report(cpm_sim* s, int* fft_radix, int* deposit_tile, int* walk_warps, float* ms8) {
+int cpm_sim_autotune_report(cpm_sim* s, int* fft_radix, int* deposit_tile, int* walk_warps, float* ms9) {
   if (!s) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_autotune_report: sim is NULL");
   if (fft_radix) *fft_radix = s->plan.max_radix;
   if (deposit_tile) *deposit_tile = 256 * s->dep_ppt;
   if (walk_warps) *walk_warps = s->tree.walk_warps;
-  if (ms8)
-    for (int i = 0; i < 8; ++i) ms8[i] = s->tune_ms[i];
+  if (ms9)
+    for (int i = 0; i < N_TUNE; ++i) ms9[i] = s->tune_ms[i];
   return CPM_OK;
 }
 
 int cpm_sim_set_tuning(cpm_sim* s, int fft_radix, int deposit_tile, int walk_warps) {
   if (!s) return set_error(nullptr, CPM_E_INVALID, "cpm_sim_set_tuning: sim is NULL");
-  if ((fft_radix != 4 && fft_radix != 8) || (deposit_tile != 512 && deposit_tile != 1024 && deposit_tile != 2048) ||
+  if ((fft_radix != 0 && fft_radix != 4 && fft_radix != 8) ||
+      (deposit_tile != 512 && deposit_tile != 1024 && deposit_tile != 2048) ||
       (walk_warps != 2 && walk_warps != 4 && walk_warps != 8))
     return set_error(&s->err, CPM_E_INVALID,
-                     "cpm_sim_set_tuning: radix 4 or 8, tile 512, 1024 or 2048, warps 2, 4 or 8");
+                     "cpm_sim_set_tuning: FFT plan 8, 4 or 0, tile 512, 1024 or 2048, warps 2, 4 or 8");
   SIM_CU(s, cudaStreamSynchronize(s->stream));
   s->plan.max_radix = fft_radix;
   s->dep_ppt = deposit_tile / 256;

@@ -334,13 +334,15 @@ int cpm_sim_load(const char* path, uint32_t extra_flags, cpm_sim** out);
 int cpm_step_factors(const cpm_cosmology* cosmo, double a0, double a1, int fp64, double* k1, double* d, double* k2);
 /* No counterpart in the reference. The launch choices the autotuner made when the simulation was
  * created (each candidate timed on the simulation's own first state; cached per workload, and in the
- * file named by the environment variable CPM_TUNE_CACHE when set): the largest radix of the Poisson
- * FFT passes (8 or 4), the deposit tile (512, 1024 or 2048 sorted particles per CTA) and the walk
- * group (2, 4 or 8 warps of 32 particles per block). ms8 (may be NULL) receives the measured ms per
- * call: radix 8, 4; tile 512, 1024, 2048; warps 2, 4, 8 (0 where not timed). */
-int cpm_sim_autotune_report(cpm_sim* sim, int* fft_radix, int* deposit_tile, int* walk_warps, float* ms8);
-/* Overrides the autotuner's choices (radix 4 or 8, tile 512, 1024 or 2048, warps 2, 4 or 8); the next
- * force evaluation uses them. Deposit tile and walk group do not change any result bit; the radix
+ * file named by the environment variable CPM_TUNE_CACHE when set): the FFT plan of the Poisson passes
+ * (8 or 4: shared-memory Stockham stages of largest radix 8 or 4 over the CTA; 0: one warp per
+ * 256- or 512-point line with register stages, radix 8 for other lengths), the deposit tile (512,
+ * 1024 or 2048 sorted particles per CTA) and the walk group (2, 4 or 8 warps of 32 particles per
+ * block). ms9 (may be NULL) receives the measured ms per call: plan 8, 4, 0; tile 512, 1024, 2048;
+ * warps 2, 4, 8 (0 where not timed). */
+int cpm_sim_autotune_report(cpm_sim* sim, int* fft_radix, int* deposit_tile, int* walk_warps, float* ms9);
+/* Overrides the autotuner's choices (FFT plan 8, 4 or 0, tile 512, 1024 or 2048, warps 2, 4 or 8); the
+ * next force evaluation uses them. Deposit tile and walk group do not change any result bit; the FFT
  * plan changes FFT rounding only. */
 int cpm_sim_set_tuning(cpm_sim* sim, int fft_radix, int deposit_tile, int walk_warps);
 /* The last tree build's deepest split level, and the number of nodes with more than 8 particles

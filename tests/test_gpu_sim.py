@@ -376,11 +376,11 @@ def test_autotuned_variants_give_the_same_forces(cpm):
     for a1 in cpm.ln_a_schedule(0.02, 1.0, 64)[:48]:
         sim.step_to(a1)
     t = sim.tuning()
-    assert t["fft_radix"] in (4, 8) and t["deposit_tile"] in (512, 1024, 2048) and t["walk_warps"] in (2, 4, 8)
+    assert t["fft_radix"] in (0, 4, 8) and t["deposit_tile"] in (512, 1024, 2048) and t["walk_warps"] in (2, 4, 8)
     assert all(v > 0.0 for v in t["ms"].values())
     st = sim.state()
     accs = {}
-    for radix in (8, 4):
+    for radix in (8, 4, 0):
         for tile in (512, 1024, 2048):
             for warps in (2, 4, 8):
                 sim.set_tuning(radix, tile, warps)
@@ -390,4 +390,26 @@ def test_autotuned_variants_give_the_same_forces(cpm):
         same_radix = accs[(key[0], 1024, 4)]
         assert np.array_equal(acc, same_radix), key
     assert rel_rms(accs[(4, 1024, 4)], accs[(8, 1024, 4)]) < 1e-6
+    assert np.array_equal(accs[(0, 1024, 4)], accs[(8, 1024, 4)])  # no warp plan for 64- and 32-point lines
+    sim.close()
+
+
+@pytest.mark.parametrize("mesh", [256, 512])
+def test_warp_fft_plan_matches_stockham_plan(cpm, mesh):
+    """FFT plan 0 (one warp per 256- or 512-point line, register stages) against the radix-8 Stockham
+    plan, whose Poisson solve is checked against the oracle at these sizes: the PM forces of the
+    same state agree to FFT rounding. Mesh 512 runs every pass on the warp plan (512-point x and y
+    lines, 256-point half-length z lines); mesh 256 its x and y passes."""
+    n_side = mesh // 4
+    cc = cpm.Cosmology(0.0, 0.3, 0.7, 70.0)
+    split = cpm.ForceSplit.with_(float(mesh), mesh, n_side, 1.0 / 30.0, 0.5)
+    sim = cpm.Simulation.from_zeldovich(cc, float(mesh), mesh, n_side, 0.96, 0.8, 0.02, 11, split,
+                                        flags=cpm._native.SIM_NO_AUTOTUNE)
+    st = sim.state()
+    accs = {}
+    for plan in (8, 0):
+        sim.set_tuning(plan, 1024, 4)
+        sim.set_state(st["x"], st["p"])
+        accs[plan] = sim.state()["acc"]
+    assert rel_rms(accs[0], accs[8]) < 1e-6
     sim.close()
