@@ -135,11 +135,6 @@ struct ConvArgs {
 // ---------------------------------------------------------------------------------------------
 // Forward convolution
 // ---------------------------------------------------------------------------------------------
-// Instruction descriptor of a forward MMA: 128 voxels x (16 channels x rows) x 16 input channels.
-__device__ __forceinline__ uint32_t idesc_rows(int rows) {
-  return umma::idesc_bf16(TILE_M, NET_C * rows, false, false);
-}
-
 template <int NSLOT>
 __global__ void __launch_bounds__(FWD_THREADS, 1) k_conv3(const __grid_constant__ CUtensorMap in_map, ConvArgs a) {
   constexpr int R = CONV_ROWS;            // output rows (consecutive y) per tile
@@ -233,7 +228,12 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) k_conv3(const __grid_constant_
       // those rows' adjacent accumulators. An output row's accumulator starts on the first MMA of
       // the triplet y = row - 1 (dx = -1, dz = -1), which is split so that the new row is
       // written without accumulation.
-      const uint32_t w_addr = umma::smem_u32(wsm);
+      // Descriptors as 64-bit words, moved by adding (bytes >> 4) to the start-address field (shared
+      // addresses stay below 256 KB, so the 14-bit field never carries): A of slot 0, row x-1, no z
+      // shift; B of the (dx, dz) = (-1, -1) stack. N = 16 x rows is bits 17.. of the instruction word.
+      const uint64_t a0 = umma::sdesc(umma::smem_u32(slots), PLANE_BYTES, 128);
+      const uint64_t b0 = umma::sdesc(umma::smem_u32(wsm), WS_BYTES / 2, 128);
+      constexpr uint32_t ID0 = umma::idesc_bf16(TILE_M, 0, false, false);
       int s = 0, ab = 0;
       uint32_t ph = 0, aph = 0;
       bool ok = true;
@@ -242,6 +242,7 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) k_conv3(const __grid_constant_
           atomicCAS(a.status, 0, NET_TIMEOUT);
           break;
         }
+        const uint32_t dbase = tmem + (uint32_t)(ab * R * NET_C);
         for (int yi = 0; yi < NY; ++yi) {
           if (!umma::mbar_wait(&full[s], ph, WAIT_BUDGET)) {
             atomicCAS(a.status, 0, NET_TIMEOUT);
@@ -249,27 +250,23 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) k_conv3(const __grid_constant_
             break;
           }
           umma::tc_fence_after();
-          const uint32_t base = umma::smem_u32(slots + (size_t)s * SLOT_BYTES);
           const int a_lo = yi - 2 > 0 ? yi - 2 : 0, a_hi = yi < R - 1 ? yi : R - 1;
           const int j = a_lo - (yi - 2);  // first stacked block used
-#pragma unroll 1
-          for (int dxi = 0; dxi < 3; ++dxi) {
+          const uint64_t as = a0 + (uint64_t)(s * (SLOT_BYTES >> 4));
+          const uint64_t bj = b0 + (uint64_t)(j * 16);
+          const uint32_t d = dbase + (uint32_t)(a_lo * NET_C);
+          const uint32_t idn = ID0 | ((uint32_t)(a_hi - a_lo + 1) << 18);
+          if (yi < R) {  // (dx, dz) = (-1, -1): rows a_lo .. yi-1 accumulate, row yi starts here
+            const int old = yi - a_lo;
+            if (old > 0) umma::mma_bf16(d, as, bj, ID0 | ((uint32_t)old << 18), 1u);
+            umma::mma_bf16(d + (uint32_t)(old * NET_C), as, bj + (uint64_t)(old * 16), ID0 | (1u << 18), 0u);
+          } else {
+            umma::mma_bf16(d, as, bj, idn, 1u);
+          }
 #pragma unroll
-            for (int dz = 0; dz < 3; ++dz) {
-              const uint64_t ad = umma::sdesc(base + (uint32_t)(dxi * ROW_BYTES + dz * 16), PLANE_BYTES, 128);
-              const uint32_t wb = w_addr + (uint32_t)((dxi * 3 + dz) * WS_BYTES + j * 256);
-              const uint32_t d = tmem + (uint32_t)((ab * R + a_lo) * NET_C);
-              if (dxi == 0 && dz == 0 && yi < R) {
-                // rows a_lo .. yi-1 accumulate, row yi starts here
-                const int old = yi - a_lo;
-                if (old > 0)
-                  umma::mma_bf16(d, ad, umma::sdesc(wb, WS_BYTES / 2, 128), idesc_rows(old), 1u);
-                umma::mma_bf16(d + (uint32_t)(old * NET_C), ad, umma::sdesc(wb + (uint32_t)(old * 256), WS_BYTES / 2, 128),
-                               idesc_rows(1), 0u);
-              } else {
-                umma::mma_bf16(d, ad, umma::sdesc(wb, WS_BYTES / 2, 128), idesc_rows(a_hi - a_lo + 1), 1u);
-              }
-            }
+          for (int k = 1; k < 9; ++k) {  // k = (dx + 1) * 3 + (dz + 1)
+            const uint32_t aoff = (uint32_t)((k / 3) * (ROW_BYTES >> 4) + (k % 3));
+            umma::mma_bf16(d, as + aoff, bj + (uint64_t)(k * (WS_BYTES >> 4)), idn, 1u);
           }
           umma::mma_commit(&empty[s]);
           if (++s == NSLOT) {
