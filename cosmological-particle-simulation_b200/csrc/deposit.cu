@@ -2,11 +2,14 @@
 //
 // Particles arrive sorted by octant key, so a chunk of consecutive particles covers a compact
 // box of cells. Each CTA accumulates its chunk into that box in shared memory with 64-bit
-// integer atomics, then flushes every non-zero cell to the global mesh with one 64-bit integer
-// atomic. Integer addition is associative, so the mesh does not depend on particle order or
-// scheduling (bit-reproducible), and it holds the exactly rounded sum of the reference's f32
-// weights `mass * w`. Chunks whose box does not fit in shared memory fall back to direct global
-// atomics (same integers, same result).
+// integer atomics, then adds the box to the global mesh: one bulk reduction (TMA unit,
+// cp.reduce.async.bulk .add.u64) per row of the box along z, split at the periodic boundary, so
+// whole rows leave shared memory in 16-byte multiples instead of one L2 atomic per cell (the box
+// starts at an even z and has an even length for that alignment). Integer addition is
+// associative, so the mesh does not depend on particle order or scheduling (bit-reproducible),
+// and it holds the exactly rounded sum of the reference's f32 weights `mass * w`. Chunks whose box
+// does not fit in shared memory fall back to direct global atomics (same integers, same result),
+// and odd meshes flush the box cell by cell with atomics.
 #include <algorithm>
 #include <cmath>
 
@@ -32,6 +35,16 @@ int fixed_point_shift(double total_mass) {
   return k;
 }
 
+// dst[i] += src[i] for size / 8 u64 elements, element-wise atomic in L2 (bulk-async group of the
+// calling thread); both addresses 16-byte aligned, size a multiple of 16.
+__device__ __forceinline__ void bulk_reduce_add_u64(unsigned long long* dst, const unsigned long long* src,
+                                                    uint32_t bytes) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(src);
+  asm volatile("cp.reduce.async.bulk.global.shared::cta.bulk_group.add.u64 [%0], [%1], %2;" ::"l"(dst), "r"(s),
+               "r"(bytes)
+               : "memory");
+}
+
 __device__ __forceinline__ unsigned long long to_fixed(float mass, float w, float scale) {
   // mass * w is the reference's f32 product; scaling by 2^k is exact.
   return __float2ull_rn(__fmul_rn(__fmul_rn(mass, w), scale));
@@ -43,7 +56,7 @@ template <int DEP_PPT>
 __global__ void __launch_bounds__(DEP_THREADS) k_deposit_fixed(const float* __restrict__ x3, size_t n, float mass,
                                                                int mesh_n, float h, float scale,
                                                                unsigned long long* __restrict__ mesh, size_t n_box) {
-  extern __shared__ unsigned long long sm_cells[];
+  extern __shared__ __align__(16) unsigned long long sm_cells[];
   __shared__ int bb[6];  // min x,y,z then max x,y,z of the stencil base
   if (threadIdx.x < 3) bb[threadIdx.x] = 0x7fffffff;
   else if (threadIdx.x < 6) bb[threadIdx.x] = -0x7fffffff;
@@ -91,9 +104,11 @@ __global__ void __launch_bounds__(DEP_THREADS) k_deposit_fixed(const float* __re
     }
   }
   __syncthreads();
-  const int e0 = bb[3] - bb[0] + 2, e1 = bb[4] - bb[1] + 2, e2 = bb[5] - bb[2] + 2;
-  const long long cells = (long long)e0 * e1 * e2;
   if (bb[0] > bb[3]) return;  // empty chunk
+  // box: x, y from the lowest base; z from the even cell at or below it, an even number of cells
+  const int z0 = bb[2] & ~1;
+  const int e0 = bb[3] - bb[0] + 2, e1 = bb[4] - bb[1] + 2, e2 = (bb[5] + 2 - z0 + 1) & ~1;
+  const long long cells = (long long)e0 * e1 * e2;
 
   if (one_box && cells <= dep_smem_cells<DEP_PPT>() && e0 > 0 && e1 > 0 && e2 > 0) {
     for (int t = threadIdx.x; t < (int)cells; t += DEP_THREADS) sm_cells[t] = 0ull;
@@ -101,7 +116,7 @@ __global__ void __launch_bounds__(DEP_THREADS) k_deposit_fixed(const float* __re
 #pragma unroll
     for (int q = 0; q < DEP_PPT; ++q) {
       if (!valid[q]) continue;
-      const int lx = cb[q].b[0] - bb[0], ly = cb[q].b[1] - bb[1], lz = cb[q].b[2] - bb[2];
+      const int lx = cb[q].b[0] - bb[0], ly = cb[q].b[1] - bb[1], lz = cb[q].b[2] - z0;
 #pragma unroll
       for (int c = 0; c < 8; ++c) {
         const int dx = (c >> 2) & 1, dy = (c >> 1) & 1, dz = c & 1;
@@ -110,6 +125,26 @@ __global__ void __launch_bounds__(DEP_THREADS) k_deposit_fixed(const float* __re
       }
     }
     __syncthreads();
+    if ((mesh_n & 1) == 0 && e2 <= mesh_n) {
+      // the atomics' results become visible to the bulk-copy (async) proxy, then each thread
+      // reduces whole box rows into the mesh
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncthreads();
+      const int zw = wrap_index(z0, mesh_n);
+      const int len1 = min(e2, mesh_n - zw), len2 = e2 - len1;
+      for (int r = threadIdx.x; r < e0 * e1; r += DEP_THREADS) {
+        const int lx = r / e1, ly = r - lx * e1;
+        const size_t gx = (size_t)wrap_index(bb[0] + lx, mesh_n);
+        const size_t gy = (size_t)wrap_index(bb[1] + ly, mesh_n);
+        unsigned long long* grow = mesh + (gx * mesh_n + gy) * mesh_n;
+        const unsigned long long* srow = sm_cells + (size_t)r * e2;
+        bulk_reduce_add_u64(grow + zw, srow, (uint32_t)len1 * 8u);
+        if (len2 > 0) bulk_reduce_add_u64(grow, srow + len1, (uint32_t)len2 * 8u);
+      }
+      asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+      asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+      return;
+    }
     // floor(t / e) as floor((t + 1/2) * fl(1/e)): (t + 1/2) / e lies at least 1/(2e) from an
     // integer, and for t < 2^15 the two f32 roundings move it by less than 2^-7 / e.
     const float inv_e2 = 1.0f / (float)e2, inv_e1 = 1.0f / (float)e1;
@@ -121,7 +156,7 @@ __global__ void __launch_bounds__(DEP_THREADS) k_deposit_fixed(const float* __re
       const int lz = t - row * e2, ly = row - lx * e1;
       const size_t gx = (size_t)wrap_index(bb[0] + lx, mesh_n);
       const size_t gy = (size_t)wrap_index(bb[1] + ly, mesh_n);
-      const size_t gz = (size_t)wrap_index(bb[2] + lz, mesh_n);
+      const size_t gz = (size_t)wrap_index(z0 + lz, mesh_n);
       atomicAdd(&mesh[(gx * mesh_n + gy) * mesh_n + gz], v);
     }
   } else {
