@@ -7,7 +7,9 @@ A batch's particles share one sort (the box index above 19 octant digits instead
 bit can round differently from a single box's; deposit, FFT, gather and kick/drift are per box the
 same arithmetic. So the initial conditions must be equal, the initial forces within 1e-6 relative RMS; after 40 steps
 (the last ones replayed from the ensemble's graph, where the chaotic growth of last-bit differences
-shows) positions within 1e-5 L, forces within 1e-4 relative RMS and the boxes' P(k) within 1e-4."""
+shows) positions within 1e-5 L, forces within 1e-4 relative RMS and the boxes' P(k) within 1e-4.
+Both sides keep the default launch choices (no autotuning): the autotuner picks an FFT plan per
+workload by timing, and two plans round differently, which the 40 chaotic steps would amplify."""
 import numpy as np
 import pytest
 
@@ -32,11 +34,13 @@ def test_every_box_of_a_mixed_ensemble_equals_its_single_run(cpm):
     for n_side, mesh, boxes, seed in [(16, 32, 3, 100), (32, 64, 2, 200), (48, 96, 2, 300)]:
         split = cpm.ForceSplit.with_(box, mesh, n_side, 1.0 / 30.0, 0.5)
         classes.append((n_side, mesh, boxes, seed, split))
-    ens = cpm.Ensemble(cc, box, 0.96, 0.8, 0.02, classes)
+    fixed = cpm._native.SIM_NO_AUTOTUNE
+    ens = cpm.Ensemble(cc, box, 0.96, 0.8, 0.02, classes, flags=fixed)
     # the forces of the initial conditions: every box against its own single-box simulation
     for ci, (n_side, mesh, boxes, seed, split) in enumerate(classes):
         for b in range(boxes):
-            single = cpm.Simulation.from_zeldovich(cc, box, mesh, n_side, 0.96, 0.8, 0.02, seed + b, split)
+            single = cpm.Simulation.from_zeldovich(cc, box, mesh, n_side, 0.96, 0.8, 0.02, seed + b, split,
+                                                    flags=fixed)
             s, e = single.state(), ens.state(ci, b)
             assert np.array_equal(e["x"], s["x"]) and np.array_equal(e["p"], s["p"]), (ci, b)
             assert rel_rms(e["acc"], s["acc"]) < 1e-6, (ci, b)
@@ -47,7 +51,8 @@ def test_every_box_of_a_mixed_ensemble_equals_its_single_run(cpm):
     assert ens.graphs() == 2
     for ci, (n_side, mesh, boxes, seed, split) in enumerate(classes):
         for b in range(boxes):
-            single = cpm.Simulation.from_zeldovich(cc, box, mesh, n_side, 0.96, 0.8, 0.02, seed + b, split)
+            single = cpm.Simulation.from_zeldovich(cc, box, mesh, n_side, 0.96, 0.8, 0.02, seed + b, split,
+                                                    flags=fixed)
             for a1 in sched:
                 single.step_to(a1)
             s, e = single.state(), ens.state(ci, b)

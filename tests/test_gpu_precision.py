@@ -17,13 +17,13 @@ pytestmark = pytest.mark.gpu
 COSMO = (0.0, 0.3, 0.7, 70.0)
 
 
-def _check(cpm, orc, sim, box, mesh, n, n_sample, seed):
+def _check(cpm, orc, sim, box, mesh, n, n_sample, seed, quad=False):
     st = sim.state()
     a = float(st["a"])
     sample = np.sort(np.random.default_rng(seed).choice(n, size=min(n_sample, n), replace=False))
     split = orc.split_with(box, mesh, round(n ** (1 / 3)), 1.0 / 30.0, 0.5)
     t0 = time.time()
-    ref = orc.accelerations_f64(st["x"], box, mesh, COSMO[1], a, split, sample)
+    ref = orc.accelerations_f64(st["x"], box, mesh, COSMO[1], a, split, sample, quadrupole=quad)
     t_acc = time.time() - t0
     got = st["acc"][sample].astype(np.float64)
     err = np.linalg.norm(got - ref, axis=1)
@@ -44,21 +44,21 @@ def _check(cpm, orc, sim, box, mesh, n, n_sample, seed):
     }
 
 
-def _run(cpm, orc, n_side, mesh, box, seed, steps, n_sample, check_start):
+def _run(cpm, orc, n_side, mesh, box, seed, steps, n_sample, check_start, quad=False):
     cc = cpm.Cosmology(*COSMO)
     split = cpm.ForceSplit.with_(box, mesh, n_side, 1.0 / 30.0, 0.5)
-    sim = cpm.Simulation.from_zeldovich(cc, box, mesh, n_side, 0.96, 0.8, 0.02, seed, split,
-                                        flags=cpm._native.SIM_FIXED_POINT)
+    flags = cpm._native.SIM_FIXED_POINT | (cpm._native.SIM_QUADRUPOLE if quad else 0)
+    sim = cpm.Simulation.from_zeldovich(cc, box, mesh, n_side, 0.96, 0.8, 0.02, seed, split, flags=flags)
     n = n_side ** 3
-    out = {}
+    out = {"quadrupole": quad}
     if check_start:
-        out["start"] = _check(cpm, orc, sim, box, mesh, n, n_sample, 1)
+        out["start"] = _check(cpm, orc, sim, box, mesh, n, n_sample, 1, quad)
     t0 = time.time()
     for a1 in cpm.ln_a_schedule(0.02, 1.0, steps):
         sim.step_to(a1)
     sim.state()
     out["gpu_run_s"] = round(time.time() - t0, 1)
-    out["end"] = _check(cpm, orc, sim, box, mesh, n, n_sample, 2)
+    out["end"] = _check(cpm, orc, sim, box, mesh, n, n_sample, 2, quad)
     sim.close()
     return out
 
@@ -73,8 +73,12 @@ def test_precision_small(cpm, orc):
 
 
 @pytest.mark.skipif(os.environ.get("CPM_PRECISION_CONFIG3") != "1", reason="full precision study on request only")
-def test_precision_config3(cpm, orc):
-    res = _run(cpm, orc, 512, 1024, 512.0, 11, 128, 100000, True)
+@pytest.mark.parametrize("quad", [False, True])
+def test_precision_config3(cpm, orc, quad):
+    """The precision mode as a whole: uint32 positions, FP64 kick/drift factors on the device and,
+    with quad, quadrupole moments of accepted nodes (checked against the FP64 oracle with the same
+    quadrupole terms)."""
+    res = _run(cpm, orc, 512, 1024, 512.0, 11, 128, 100000, True, quad)
     print(json.dumps({"precision_config3": res}))
     for key in ("start", "end"):
         r = res[key]
