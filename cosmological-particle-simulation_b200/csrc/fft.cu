@@ -143,29 +143,37 @@ __device__ __forceinline__ void dft(float2* v) {
 
 // One Stockham stage of radix R on the TW lines of a tile (element t of line l at t*TLD + l),
 // T threads. Twiddle exp(-2 pi i m / N) is tw[m * TS] (TS = 2 when the table is for length 2N).
-template <int N, int R, int NS, bool INV, int T, int TS>
-__device__ __forceinline__ void stockham_stage(float2* sm, const float2* __restrict__ tw) {
+// NT = 2 transforms a second tile (sm1) in the same stage: one pair of barriers and one set of
+// twiddle loads serve both.
+template <int N, int R, int NS, bool INV, int T, int TS, int NT = 1>
+__device__ __forceinline__ void stockham_stage(float2* sm0, float2* sm1, const float2* __restrict__ tw) {
   constexpr int NB = N / R;
   constexpr int TOTAL = TW * NB;
   constexpr int BPT = (TOTAL + T - 1) / T;
-  float2 v[BPT][R];
+  float2 v[NT][BPT][R];
 #pragma unroll
   for (int q = 0; q < BPT; ++q) {
     const int b = threadIdx.x + q * T;
     if (TOTAL % T == 0 || b < TOTAL) {
       const int l = b % TW, j = b / TW;
 #pragma unroll
-      for (int r = 0; r < R; ++r) v[q][r] = sm[(j + r * NB) * TLD + l];
+      for (int p = 0; p < NT; ++p) {
+        const float2* sm = p ? sm1 : sm0;
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[p][q][r] = sm[(j + r * NB) * TLD + l];
+      }
       if constexpr (NS > 1) {
         const int k = j % NS;
 #pragma unroll
         for (int r = 1; r < R; ++r) {
           float2 w = __ldg(tw + r * k * (N / (NS * R)) * TS);
           if (INV) w.y = -w.y;
-          v[q][r] = cmul(v[q][r], w);
+#pragma unroll
+          for (int p = 0; p < NT; ++p) v[p][q][r] = cmul(v[p][q][r], w);
         }
       }
-      dft<R, INV>(v[q]);
+#pragma unroll
+      for (int p = 0; p < NT; ++p) dft<R, INV>(v[p][q]);
     }
   }
   __syncthreads();
@@ -177,7 +185,11 @@ __device__ __forceinline__ void stockham_stage(float2* sm, const float2* __restr
       const int k = j % NS;
       const int base = (j / NS) * NS * R + k;
 #pragma unroll
-      for (int r = 0; r < R; ++r) sm[(base + r * NS) * TLD + l] = v[q][r];
+      for (int p = 0; p < NT; ++p) {
+        float2* sm = p ? sm1 : sm0;
+#pragma unroll
+        for (int r = 0; r < R; ++r) sm[(base + r * NS) * TLD + l] = v[p][q][r];
+      }
     }
   }
   __syncthreads();
@@ -201,12 +213,12 @@ constexpr bool smooth235(int n) {
   return n == 1;
 }
 
-template <int N, int NS, bool INV, int T, int TS, int MR>
-__device__ __forceinline__ void fft_stages(float2* sm, const float2* __restrict__ tw) {
+template <int N, int NS, bool INV, int T, int TS, int MR, int NT = 1>
+__device__ __forceinline__ void fft_stages(float2* sm0, float2* sm1, const float2* __restrict__ tw) {
   if constexpr (NS < N) {
     constexpr int R = next_radix<N / NS, MR>();
-    stockham_stage<N, R, NS, INV, T, TS>(sm, tw);
-    fft_stages<N, NS * R, INV, T, TS, MR>(sm, tw);
+    stockham_stage<N, R, NS, INV, T, TS, NT>(sm0, sm1, tw);
+    fft_stages<N, NS * R, INV, T, TS, MR, NT>(sm0, sm1, tw);
   }
 }
 
@@ -357,7 +369,20 @@ __device__ __forceinline__ void fft_lines(float2* sm, const float2* __restrict__
     warp_fft_line<N, INV, TS>(sm, threadIdx.x >> 5, tw);
     __syncthreads();
   } else {
-    fft_stages<N, 1, INV, T, TS, (MR == 0 ? 8 : MR)>(sm, tw);
+    fft_stages<N, 1, INV, T, TS, (MR == 0 ? 8 : MR)>(sm, sm, tw);
+  }
+}
+
+// Two independent tiles transformed together (the same length and direction).
+template <int N, bool INV, int T, int TS = 1, int MR = 8>
+__device__ __forceinline__ void fft_lines2(float2* a, float2* b, const float2* __restrict__ tw) {
+  if constexpr (MR == 0 && WarpPlan<N>::ok) {
+    static_assert(T == 32 * TW, "one warp per line");
+    warp_fft_line<N, INV, TS>(a, threadIdx.x >> 5, tw);
+    warp_fft_line<N, INV, TS>(b, threadIdx.x >> 5, tw);
+    __syncthreads();
+  } else {
+    fft_stages<N, 1, INV, T, TS, (MR == 0 ? 8 : MR), 2>(a, b, tw);
   }
 }
 
@@ -689,8 +714,7 @@ __global__ void __launch_bounds__(T) k_poisson_x(const float2* __restrict__ spec
                                          __fadd_rn(__fmul_rn(v.x, nk), __fmul_rn(v.y, 0.0f)));
         }
         __syncthreads();
-        fft_lines<N, true, T, 1, MR>(gxb, tw);
-        fft_lines<N, true, T, 1, MR>(phi, tw);
+        fft_lines2<N, true, T, 1, MR>(gxb, phi, tw);
         // -i k_x phi to slot 0; the x-transformed phi to slot 1, from which the y pass forms the
         // y and z components (k_y and k_z are constant along an x line)
         store_cols<N, T>(gxb, spec_out, base, g.elem_stride, valid);
@@ -730,8 +754,7 @@ __global__ void __launch_bounds__(T) k_grad_yz(float2* spec, long long comp_stri
                                          __fadd_rn(__fmul_rn(p.x, nkz), __fmul_rn(p.y, 0.0f)));
         }
         __syncthreads();
-        fft_lines<N, true, T, 1, MR>(cur, tw);
-        fft_lines<N, true, T, 1, MR>(gzb, tw);
+        fft_lines2<N, true, T, 1, MR>(cur, gzb, tw);
         store_cols<N, T>(cur, phi_slot, base, g.elem_stride, valid);
         store_cols<N, T>(gzb, spec + 2 * comp_stride, base, g.elem_stride, valid);
       });

@@ -135,10 +135,14 @@ struct ConvArgs {
 // ---------------------------------------------------------------------------------------------
 // Forward convolution
 // ---------------------------------------------------------------------------------------------
-template <int NSLOT>
+// FOLD: the first layer on the folded input (channel 3 (dy+1) + (dz+1) holds delta at (y+dy, z+dz),
+// written by k_net_input_fold): the y and z taps are input channels, so an output row takes the
+// three x rows at its own y, one MMA of 128 x 16 x 16 each (K = 9 live channels), instead of 27 taps
+// over a single live channel.
+template <int NSLOT, bool FOLD>
 __global__ void __launch_bounds__(FWD_THREADS, 1) k_conv3(const __grid_constant__ CUtensorMap in_map, ConvArgs a) {
   constexpr int R = CONV_ROWS;            // output rows (consecutive y) per tile
-  constexpr int NY = R + 2;               // input row triplets per tile: y0-1 .. y0+R
+  constexpr int NY = FOLD ? R : R + 2;    // input row triplets per tile: y0-1 .. y0+R (folded: y0 .. y0+R-1)
   extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t* slots = smem;                               // [NSLOT][3 rows x-1, x, x+1][ROW_BYTES]
   uint8_t* wsm = smem + NSLOT * SLOT_BYTES;            // weights stacked over dy, [dx][dz][chunk][48][8]
@@ -155,12 +159,24 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) k_conv3(const __grid_constant_
   const int yq_count = n / R;
   // Restack the weights [tap][chunk][cout][8 cin] as, per (dx, dz), one N = 48 operand whose rows
   // are (dy = +1, 0, -1) x cout: the output rows fed by one input row, in increasing y.
-  for (int i = threadIdx.x; i < W_BYTES / 16; i += FWD_THREADS) {
-    const int co = i % 48, blk = i / 48;  // blk = (dxi * 3 + dz) * 2 + chunk
-    const int ch = blk & 1, dxz = blk >> 1, dxi = dxz / 3, dz = dxz % 3;
-    const int dyi = 2 - co / 16, c = co % 16;
-    const int tap = (dxi * 3 + dyi) * 3 + dz;
-    reinterpret_cast<uint4*>(wsm)[i] = __ldg(reinterpret_cast<const uint4*>(a.w) + (tap * 2 + ch) * 16 + c);
+  if constexpr (FOLD) {
+    // per dx: [chunk 2][co 16][8 channels], channel c = 3 dyi + dzi < 9 from input channel 0 of tap
+    // (dx, dyi - 1, dzi - 1)
+    const __nv_bfloat16 zero = __float2bfloat16_rn(0.0f);
+    __nv_bfloat16* wf = reinterpret_cast<__nv_bfloat16*>(wsm);
+    for (int i = threadIdx.x; i < 3 * 2 * NET_C * 8; i += FWD_THREADS) {
+      const int k = i % 8, co = (i / 8) % NET_C, ch = (i / (8 * NET_C)) % 2, dxi = i / (16 * NET_C);
+      const int c = ch * 8 + k;
+      wf[i] = c < 9 ? a.w[(((dxi * 3 + c / 3) * 3 + c % 3) * 2 * NET_C + co) * 8] : zero;
+    }
+  } else {
+    for (int i = threadIdx.x; i < W_BYTES / 16; i += FWD_THREADS) {
+      const int co = i % 48, blk = i / 48;  // blk = (dxi * 3 + dz) * 2 + chunk
+      const int ch = blk & 1, dxz = blk >> 1, dxi = dxz / 3, dz = dxz % 3;
+      const int dyi = 2 - co / 16, c = co % 16;
+      const int tap = (dxi * 3 + dyi) * 3 + dz;
+      reinterpret_cast<uint4*>(wsm)[i] = __ldg(reinterpret_cast<const uint4*>(a.w) + (tap * 2 + ch) * 16 + c);
+    }
   }
   if (threadIdx.x == 0) {
     for (int s = 0; s < NSLOT; ++s) {
@@ -201,7 +217,7 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) k_conv3(const __grid_constant_
             ok = false;
             break;
           }
-          const int ys = (y0 + yi - 1 + n) % n;
+          const int ys = (y0 + yi - (FOLD ? 0 : 1) + n) % n;
           umma::mbar_arrive_expect_tx(&full[s], 3 * ROW_BYTES);
           for (int r = 0; r < 3; ++r) {
             const int xs = (x + r - 1 + n) % n;
@@ -250,9 +266,23 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) k_conv3(const __grid_constant_
             break;
           }
           umma::tc_fence_after();
+          const uint64_t as = a0 + (uint64_t)(s * (SLOT_BYTES >> 4));
+          if constexpr (FOLD) {  // output row yi from the rows x-1, x, x+1 at its y, z shift 0
+            const uint64_t bf = umma::sdesc(umma::smem_u32(wsm), 256, 128);
+            const uint32_t d = dbase + (uint32_t)(yi * NET_C);
+#pragma unroll
+            for (int dxi = 0; dxi < 3; ++dxi)
+              umma::mma_bf16(d, as + (uint64_t)(dxi * (ROW_BYTES >> 4) + 1), bf + (uint64_t)(dxi * 32),
+                             ID0 | (1u << 18), dxi ? 1u : 0u);
+            umma::mma_commit(&empty[s]);
+            if (++s == NSLOT) {
+              s = 0;
+              ph ^= 1;
+            }
+            continue;
+          }
           const int a_lo = yi - 2 > 0 ? yi - 2 : 0, a_hi = yi < R - 1 ? yi : R - 1;
           const int j = a_lo - (yi - 2);  // first stacked block used
-          const uint64_t as = a0 + (uint64_t)(s * (SLOT_BYTES >> 4));
           const uint64_t bj = b0 + (uint64_t)(j * 16);
           const uint32_t d = dbase + (uint32_t)(a_lo * NET_C);
           const uint32_t idn = ID0 | ((uint32_t)(a_hi - a_lo + 1) << 18);
@@ -527,6 +557,36 @@ __global__ void k_net_input(const float* __restrict__ delta, const unsigned long
   }
 }
 
+// The first layer's input with its y and z taps folded into channels: channel 3 dyi + dzi of voxel
+// (x, y, z) holds s_in delta at (x, y + dyi - 1, z + dzi - 1) (periodic), channels 9-15 are 0 — the
+// same BF16 values as k_net_input's channel 0, nine times. A CTA covers 8 y by 32 z of one x plane
+// and stages the 10 x 34 neighbourhood in shared memory. delta as in k_net_input.
+__global__ void __launch_bounds__(256) k_net_input_fold(const unsigned long long* __restrict__ fx, float inv_fx,
+                                                        float mean, float in_scale, TensorGeo g,
+                                                        __nv_bfloat16* __restrict__ out) {
+  __shared__ float sd[10][34];
+  const int n = g.n;
+  const int z0 = blockIdx.x * 32, y0 = blockIdx.y * 8, x = blockIdx.z;
+  const int tid = threadIdx.y * 32 + threadIdx.x;
+  for (int k = tid; k < 10 * 34; k += 256) {
+    const int yy = k / 34, zz = k % 34;
+    const int y = (y0 - 1 + yy + n) % n, z = (z0 - 1 + zz + n) % n;
+    const float c = __fmul_rn(__ull2float_rn(fx[((size_t)x * n + y) * n + z]), inv_fx);
+    sd[yy][zz] = __fsub_rn(__fdiv_rn(c, mean), 1.0f) * in_scale;
+  }
+  __syncthreads();
+  const int z = z0 + threadIdx.x, y = y0 + threadIdx.y;
+  if (z >= n || y >= n) return;
+  float v[10];
+#pragma unroll
+  for (int c = 0; c < 9; ++c) v[c] = sd[threadIdx.y + c / 3][threadIdx.x + c % 3];
+  v[9] = 0.0f;
+  const uint4 c0 = make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]), pack_bf16x2(v[4], v[5]),
+                              pack_bf16x2(v[6], v[7]));
+  const uint4 c1 = make_uint4(pack_bf16x2(v[8], v[9]), 0u, 0u, 0u);
+  store_voxel16(out, g, x, y, z, c0, c1);
+}
+
 // Gradient of the loss with respect to the field, as a BF16 tensor: channels 0-2 = s * dF, rest 0.
 __global__ void k_net_grad_input(const float4* __restrict__ df, float s, TensorGeo g, __nv_bfloat16* __restrict__ out) {
   const size_t m = (size_t)g.n * g.n * g.n;
@@ -712,7 +772,7 @@ size_t tensor_bytes(int n) { return (size_t)n * n * 2 * ((size_t)n + 8) * 8 * si
 
 void launch_conv(cpm_net* net, const CUtensorMap& in_map, int layer, bool transpose, __nv_bfloat16* out16,
                  float4* out_f4, const __nv_bfloat16* gate, int act, float out_scale, const float* out_scale_dev,
-                 cudaStream_t s) {
+                 cudaStream_t s, bool fold = false) {
   ConvArgs a;
   a.g = net->g;
   a.tiles_z = (net->n + TILE_M - 1) / TILE_M;
@@ -726,10 +786,15 @@ void launch_conv(cpm_net* net, const CUtensorMap& in_map, int layer, bool transp
   a.out_scale_dev = out_scale_dev;
   a.status = net_status(net);
   const size_t smem = conv_smem_bytes(CONV_SLOTS);
-  cudaFuncSetAttribute(k_conv3<CONV_SLOTS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const long long grid = std::min<long long>(a.tiles, sm_count());
   count_launch();
-  k_conv3<CONV_SLOTS><<<(unsigned)grid, FWD_THREADS, smem, s>>>(in_map, a);
+  if (fold) {
+    cudaFuncSetAttribute(k_conv3<CONV_SLOTS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_conv3<CONV_SLOTS, true><<<(unsigned)grid, FWD_THREADS, smem, s>>>(in_map, a);
+  } else {
+    cudaFuncSetAttribute(k_conv3<CONV_SLOTS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_conv3<CONV_SLOTS, false><<<(unsigned)grid, FWD_THREADS, smem, s>>>(in_map, a);
+  }
 }
 
 void launch_wgrad(cpm_net* net, const CUtensorMap& grad_map, const CUtensorMap& in_map, int layer, cudaStream_t s) {
@@ -797,13 +862,24 @@ int ensure_train(cpm_net* net) {
 }
 
 // Input tensor from delta (f32 mesh) or the fixed-point mass mesh, then the three layers into `field`.
+// fold (inference from the mass mesh): the first layer on the folded input; the training path keeps
+// the single-channel input, whose tensor the first layer's weight gradient reads.
 void net_forward_launch(cpm_net* net, const float* delta, const unsigned long long* fx, int fx_shift, float mean,
-                        float in_scale, float out_scale, const float* out_scale_dev, float4* field, cudaStream_t s) {
+                        float in_scale, float out_scale, const float* out_scale_dev, float4* field, cudaStream_t s,
+                        bool fold = false) {
   const size_t m = (size_t)net->n * net->n * net->n;
+  const int n = net->n;
   count_launch();
-  k_net_input<<<grid_1d(m), 256, 0, s>>>(delta, fx, std::ldexp(1.0f, -fx_shift), mean, in_scale, net->g,
-                                         static_cast<__nv_bfloat16*>(net->t_in.p));
-  launch_conv(net, net->map_in, 0, false, static_cast<__nv_bfloat16*>(net->t_a1.p), nullptr, nullptr, 1, 1.0f, nullptr, s);
+  if (fold && fx) {
+    k_net_input_fold<<<dim3((unsigned)((n + 31) / 32), (unsigned)((n + 7) / 8), (unsigned)n), dim3(32, 8), 0, s>>>(
+        fx, std::ldexp(1.0f, -fx_shift), mean, in_scale, net->g, static_cast<__nv_bfloat16*>(net->t_in.p));
+  } else {
+    fold = false;
+    k_net_input<<<grid_1d(m), 256, 0, s>>>(delta, fx, std::ldexp(1.0f, -fx_shift), mean, in_scale, net->g,
+                                           static_cast<__nv_bfloat16*>(net->t_in.p));
+  }
+  launch_conv(net, net->map_in, 0, false, static_cast<__nv_bfloat16*>(net->t_a1.p), nullptr, nullptr, 1, 1.0f, nullptr, s,
+              fold);
   launch_conv(net, net->map_a1, 1, false, static_cast<__nv_bfloat16*>(net->t_a2.p), nullptr, nullptr, 1, 1.0f, nullptr, s);
   launch_conv(net, net->map_a2, 2, false, nullptr, field, nullptr, 0, out_scale, out_scale_dev, s);
 }
@@ -833,7 +909,7 @@ namespace cpm {
 float4* net_field_from_mesh(cpm_net* net, const unsigned long long* fx, int fx_shift, float mean, float in_scale,
                             float out_scale, const float* out_scale_dev, cudaStream_t s) {
   float4* field = static_cast<float4*>(net->field.p);
-  net_forward_launch(net, nullptr, fx, fx_shift, mean, in_scale, out_scale, out_scale_dev, field, s);
+  net_forward_launch(net, nullptr, fx, fx_shift, mean, in_scale, out_scale, out_scale_dev, field, s, true);
   return field;
 }
 int net_mesh(const cpm_net* net) { return net ? net->n : 0; }

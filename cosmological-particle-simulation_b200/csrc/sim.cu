@@ -36,14 +36,13 @@
 
 #include "cpm_host.h"
 #include "cpm_internal.cuh"
+#include "tune_cache.h"
 
 using namespace cpm;
 
 namespace {
 constexpr int N_PHASES = 8;
 }
-
-constexpr int N_TUNE = 9;  // autotuner candidates: 3 FFT plans, 3 deposit tiles, 3 walk groups
 
 struct cpm_sim {
   cpm_sim_params P{};
@@ -266,45 +265,12 @@ static int sim_accelerations(cpm_sim* s, float a, const StepScalars* dev = nullp
 // quadrupoles) for the process, and in the file named by CPM_TUNE_CACHE when it is set (one line
 // per workload: key, plan, tile, warps). CPM_SIM_NO_AUTOTUNE keeps 8, 4 and 4.
 namespace {
-struct TuneChoice {
-  int radix = 8, ppt = 4, warps = 4;
-  float ms[N_TUNE] = {};  // plan 8, 4, 0; tile 512, 1024, 2048; warps 2, 4, 8
-};
 std::mutex g_tune_mu;
 std::map<std::string, TuneChoice> g_tune_cache;
 bool g_tune_file_read = false;
 
-std::string tune_key(const cpm_sim* s) {
-  char buf[160];
-  std::snprintf(buf, sizeof(buf), "n=%zu mesh=%d boxes=%d tree=%d quad=%d", per_box(s), s->P.mesh_n, s->nb,
-                s->P.use_tree, (s->P.flags & CPM_SIM_QUADRUPOLE) ? 1 : 0);
-  return buf;
-}
-
-void tune_file_load() {
-  g_tune_file_read = true;
-  const char* path = std::getenv("CPM_TUNE_CACHE");
-  if (!path) return;
-  FILE* f = std::fopen(path, "r");
-  if (!f) return;
-  char line[256];
-  while (std::fgets(line, sizeof(line), f)) {
-    const char* bar = std::strchr(line, '|');
-    if (!bar) continue;
-    TuneChoice c;
-    if (std::sscanf(bar + 1, "%d %d %d", &c.radix, &c.ppt, &c.warps) == 3)
-      g_tune_cache[std::string(line, (size_t)(bar - line))] = c;
-  }
-  std::fclose(f);
-}
-
-void tune_file_append(const std::string& key, const TuneChoice& c) {
-  const char* path = std::getenv("CPM_TUNE_CACHE");
-  if (!path) return;
-  FILE* f = std::fopen(path, "a");
-  if (!f) return;
-  std::fprintf(f, "%s|%d %d %d\n", key.c_str(), c.radix, c.ppt, c.warps);
-  std::fclose(f);
+std::string sim_tune_key(const cpm_sim* s) {
+  return cpm::tune_key(per_box(s), s->P.mesh_n, s->nb, s->P.use_tree, (s->P.flags & CPM_SIM_QUADRUPOLE) ? 1 : 0);
 }
 
 template <typename F>
@@ -335,14 +301,17 @@ static void apply_tuning(cpm_sim* s, const TuneChoice& c) {
 static void sim_apply_cached_tuning(cpm_sim* s) {
   if (s->P.flags & CPM_SIM_NO_AUTOTUNE) return;
   std::lock_guard<std::mutex> lock(g_tune_mu);
-  if (!g_tune_file_read) tune_file_load();
-  auto it = g_tune_cache.find(tune_key(s));
+  if (!g_tune_file_read) {
+    tune_file_load(std::getenv("CPM_TUNE_CACHE"), g_tune_cache);
+    g_tune_file_read = true;
+  }
+  auto it = g_tune_cache.find(sim_tune_key(s));
   if (it != g_tune_cache.end()) apply_tuning(s, it->second);
 }
 
 static int sim_autotune(cpm_sim* s) {
   if ((s->P.flags & CPM_SIM_NO_AUTOTUNE) || s->tuned) return CPM_OK;
-  const std::string key = tune_key(s);
+  const std::string key = sim_tune_key(s);
   const int radix_used = s->plan.max_radix;
   SIM_CU(s, cudaStreamSynchronize(s->stream));
   cudaEvent_t e0, e1;
@@ -354,47 +323,39 @@ static int sim_autotune(cpm_sim* s) {
   PoissonParams pp =
       make_poisson_params(mn, s->box, s->P.cosmo.omega_m, s->a, r_split, (s->P.flags & CPM_SIM_DECONVOLVE) ? 1 : 0);
   pp.boxes = s->nb;
-  const int radices[3] = {8, 4, 0};
-  float best = 1e30f;
   for (int k = 0; k < 3; ++k) {
-    s->plan.max_radix = radices[k];
+    s->plan.max_radix = TUNE_PLANS[k];
     c.ms[k] = time_ms(s->stream, e0, e1, [&] {
       launch_poisson(s->plan, pp, nullptr, as<unsigned long long>(s->fx), s->shift, s->mean, as<float2>(s->spec),
                      as<float>(s->gx), as<float>(s->gy), as<float>(s->gz), s->stream);
     });
-    if (c.ms[k] < best) best = c.ms[k], c.radix = radices[k];
   }
-  const int tiles[3] = {2, 4, 8};
-  best = 1e30f;
   for (int k = 0; k < 3; ++k) {
     c.ms[3 + k] = time_ms(s->stream, e0, e1, [&] {
       launch_deposit_fixed(as<float>(s->x), s->n, 1.0f, mn, s->h, s->shift, as<unsigned long long>(s->fx), s->stream,
-                           tiles[k], batch_box(s));
+                           TUNE_PPT[k], batch_box(s));
     });
-    if (c.ms[3 + k] < best) best = c.ms[3 + k], c.ppt = tiles[k];
   }
   if (s->P.use_tree && s->tree.geo.p && !(s->P.flags & CPM_SIM_QUADRUPOLE)) {
     int rc = ensure(s->host_tmp, 3 * s->n * sizeof(float)) == cudaSuccess ? CPM_OK : CPM_E_NOMEM;
     if (rc) return set_error(&s->err, rc, "autotune: scratch allocation failed");
     const float kk = tree_coupling(s->P.cosmo.omega_m, s->box, s->a, per_box(s));
-    const int warps[3] = {2, 4, 8};
-    best = 1e30f;
     for (int k = 0; k < 3; ++k) {
-      s->tree.walk_warps = warps[k];
+      s->tree.walk_warps = TUNE_WARPS[k];
       c.ms[6 + k] = time_ms(s->stream, e0, e1, [&] {
         launch_tree_walk(s->tree, as<float>(s->x), s->n, s->box, s->P.split, kk, as<float>(s->host_tmp), 0, nullptr,
                          as<DevStatus>(s->status), s->stream);
       });
-      if (c.ms[6 + k] < best) best = c.ms[6 + k], c.warps = warps[k];
     }
   }
+  tune_select(c);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   apply_tuning(s, c);
   {
     std::lock_guard<std::mutex> lock(g_tune_mu);
     g_tune_cache[key] = c;
-    tune_file_append(key, c);
+    tune_file_append(std::getenv("CPM_TUNE_CACHE"), key, c);
   }
   int rc = sim_check(s);
   // the first force evaluation ran with another radix plan: repeat it with the one kept
