@@ -25,7 +25,7 @@
 //
 // The Poisson solve runs as
 //   1. z pass: R2C of each z row; the input is the f32 delta or the u64 fixed-point mass mesh,
-//      converted in shared memory to delta = c/mean - 1 (integrator.rs:117-126);
+//      converted on load to delta = c/mean - 1 (integrator.rs:117-126);
 //   2. y pass: forward c2c along y;
 //   3. x pass: forward c2c along x, the Green's function of poisson.rs:52-74 in the reference's f32
 //      operation order (optionally divided by the CIC window squared), then two inverse x
@@ -548,61 +548,61 @@ __global__ void __launch_bounds__(T) k_fft_rows(float2* data, int rows, const fl
 
 // z pass, forward: TW real rows of length N -> N/2+1 complex each (rows of the padded half
 // spectrum), as an N/2-point complex transform of z[m] = x[2m] + i x[2m+1]. Input: f32 delta, or
-// the u64 fixed-point mass mesh (c = fx * 2^-k in f32, delta = c / mean - 1). The raw pairs land
-// in 16-byte slots of a staging buffer and are converted into the complex tile.
-// Shared memory: NBUF staging buffers of M*TLD 16-byte slots, then the M*TLD complex tile.
-template <int N, int NBUF, int T, int MR = 8>
+// the u64 fixed-point mass mesh (c = fx * 2^-k in f32, delta = c / mean - 1). Each thread loads its
+// input pairs straight into registers (16-byte loads of two u64 cells, all of a tile's loads issued
+// before any is used), converts them and writes the complex tile: shared memory holds only that
+// tile, so several CTAs per SM keep the loads of their tiles in flight.
+template <int N, int T, int MR = 8>
 __global__ void __launch_bounds__(T) k_r2c_z(const float* __restrict__ delta,
                                              const unsigned long long* __restrict__ fx, float inv_scale, float mean,
                                              float2* __restrict__ spec, int rows, const float2* __restrict__ tw) {
   extern __shared__ float2 smem[];
   constexpr int M = N / 2, NH = N / 2 + 1, NHP = N / 2 + 2;
-  float2* cplx = smem + NBUF * 2 * M * TLD;
-  pipeline<NBUF>(
-      smem, 2 * M * TLD, (rows + TW - 1) / TW,
-      [&](float2* buf, int tile) {
-        const int row0 = tile * TW, valid = min(TW, rows - row0);
-        for (int q = threadIdx.x; q < row_span<M>(M); q += T) {
-          const int m = row_t<M>(q), l = row_l<M>(q);
-          if (l >= valid || m >= M) continue;
-          const size_t gi = (size_t)(row0 + l) * N + 2 * m;
-          if (fx)
-            cp_async16(buf + 2 * (m * TLD + l), fx + gi);
-          else
-            cp_async8(buf + 2 * (m * TLD + l), delta + gi);
+  constexpr int SPAN = TW * ((M + 15) / 16) * 16;  // row_span<M>(M)
+  constexpr int PER = (SPAN + T - 1) / T;
+  float2* cplx = smem;
+  const int tiles = (rows + TW - 1) / TW;
+  for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const int row0 = tile * TW, valid = min(TW, rows - row0);
+    float2 v[PER];
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+      const int q = threadIdx.x + k * T;
+      const int m = row_t<M>(q), l = row_l<M>(q);
+      v[k] = make_float2(0.0f, 0.0f);
+      if (q < SPAN && l < valid && m < M) {
+        const size_t gi = (size_t)(row0 + l) * N + 2 * m;
+        if (fx) {
+          const ulonglong2 u = __ldg(reinterpret_cast<const ulonglong2*>(fx + gi));
+          const float c0 = __fmul_rn(__ull2float_rn(u.x), inv_scale);
+          const float c1 = __fmul_rn(__ull2float_rn(u.y), inv_scale);
+          v[k] = make_float2(__fsub_rn(__fdiv_rn(c0, mean), 1.0f), __fsub_rn(__fdiv_rn(c1, mean), 1.0f));
+        } else {
+          v[k] = __ldg(reinterpret_cast<const float2*>(delta + gi));
         }
-      },
-      [&](float2* raw, int tile) {
-        const int row0 = tile * TW, valid = min(TW, rows - row0);
-        for (int q = threadIdx.x; q < M * TW; q += T) {
-          const int l = q % TW, m = q / TW;
-          float2 v = make_float2(0.0f, 0.0f);
-          if (l < valid) {
-            if (fx) {
-              const ulonglong2 u = reinterpret_cast<const ulonglong2*>(raw)[m * TLD + l];
-              const float c0 = __fmul_rn(__ull2float_rn(u.x), inv_scale);
-              const float c1 = __fmul_rn(__ull2float_rn(u.y), inv_scale);
-              v = make_float2(__fsub_rn(__fdiv_rn(c0, mean), 1.0f), __fsub_rn(__fdiv_rn(c1, mean), 1.0f));
-            } else {
-              v = raw[2 * (m * TLD + l)];
-            }
-          }
-          cplx[m * TLD + l] = v;
-        }
-        __syncthreads();
-        fft_lines<M, false, T, 2, MR>(cplx, tw);
-        // X[k] = (Z[k] + conj(Z[M-k]))/2 + w^k (Z[k] - conj(Z[M-k]))/(2i), w = exp(-2 pi i / N)
-        for (int q = threadIdx.x; q < row_span<M>(NH); q += T) {
-          const int k = row_t<M>(q), l = row_l<M>(q);
-          if (l >= valid || k >= NH) continue;
-          // Z is M-periodic: Z[M] = Z[0] (k runs over 0..M)
-          const float2 zk = cplx[(k == M ? 0 : k) * TLD + l];
-          const float2 zm = cplx[(k == 0 ? 0 : M - k) * TLD + l];
-          const float2 fe = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
-          const float2 fo = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
-          spec[(size_t)(row0 + l) * NHP + k] = cadd(fe, cmul(__ldg(tw + k), fo));
-        }
-      });
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+      const int q = threadIdx.x + k * T;
+      const int m = row_t<M>(q), l = row_l<M>(q);
+      if (q < SPAN && m < M) cplx[m * TLD + l] = v[k];
+    }
+    __syncthreads();
+    fft_lines<M, false, T, 2, MR>(cplx, tw);
+    // X[k] = (Z[k] + conj(Z[M-k]))/2 + w^k (Z[k] - conj(Z[M-k]))/(2i), w = exp(-2 pi i / N)
+    for (int q = threadIdx.x; q < row_span<M>(NH); q += T) {
+      const int k = row_t<M>(q), l = row_l<M>(q);
+      if (l >= valid || k >= NH) continue;
+      // Z is M-periodic: Z[M] = Z[0] (k runs over 0..M)
+      const float2 zk = cplx[(k == M ? 0 : k) * TLD + l];
+      const float2 zm = cplx[(k == 0 ? 0 : M - k) * TLD + l];
+      const float2 fe = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+      const float2 fo = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+      spec[(size_t)(row0 + l) * NHP + k] = cadd(fe, cmul(__ldg(tw + k), fo));
+    }
+    __syncthreads();  // the next tile overwrites the complex tile
+  }
 }
 
 // z pass, inverse: N/2+1 complex per row -> N real values times scale, as an N/2-point complex
@@ -930,9 +930,7 @@ static void r2c3_n(const FftPlan& p, const float* delta, const unsigned long lon
   const int rows = N * N;
   {
     constexpr int T = threads_for<M>();
-    constexpr int NB = 2 * (4 * c_tile(M) + c_tile(M)) <= SMEM_LIMIT ? 2 : 1;  // two CTAs per SM
-    const size_t smem = (2 * NB + 1) * c_tile(M);
-    launch_persistent(k_r2c_z<N, NB, T>, T, smem, (rows + TW - 1) / TW, s, delta, fx, std::ldexp(1.0f, -fx_shift),
+    launch_persistent(k_r2c_z<N, T>, T, c_tile(M), (rows + TW - 1) / TW, s, delta, fx, std::ldexp(1.0f, -fx_shift),
                       mean, spec, rows, tw);
   }
   cols_pass<N>(spec, 0, 1, ColGeo{n * NHP, NHP, NH, 0, N}, 0, tw, s);  // y lines, outer = x
@@ -963,11 +961,9 @@ static void poisson_n(const FftPlan& p, const PoissonParams& pp, const float* de
     // Slot 0 holds the forward spectrum; the x pass reads each tile of it before writing the
     // same tile of slots 0..2, and tiles are disjoint, so the update in place is safe.
     float2* s0 = spec;
-    {  // 1. z: R2C into slot 0 (staging buffers of 16-byte slots + one complex tile)
+    {  // 1. z: R2C into slot 0 (one complex tile in shared memory per CTA)
       constexpr int T = threads_for<M, MR>();
-      constexpr int NB = 2 * (4 * c_tile(M) + c_tile(M)) <= SMEM_LIMIT ? 2 : 1;  // two CTAs per SM
-      const size_t smem = (2 * NB + 1) * c_tile(M);
-      launch_persistent(k_r2c_z<N, NB, T, MR>, T, smem, row_tiles, s, delta, fx, std::ldexp(1.0f, -fx_shift), mean, s0,
+      launch_persistent(k_r2c_z<N, T, MR>, T, c_tile(M), row_tiles, s, delta, fx, std::ldexp(1.0f, -fx_shift), mean, s0,
                         rows, tw);
     }
     // 2. y forward on slot 0: lines along y (stride NHP), columns along kz adjacent, outer = x
