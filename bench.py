@@ -518,6 +518,10 @@ def main() -> int:
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         ap.error("--warmup must be >= 3")
+    # The timed steps end at z = 0: a workload's schedule has steps_total steps (warm-up included).
+    total = ENSEMBLE["steps_total"] if args.workload == "ensemble" else WORKLOADS[args.workload]["steps_total"]
+    if args.impl == "ours" and not args.load_state and args.warmup + args.steps > total:
+        args.steps = max(1, total - args.warmup)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

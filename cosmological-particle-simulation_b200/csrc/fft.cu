@@ -442,22 +442,31 @@ __device__ __forceinline__ int row_span(int count) {
   return TT * TW * ((count + TT - 1) / TT);
 }
 
+// Column transfers: thread tid moves column l = tid % TW of rows t = tid / TW, tid / TW + T / TW, ...;
+// its global address advances by a fixed (T / TW) rows per step (T is a multiple of TW).
 template <int N, int T>
 __device__ __forceinline__ void async_load_cols(float2* buf, const float2* src, long long base, long long es,
                                                 int valid) {
-  for (int q = threadIdx.x; q < N * TW; q += T) {
-    const int l = q % TW, t = q / TW;
-    if (l < valid) cp_async8(buf + t * TLD + l, src + base + l + (long long)t * es);
-  }
+  static_assert(T % TW == 0, "whole rows per step");
+  constexpr int RS = T / TW;
+  const int l = threadIdx.x % TW;
+  if (l >= valid) return;
+  const float2* g = src + base + l + (long long)(threadIdx.x / TW) * es;
+  const long long step = (long long)RS * es;
+#pragma unroll 2
+  for (int t = threadIdx.x / TW; t < N; t += RS, g += step) cp_async8(buf + t * TLD + l, g);
 }
 
 template <int N, int T>
 __device__ __forceinline__ void store_cols(const float2* buf, float2* dst, long long base, long long es, int valid) {
-#pragma unroll 4
-  for (int q = threadIdx.x; q < N * TW; q += T) {
-    const int l = q % TW, t = q / TW;
-    if (l < valid) dst[base + l + (long long)t * es] = buf[t * TLD + l];
-  }
+  static_assert(T % TW == 0, "whole rows per step");
+  constexpr int RS = T / TW;
+  const int l = threadIdx.x % TW;
+  if (l >= valid) return;
+  float2* g = dst + base + l + (long long)(threadIdx.x / TW) * es;
+  const long long step = (long long)RS * es;
+#pragma unroll 2
+  for (int t = threadIdx.x / TW; t < N; t += RS, g += step) *g = buf[t * TLD + l];
 }
 
 // Persistent pipeline: each CTA walks tiles blockIdx.x, +gridDim.x, ...; with NBUF = 2 the next
