@@ -1129,7 +1129,8 @@ void orc_sim_last_timings(const orc_sim* s, double* t6) {
 
 void orc_step_sample(const orc_cosmology* c, float box, int mesh_n, const float* x3, const float* p3,
                      const float* acc3, size_t n, float a0, float a1, const orc_split* split,
-                     const uint32_t* subset, size_t m, int threads, double* t7, float* acc_subset) {
+                     const uint32_t* subset, size_t m, int threads, double* t7, float* acc_subset,
+                     float* acc_subset_com64) {
 #ifdef _OPENMP
   if (threads > 0) omp_set_num_threads(threads);
 #else
@@ -1178,6 +1179,7 @@ void orc_step_sample(const orc_cosmology* c, float box, int mesh_n, const float*
   if (acc_subset)  // the force evaluated at a1 for the sampled particles (outside the timed phases)
     for (size_t t = 0; t < m; ++t)
       for (int q = 0; q < 3; ++q) acc_subset[3 * t + q] = acc[3 * (size_t)subset[t] + q];
+
   const float k2 = kick_factor(*c, am, a1);
   kick(p.data(), acc.data(), n, k2);
   const double t7e = now_s();
@@ -1188,6 +1190,25 @@ void orc_step_sample(const orc_cosmology* c, float box, int mesh_n, const float*
   t7[4] = t5 - t4;
   t7[5] = t6 - t5;
   t7[6] = t7e - t6;
+  if (acc_subset_com64 && split) {  // the same force with FP64 centre-of-mass sums (after the timing)
+    Tree tree64;
+    tree64.com_f64 = 1;
+    tree64.build(x.data(), n, box);
+    const float L = box;
+    const float kc = 1.5f * c->omega_m * (L * L * L) / (4.0f * (float)3.14159265358979323846 * a1 * (float)n);
+#pragma omp parallel
+    {
+      std::vector<uint32_t> stack;
+#pragma omp for schedule(dynamic, 64)
+      for (long long t = 0; t < (long long)m; ++t) {
+        float sr[3];
+        const size_t i = subset[t];
+        tree64.accel_on(i, *split, kc, stack, sr, nullptr);
+        for (int q = 0; q < 3; ++q)  // the PM part of acc[i] (same f32 value), then the tree force
+          acc_subset_com64[3 * (size_t)t + q] = interpolate(mesh_n, box, g.data() + (size_t)q * mm, x.data() + 3 * i) + sr[q];
+      }
+    }
+  }
 }
 
 float orc_power(const orc_cosmology* c, const orc_pspec* ps, float k) { return power(*c, *ps, k); }

@@ -113,11 +113,14 @@ void orc_sim_last_timings(const orc_sim* s, double* t6);
  * at a0 -> a1, for the CPU baseline. Every phase runs on all n particles except the tree walk, which
  * runs for the m particles listed in `subset` (the caller scales it by n / m). The state is not
  * modified. t7 receives seconds for: kick+drift, deposit, Poisson, gather, tree build, walk of the
- * subset, second kick. `threads` > 0 sets the OpenMP thread count. */
+ * subset, second kick. `threads` > 0 sets the OpenMP thread count. acc_subset (may be NULL) receives
+ * the force at a1 (PM + tree) of the subset; acc_subset_com64 (may be NULL) the same with the tree's
+ * centres of mass summed in FP64 and rounded once (the diagnostic twin of tree_accelerations),
+ * computed outside the timed phases. */
 void orc_step_sample(const orc_cosmology* c, float box, int mesh_n, const float* x3, const float* p3,
                      const float* acc3, size_t n, float a0, float a1, const orc_split* split,
                      const uint32_t* subset, size_t m, int threads, double* t7,
-                     float* acc_subset);
+                     float* acc_subset, float* acc_subset_com64);
 
 /* ics.rs */
 float orc_power(const orc_cosmology* c, const orc_pspec* ps, float k);           /* :27-33 */

@@ -109,7 +109,7 @@ def lib() -> C.CDLL:
         "orc64_accelerations_ex": (None, [f32p, sz, C.c_double, i, C.c_double, C.c_double, C.c_void_p, C.c_double,
                                           u32p, sz, f64p, i]),
         "orc_step_sample": (None, [C.POINTER(Cosmology), fl, i, f32p, f32p, f32p, sz, fl, fl, C.c_void_p, u32p, sz,
-                                   i, f64p, C.c_void_p]),
+                                   i, f64p, C.c_void_p, C.c_void_p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -445,17 +445,22 @@ def num_threads() -> int:
 
 
 def step_sample(c: Cosmology, box: float, mesh_n: int, x, p, acc, a0: float, a1: float, split: Split | None,
-                subset, threads: int = 0, want_acc: bool = False):
+                subset, threads: int = 0, want_acc: bool = False, want_com64: bool = False):
     """Seconds of each phase of one reference KDK step on (x, p, acc); the walk runs for `subset` only.
     Returns [kick+drift, deposit, poisson, gather, tree build, walk(subset), second kick], and with
-    `want_acc` also the force at a1 (PM + tree) of the subset particles, shape (len(subset), 3)."""
+    `want_acc` also the force at a1 (PM + tree) of the subset particles, shape (len(subset), 3);
+    with `want_com64` as well the same force with FP64 centre-of-mass sums (untimed)."""
     x, p, acc = _f32(x), _f32(p), _f32(acc)
     sub = np.ascontiguousarray(subset, dtype=np.uint32)
     t = np.zeros(7, np.float64)
     out = np.empty((len(sub), 3), np.float32) if want_acc else None
+    out64 = np.empty((len(sub), 3), np.float32) if want_com64 else None
     lib().orc_step_sample(C.byref(c), box, mesh_n, x, p, acc, len(x), a0, a1,
                           C.cast(C.pointer(split), C.c_void_p) if split is not None else None, sub, len(sub),
-                          threads, t, out.ctypes.data if want_acc else None)
+                          threads, t, out.ctypes.data if want_acc else None,
+                          out64.ctypes.data if want_com64 else None)
+    if want_com64:
+        return t, out, out64
     return (t, out) if want_acc else t
 
 
