@@ -4,7 +4,9 @@
 // (integrator.rs:144-159). With a net attached to the simulation, the step instead
 //   1. gathers, per particle, with one CIC stencil (mesh.rs:29-77): the three PM force components
 //      (bit-identical to the plain gather), the density contrast delta_i from the fixed-point mass
-//      mesh (delta = c / mean - 1 per cell, integrator.rs:117-126) and the net's field F;
+//      mesh (delta = c / mean - 1 per cell as in integrator.rs:117-126, with the division by the mean
+//      taken as a product with its reciprocal: delta_i only selects the force model) and the net's
+//      field F;
 //      acc = g_pm + F where delta_i < threshold, acc = g_pm and flag_i = 1 elsewhere;
 //   2. compacts the flagged (dense) particles into a list that keeps the sorted order;
 //   3. walks the tree (tree.rs:264-310 rules, unchanged) for the listed particles only, adding
@@ -23,6 +25,7 @@ __global__ void k_learned_gather(const float* __restrict__ gx, const float* __re
   const float x[3] = {x3[3 * i], x3[3 * i + 1], x3[3 * i + 2]};
   CicBase c;
   cic_base(x, h, mesh_n, c);
+  const float inv_mean = 1.0f / mean;
   float sx = -0.0f, sy = -0.0f, sz = -0.0f, d = 0.0f;
   float fx0 = 0.0f, fy0 = 0.0f, fz0 = 0.0f;
 #pragma unroll
@@ -32,7 +35,8 @@ __global__ void k_learned_gather(const float* __restrict__ gx, const float* __re
     sx = __fadd_rn(sx, __fmul_rn(__ldg(gx + idx), w));
     sy = __fadd_rn(sy, __fmul_rn(__ldg(gy + idx), w));
     sz = __fadd_rn(sz, __fmul_rn(__ldg(gz + idx), w));
-    const float cell = __fsub_rn(__fdiv_rn(__fmul_rn(__ull2float_rn(__ldg(fx + idx)), inv_fx), mean), 1.0f);
+    // the cell's density contrast for the threshold test only (not a force term): c * (1 / mean) - 1
+    const float cell = __fmul_rn(__ull2float_rn(__ldg(fx + idx)), inv_fx) * inv_mean - 1.0f;
     d += w * cell;
     const float4 f = __ldg(field + idx);
     fx0 += w * f.x;
