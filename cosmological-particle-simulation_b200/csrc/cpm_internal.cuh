@@ -268,6 +268,15 @@ void launch_tree_walk(const TreeNodes& t, const float* sorted_x3, size_t n, floa
                       const float* k_dev = nullptr, const uint32_t* list = nullptr, const uint32_t* list_n = nullptr);
 // Releases the walk's per-tree state (the fitted pair-force coefficients).
 void tree_walk_free(TreeNodes& t);
+// Walk order (walk.cu): keys[i] = 24-bit Hilbert key of sorted particle i, idx[i] = i; sorted by
+// radix_sort_pairs over walk_order_key_bits() bits, idx is the order in which warps take particles.
+void launch_walk_order_keys(const float* sorted_x3, size_t n, float box, uint64_t* keys, uint32_t* idx,
+                            cudaStream_t s);
+int walk_order_key_bits();
+// list = the particles of `order` whose flag is set, in that order, and *count their number; fo and
+// offset are scratch of n words. With flag null only *count = n is set (the list is `order`).
+cudaError_t launch_ordered_list(const uint32_t* order, const uint32_t* flag, size_t n, uint32_t* fo, uint32_t* offset,
+                                uint32_t* list, uint32_t* count, DevBuf& scan_tmp, cudaStream_t s);
 
 // ---------------------------------------------------------------------------------------------
 // Particle updates — kdk.cu

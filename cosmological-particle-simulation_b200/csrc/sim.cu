@@ -86,6 +86,9 @@ struct cpm_sim {
   float net_threshold = 50.0f;
   float net_in_scale = 1.0f;
   DevBuf flag, offset, list, list_n, scan_tmp;
+  // The walk's particle order (Hilbert order of the sorted particles; single boxes): keys, the order,
+  // and the flags of the learned step in that order.
+  DevBuf wkeys, worder, wflag;
   // A batch of nb boxes of n_box particles each (the ensemble): particles box by box, nb meshes one
   // after another, the box index above `levels` octant digits in the sort keys. nb = 1: one box.
   int nb = 1;
@@ -226,14 +229,31 @@ static int sim_accelerations(cpm_sim* s, float a, const StepScalars* dev = nullp
     launch_learned_gather(as<float>(s->gx), as<float>(s->gy), as<float>(s->gz), as<unsigned long long>(s->fx),
                           s->shift, s->mean, field, as<float>(s->x), n, mn, s->h, s->net_threshold, as<float>(s->acc),
                           as<uint32_t>(s->flag), s->stream);
-    SIM_CU(s, launch_compact(as<uint32_t>(s->flag), as<uint32_t>(s->offset), n, as<uint32_t>(s->list),
-                             as<uint32_t>(s->list_n), s->scan_tmp, s->stream));
   } else {
     launch_interpolate3(as<float>(s->gx), as<float>(s->gy), as<float>(s->gz), as<float>(s->x), n, mn, s->h,
                         as<float>(s->acc), s->stream, batch_box(s));
   }
   mark(s, 5);
   if (s->P.use_tree) {
+    // The walk takes the particles in Hilbert order (a list over the sorted particles; single
+    // boxes): the dense ones of a learned step, or all of them.
+    const bool ordered = s->nb == 1;
+    if (ordered) {
+      SIM_CU(s, ensure(s->wkeys, n * sizeof(uint64_t)));
+      SIM_CU(s, ensure(s->worder, n * sizeof(uint32_t)));
+      SIM_CU(s, ensure(s->list_n, sizeof(uint32_t)));
+      launch_walk_order_keys(as<float>(s->x), n, s->box, as<uint64_t>(s->wkeys), as<uint32_t>(s->worder), s->stream);
+      SIM_CU(s, radix_sort_pairs(as<uint64_t>(s->wkeys), as<uint32_t>(s->worder), n, walk_order_key_bits(), s->sort,
+                                 s->stream));
+      SIM_CU(s, launch_ordered_list(as<uint32_t>(s->worder), learned ? as<uint32_t>(s->flag) : nullptr, n,
+                                    as<uint32_t>(s->wflag), as<uint32_t>(s->offset), as<uint32_t>(s->list),
+                                    as<uint32_t>(s->list_n), s->scan_tmp, s->stream));
+    } else if (learned) {
+      SIM_CU(s, launch_compact(as<uint32_t>(s->flag), as<uint32_t>(s->offset), n, as<uint32_t>(s->list),
+                               as<uint32_t>(s->list_n), s->scan_tmp, s->stream));
+    }
+    const uint32_t* walk_list = learned ? as<uint32_t>(s->list) : (ordered ? as<uint32_t>(s->worder) : nullptr);
+    const uint32_t* walk_n = (learned || ordered) ? as<uint32_t>(s->list_n) : nullptr;
     const float quad_half = (s->P.flags & CPM_SIM_QUADRUPOLE) ? quad_half_bound(s->P.split) : 0.0f;
     SIM_CU(s, tree_build(s->tree, as<uint64_t>(s->keys), as<float>(s->x), n, s->box, as<DevStatus>(s->status),
                          s->stream, quad_half, s->levels, batch_box(s)));
@@ -242,8 +262,7 @@ static int sim_accelerations(cpm_sim* s, float a, const StepScalars* dev = nullp
     const float k = tree_coupling(s->P.cosmo.omega_m, s->box, a, per_box(s));
     launch_tree_walk(s->tree, as<float>(s->x), n, s->box, s->P.split, k, as<float>(s->acc), 1,
                      as<TreeCounters>(s->counters), as<DevStatus>(s->status), s->stream,
-                     dev ? &dev->tree_k : nullptr, learned ? as<uint32_t>(s->list) : nullptr,
-                     learned ? as<uint32_t>(s->list_n) : nullptr);
+                     dev ? &dev->tree_k : nullptr, walk_list, walk_n);
   } else {
     mark(s, 6);
   }
@@ -340,11 +359,15 @@ static int sim_autotune(cpm_sim* s) {
     int rc = ensure(s->host_tmp, 3 * s->n * sizeof(float)) == cudaSuccess ? CPM_OK : CPM_E_NOMEM;
     if (rc) return set_error(&s->err, rc, "autotune: scratch allocation failed");
     const float kk = tree_coupling(s->P.cosmo.omega_m, s->box, s->a, per_box(s));
+    // the walk as the step runs it: in walk order (the first force evaluation left the list)
+    const bool learned = s->net != nullptr;
+    const uint32_t* wl = s->nb == 1 ? (learned ? as<uint32_t>(s->list) : as<uint32_t>(s->worder)) : nullptr;
+    const uint32_t* wn = s->nb == 1 ? as<uint32_t>(s->list_n) : nullptr;
     for (int k = 0; k < 3; ++k) {
       s->tree.walk_warps = TUNE_WARPS[k];
       c.ms[6 + k] = time_ms(s->stream, e0, e1, [&] {
         launch_tree_walk(s->tree, as<float>(s->x), s->n, s->box, s->P.split, kk, as<float>(s->host_tmp), 0, nullptr,
-                         as<DevStatus>(s->status), s->stream);
+                         as<DevStatus>(s->status), s->stream, nullptr, wl, wn);
       });
     }
   }
@@ -906,7 +929,7 @@ int cpm_sim_set_learned(cpm_sim* s, cpm_net* net, float delta_threshold, float i
   if (net && (!std::isfinite(delta_threshold) || !(in_scale > 0.0f) || !std::isfinite(in_scale)))
     return set_error(&s->err, CPM_E_INVALID, "cpm_sim_set_learned: threshold must be finite and in_scale > 0");
   if (net) {
-    for (DevBuf* b : {&s->flag, &s->offset, &s->list}) SIM_CU(s, ensure(*b, s->n * sizeof(uint32_t)));
+    for (DevBuf* b : {&s->flag, &s->offset, &s->list, &s->wflag}) SIM_CU(s, ensure(*b, s->n * sizeof(uint32_t)));
     SIM_CU(s, ensure(s->list_n, sizeof(uint32_t)));
     SIM_CU(s, cudaMemsetAsync(s->list_n.p, 0, sizeof(uint32_t), s->stream));
   }
@@ -993,7 +1016,7 @@ int cpm_sim_destroy(cpm_sim* s) {
                     &s->tree.mass, &s->tree.link, &s->tree.counters, &s->tree.prefix, &s->tree.scan_tmp, &s->tree.x4, &s->tree.quad, &s->x, &s->p,
                     &s->acc, &s->id, &s->x2, &s->p2, &s->id2, &s->keys, &s->vals, &s->fx, &s->gx, &s->gy, &s->gz,
                     &s->spec, &s->status, &s->counters, &s->pk, &s->q, &s->q2, &s->snap, &s->flag, &s->offset,
-                    &s->list, &s->list_n, &s->scan_tmp})
+                    &s->list, &s->list_n, &s->scan_tmp, &s->wkeys, &s->worder, &s->wflag})
     release(*b);
   tree_walk_free(s->tree);
   release(s->host_tmp);
