@@ -268,11 +268,12 @@ void launch_tree_walk(const TreeNodes& t, const float* sorted_x3, size_t n, floa
                       const float* k_dev = nullptr, const uint32_t* list = nullptr, const uint32_t* list_n = nullptr);
 // Releases the walk's per-tree state (the fitted pair-force coefficients).
 void tree_walk_free(TreeNodes& t);
-// Walk order (walk.cu): keys[i] = 24-bit Hilbert key of sorted particle i, idx[i] = i; sorted by
-// radix_sort_pairs over walk_order_key_bits() bits, idx is the order in which warps take particles.
+// Walk order (walk.cu): keys[i] = 24-bit Hilbert key of sorted particle i (with its box index above
+// it in a batch of boxes of n_box particles), idx[i] = i; sorted by radix_sort_pairs over
+// walk_order_key_bits(boxes) bits, idx is the order in which warps take particles.
 void launch_walk_order_keys(const float* sorted_x3, size_t n, float box, uint64_t* keys, uint32_t* idx,
-                            cudaStream_t s);
-int walk_order_key_bits();
+                            cudaStream_t s, size_t n_box = 0);
+int walk_order_key_bits(size_t boxes);
 // list = the particles of `order` whose flag is set, in that order, and *count their number; fo and
 // offset are scratch of n words. With flag null only *count = n is set (the list is `order`).
 cudaError_t launch_ordered_list(const uint32_t* order, const uint32_t* flag, size_t n, uint32_t* fo, uint32_t* offset,
@@ -358,8 +359,5 @@ int* net_status_word(cpm_net* net);
 void launch_learned_gather(const float* gx, const float* gy, const float* gz, const unsigned long long* fx, int shift,
                            float mean, const float4* field, const float* x3, size_t n, int mesh_n, float h,
                            float threshold, float* out3, uint32_t* flag, cudaStream_t s);
-// list = indices i with flag_i = 1 in increasing order, *count = their number (offset: scratch).
-cudaError_t launch_compact(const uint32_t* flag, uint32_t* offset, size_t n, uint32_t* list, uint32_t* count,
-                           DevBuf& scan_tmp, cudaStream_t s);
 
 }  // namespace cpm

@@ -235,25 +235,20 @@ static int sim_accelerations(cpm_sim* s, float a, const StepScalars* dev = nullp
   }
   mark(s, 5);
   if (s->P.use_tree) {
-    // The walk takes the particles in Hilbert order (a list over the sorted particles; single
-    // boxes): the dense ones of a learned step, or all of them.
-    const bool ordered = s->nb == 1;
-    if (ordered) {
-      SIM_CU(s, ensure(s->wkeys, n * sizeof(uint64_t)));
-      SIM_CU(s, ensure(s->worder, n * sizeof(uint32_t)));
-      SIM_CU(s, ensure(s->list_n, sizeof(uint32_t)));
-      launch_walk_order_keys(as<float>(s->x), n, s->box, as<uint64_t>(s->wkeys), as<uint32_t>(s->worder), s->stream);
-      SIM_CU(s, radix_sort_pairs(as<uint64_t>(s->wkeys), as<uint32_t>(s->worder), n, walk_order_key_bits(), s->sort,
-                                 s->stream));
-      SIM_CU(s, launch_ordered_list(as<uint32_t>(s->worder), learned ? as<uint32_t>(s->flag) : nullptr, n,
-                                    as<uint32_t>(s->wflag), as<uint32_t>(s->offset), as<uint32_t>(s->list),
-                                    as<uint32_t>(s->list_n), s->scan_tmp, s->stream));
-    } else if (learned) {
-      SIM_CU(s, launch_compact(as<uint32_t>(s->flag), as<uint32_t>(s->offset), n, as<uint32_t>(s->list),
-                               as<uint32_t>(s->list_n), s->scan_tmp, s->stream));
-    }
-    const uint32_t* walk_list = learned ? as<uint32_t>(s->list) : (ordered ? as<uint32_t>(s->worder) : nullptr);
-    const uint32_t* walk_n = (learned || ordered) ? as<uint32_t>(s->list_n) : nullptr;
+    // The walk takes the particles in Hilbert order (a list over the sorted particles; box by box
+    // in a batch): the dense ones of a learned step, or all of them.
+    SIM_CU(s, ensure(s->wkeys, n * sizeof(uint64_t)));
+    SIM_CU(s, ensure(s->worder, n * sizeof(uint32_t)));
+    SIM_CU(s, ensure(s->list_n, sizeof(uint32_t)));
+    launch_walk_order_keys(as<float>(s->x), n, s->box, as<uint64_t>(s->wkeys), as<uint32_t>(s->worder), s->stream,
+                           batch_box(s));
+    SIM_CU(s, radix_sort_pairs(as<uint64_t>(s->wkeys), as<uint32_t>(s->worder), n,
+                               walk_order_key_bits((size_t)s->nb), s->sort, s->stream));
+    SIM_CU(s, launch_ordered_list(as<uint32_t>(s->worder), learned ? as<uint32_t>(s->flag) : nullptr, n,
+                                  as<uint32_t>(s->wflag), as<uint32_t>(s->offset), as<uint32_t>(s->list),
+                                  as<uint32_t>(s->list_n), s->scan_tmp, s->stream));
+    const uint32_t* walk_list = learned ? as<uint32_t>(s->list) : as<uint32_t>(s->worder);
+    const uint32_t* walk_n = as<uint32_t>(s->list_n);
     const float quad_half = (s->P.flags & CPM_SIM_QUADRUPOLE) ? quad_half_bound(s->P.split) : 0.0f;
     SIM_CU(s, tree_build(s->tree, as<uint64_t>(s->keys), as<float>(s->x), n, s->box, as<DevStatus>(s->status),
                          s->stream, quad_half, s->levels, batch_box(s)));
@@ -361,8 +356,8 @@ static int sim_autotune(cpm_sim* s) {
     const float kk = tree_coupling(s->P.cosmo.omega_m, s->box, s->a, per_box(s));
     // the walk as the step runs it: in walk order (the first force evaluation left the list)
     const bool learned = s->net != nullptr;
-    const uint32_t* wl = s->nb == 1 ? (learned ? as<uint32_t>(s->list) : as<uint32_t>(s->worder)) : nullptr;
-    const uint32_t* wn = s->nb == 1 ? as<uint32_t>(s->list_n) : nullptr;
+    const uint32_t* wl = learned ? as<uint32_t>(s->list) : as<uint32_t>(s->worder);
+    const uint32_t* wn = as<uint32_t>(s->list_n);
     for (int k = 0; k < 3; ++k) {
       s->tree.walk_warps = TUNE_WARPS[k];
       c.ms[6 + k] = time_ms(s->stream, e0, e1, [&] {

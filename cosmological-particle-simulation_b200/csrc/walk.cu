@@ -440,7 +440,8 @@ __global__ void __launch_bounds__(WARPS * 32) k_tree_walk(const uint4* __restric
   // is copied into the other buffer while the current one is summed.
   // The walk starts at the root: node 0, or in a batch of boxes the root of the warp's box (nodes
   // 0 .. boxes - 1; a box's particles fill whole warps).
-  const uint32_t root = (!LIST && w.n_box) ? (uint32_t)(t / w.n_box) : 0u;
+  // (a list keeps each box's particles in whole warps: the first valid lane's box is the warp's)
+  const uint32_t root = w.n_box ? __shfl_sync(FULL, (uint32_t)(i / w.n_box), __ffs(group) - 1) : 0u;
   uint32_t b_count = 1, b_mask = group, b_first = root;
   int cur = 0;
   if (lane == 0) {
@@ -719,7 +720,9 @@ __device__ __forceinline__ uint32_t hilbert_key24(uint32_t a0, uint32_t a1, uint
   return key;
 }
 
-__global__ void k_walk_order_keys(const float* __restrict__ x3, size_t n, float cells_per_box,
+// In a batch of boxes (n_box particles each, box by box) the box index sits above the 24 key bits, so
+// the order keeps every box's particles together (whole warps: n_box is a multiple of 32).
+__global__ void k_walk_order_keys(const float* __restrict__ x3, size_t n, float cells_per_box, size_t n_box,
                                   uint64_t* __restrict__ keys, uint32_t* __restrict__ idx) {
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     uint32_t q[3];
@@ -729,19 +732,27 @@ __global__ void k_walk_order_keys(const float* __restrict__ x3, size_t n, float 
       constexpr float top = (float)((1u << WALK_ORDER_BITS) - 1);
       q[k] = f > 0.0f ? (f < top ? (uint32_t)f : (uint32_t)top) : 0u;
     }
-    keys[i] = hilbert_key24(q[0], q[1], q[2]);
+    const uint64_t boxi = n_box ? (uint64_t)(i / n_box) : 0ull;
+    keys[i] = (boxi << (3 * WALK_ORDER_BITS)) | hilbert_key24(q[0], q[1], q[2]);
     idx[i] = (uint32_t)i;
   }
 }
 
 void launch_walk_order_keys(const float* sorted_x3, size_t n, float box, uint64_t* keys, uint32_t* idx,
-                            cudaStream_t s) {
+                            cudaStream_t s, size_t n_box) {
   if (n == 0) return;
   count_launch();
   const unsigned blocks = (unsigned)std::min<size_t>((n + 255) / 256, 148 * 16);
-  k_walk_order_keys<<<blocks, 256, 0, s>>>(sorted_x3, n, (float)(1u << WALK_ORDER_BITS) / box, keys, idx);
+  k_walk_order_keys<<<blocks, 256, 0, s>>>(sorted_x3, n, (float)(1u << WALK_ORDER_BITS) / box, n_box, keys, idx);
 }
-int walk_order_key_bits() { return 3 * WALK_ORDER_BITS; }
+int walk_order_key_bits(size_t boxes) {
+  int b = 3 * WALK_ORDER_BITS;
+  while (boxes > 1) {
+    ++b;
+    boxes = (boxes + 1) / 2;
+  }
+  return b;
+}
 
 // list[t] = order[t] for the flagged particles, in walk order (the compaction of a flag over the
 // walk order); count = their number. offset = exclusive scan of flag[order[t]].
