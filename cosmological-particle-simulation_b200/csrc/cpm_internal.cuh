@@ -137,9 +137,11 @@ struct SortScratch {
 
 // Octant keys (tree.rs descent) of positions (AoS f32 or float4), values = 0..n-1.
 // With n_box > 0 (a batch of boxes of n_box particles each, in box order), the box index is placed
-// above the 3 * levels octant bits.
+// above the 3 * levels octant bits. With hkeys, also the Hilbert keys of the same cubes (the same
+// box bits): sorted by them, every octree node's particles stay contiguous.
 void launch_octant_keys(const float* x3, size_t n, float box, int levels, uint64_t* keys, uint32_t* vals,
-                        DevStatus* st, cudaStream_t s, size_t n_box = 0);
+                        DevStatus* st, cudaStream_t s, size_t n_box = 0, uint64_t* hkeys = nullptr);
+void launch_permute_u64(const uint64_t* in, const uint32_t* perm, size_t n, uint64_t* out, cudaStream_t s);
 // Stable LSD sort of the low `bits` bits of keys; result in keys/vals (ping-pong handled inside).
 cudaError_t radix_sort_pairs(uint64_t* keys, uint32_t* vals, size_t n, int bits, SortScratch& sc,
                              cudaStream_t s);
@@ -253,9 +255,12 @@ struct TreeCounters {
 // With n_box > 0 the keys hold a batch of boxes (box index above `levels` octant digits, boxes of
 // n_box particles in order): one root per box (nodes 0 .. boxes - 1), and the walk starts each
 // group of 32 particles at its box's root.
+// sorted_keys orders the particles: octant keys, or Hilbert keys (then octant_keys gives each
+// particle's octant key in the same order, from which a child's octant is read); a node's children
+// are stored in the order of its sort digits.
 cudaError_t tree_build(TreeNodes& t, const uint64_t* sorted_keys, const float* sorted_x3, size_t n, float box,
                        DevStatus* st, cudaStream_t s, float quad_half_max = 0.0f, int levels = KEY_LEVELS,
-                       size_t n_box = 0);
+                       size_t n_box = 0, const uint64_t* octant_keys = nullptr);
 // Half size from which a node can never be accepted by the walk (prune radius r_cut + sqrt(3) half
 // from the centre, centre of mass inside the cube, 2 half < theta r): +inf when theta >= 1/sqrt(3).
 float quad_half_bound(const cpm_force_split& split);
@@ -268,17 +273,6 @@ void launch_tree_walk(const TreeNodes& t, const float* sorted_x3, size_t n, floa
                       const float* k_dev = nullptr, const uint32_t* list = nullptr, const uint32_t* list_n = nullptr);
 // Releases the walk's per-tree state (the fitted pair-force coefficients).
 void tree_walk_free(TreeNodes& t);
-// Walk order (walk.cu): keys[i] = 24-bit Hilbert key of sorted particle i (with its box index above
-// it in a batch of boxes of n_box particles), idx[i] = i; sorted by radix_sort_pairs over
-// walk_order_key_bits(boxes) bits, idx is the order in which warps take particles.
-void launch_walk_order_keys(const float* sorted_x3, size_t n, float box, uint64_t* keys, uint32_t* idx,
-                            cudaStream_t s, size_t n_box = 0);
-int walk_order_key_bits(size_t boxes);
-// list = the particles of `order` whose flag is set, in that order, and *count their number; fo and
-// offset are scratch of n words. With flag null only *count = n is set (the list is `order`).
-cudaError_t launch_ordered_list(const uint32_t* order, const uint32_t* flag, size_t n, uint32_t* fo, uint32_t* offset,
-                                uint32_t* list, uint32_t* count, DevBuf& scan_tmp, cudaStream_t s);
-
 // ---------------------------------------------------------------------------------------------
 // Particle updates — kdk.cu
 // ---------------------------------------------------------------------------------------------
@@ -359,5 +353,8 @@ int* net_status_word(cpm_net* net);
 void launch_learned_gather(const float* gx, const float* gy, const float* gz, const unsigned long long* fx, int shift,
                            float mean, const float4* field, const float* x3, size_t n, int mesh_n, float h,
                            float threshold, float* out3, uint32_t* flag, cudaStream_t s);
+// list = indices i with flag_i = 1 in increasing order, *count = their number (offset: scratch).
+cudaError_t launch_compact(const uint32_t* flag, uint32_t* offset, size_t n, uint32_t* list, uint32_t* count,
+                           DevBuf& scan_tmp, cudaStream_t s);
 
 }  // namespace cpm

@@ -8,8 +8,8 @@
 //      taken as a product with its reciprocal: delta_i only selects the force model) and the net's
 //      field F;
 //      acc = g_pm + F where delta_i < threshold, acc = g_pm and flag_i = 1 elsewhere;
-//   2. (sim.cu, with walk.cu's helpers) lists the flagged (dense) particles in the walk's Hilbert
-//      order;
+//   2. compacts the flagged (dense) particles into a list that keeps the sorted order (a Hilbert
+//      order in a simulation);
 //   3. walks the tree (tree.rs:264-310 rules, unchanged) for the listed particles only, adding
 //      their short-range force to acc.
 #include "cpm_internal.cuh"
@@ -56,6 +56,14 @@ __global__ void k_learned_gather(const float* __restrict__ gx, const float* __re
   flag[i] = dense ? 1u : 0u;
 }
 
+__global__ void k_compact(const uint32_t* __restrict__ flag, const uint32_t* __restrict__ offset, size_t n,
+                          uint32_t* __restrict__ list, uint32_t* __restrict__ count) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (flag[i]) list[offset[i]] = (uint32_t)i;
+  if (i == n - 1) *count = offset[i] + flag[i];
+}
+
 void launch_learned_gather(const float* gx, const float* gy, const float* gz, const unsigned long long* fx, int shift,
                            float mean, const float4* field, const float* x3, size_t n, int mesh_n, float h,
                            float threshold, float* out3, uint32_t* flag, cudaStream_t s) {
@@ -63,6 +71,16 @@ void launch_learned_gather(const float* gx, const float* gy, const float* gz, co
   count_launch();
   k_learned_gather<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(gx, gy, gz, fx, ldexpf(1.0f, -shift), mean, field, x3,
                                                                n, mesh_n, h, threshold, out3, flag);
+}
+
+cudaError_t launch_compact(const uint32_t* flag, uint32_t* offset, size_t n, uint32_t* list, uint32_t* count,
+                           DevBuf& scan_tmp, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  cudaError_t e = exclusive_scan_u32(flag, offset, n, scan_tmp, s);
+  if (e != cudaSuccess) return e;
+  count_launch();
+  k_compact<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(flag, offset, n, list, count);
+  return cudaGetLastError();
 }
 
 }  // namespace cpm

@@ -86,9 +86,9 @@ struct cpm_sim {
   float net_threshold = 50.0f;
   float net_in_scale = 1.0f;
   DevBuf flag, offset, list, list_n, scan_tmp;
-  // The walk's particle order (Hilbert order of the sorted particles; single boxes): keys, the order,
-  // and the flags of the learned step in that order.
-  DevBuf wkeys, worder, wflag;
+  // Octant keys of the particles (the sort is by Hilbert keys in `keys`): as computed, and in the
+  // sorted order (the tree build reads each child's octant from them).
+  DevBuf okeys, okeys_sorted;
   // A batch of nb boxes of n_box particles each (the ensemble): particles box by box, nb meshes one
   // after another, the box index above `levels` octant digits in the sort keys. nb = 1: one box.
   int nb = 1;
@@ -193,9 +193,14 @@ static int sim_accelerations(cpm_sim* s, float a, const StepScalars* dev = nullp
   const size_t n = s->n;
   const int mn = s->P.mesh_n;
   mark(s, 1);
-  launch_octant_keys(as<float>(s->x), n, s->box, s->levels, as<uint64_t>(s->keys), as<uint32_t>(s->vals),
-                     as<DevStatus>(s->status), s->stream, batch_box(s));
+  // Hilbert order: sorting by the Hilbert keys of the octant cubes keeps every octree node's
+  // particles contiguous (the tree is the same), and the walk's groups of 32 consecutive particles
+  // are more compact than in octant order, so fewer sources lie in a group's reach but outside its
+  // particles' own.
+  launch_octant_keys(as<float>(s->x), n, s->box, s->levels, as<uint64_t>(s->okeys), as<uint32_t>(s->vals),
+                     as<DevStatus>(s->status), s->stream, batch_box(s), as<uint64_t>(s->keys));
   SIM_CU(s, radix_sort_pairs(as<uint64_t>(s->keys), as<uint32_t>(s->vals), n, 63, s->sort, s->stream));
+  launch_permute_u64(as<uint64_t>(s->okeys), as<uint32_t>(s->vals), n, as<uint64_t>(s->okeys_sorted), s->stream);
   launch_permute3(as<float>(s->x), as<uint32_t>(s->vals), n, as<float>(s->x2), s->stream);
   launch_permute3(as<float>(s->p), as<uint32_t>(s->vals), n, as<float>(s->p2), s->stream);
   launch_permute_u32(as<uint32_t>(s->id), as<uint32_t>(s->vals), n, as<uint32_t>(s->id2), s->stream);
@@ -235,23 +240,14 @@ static int sim_accelerations(cpm_sim* s, float a, const StepScalars* dev = nullp
   }
   mark(s, 5);
   if (s->P.use_tree) {
-    // The walk takes the particles in Hilbert order (a list over the sorted particles; box by box
-    // in a batch): the dense ones of a learned step, or all of them.
-    SIM_CU(s, ensure(s->wkeys, n * sizeof(uint64_t)));
-    SIM_CU(s, ensure(s->worder, n * sizeof(uint32_t)));
-    SIM_CU(s, ensure(s->list_n, sizeof(uint32_t)));
-    launch_walk_order_keys(as<float>(s->x), n, s->box, as<uint64_t>(s->wkeys), as<uint32_t>(s->worder), s->stream,
-                           batch_box(s));
-    SIM_CU(s, radix_sort_pairs(as<uint64_t>(s->wkeys), as<uint32_t>(s->worder), n,
-                               walk_order_key_bits((size_t)s->nb), s->sort, s->stream));
-    SIM_CU(s, launch_ordered_list(as<uint32_t>(s->worder), learned ? as<uint32_t>(s->flag) : nullptr, n,
-                                  as<uint32_t>(s->wflag), as<uint32_t>(s->offset), as<uint32_t>(s->list),
-                                  as<uint32_t>(s->list_n), s->scan_tmp, s->stream));
-    const uint32_t* walk_list = learned ? as<uint32_t>(s->list) : as<uint32_t>(s->worder);
-    const uint32_t* walk_n = as<uint32_t>(s->list_n);
+    if (learned)
+      SIM_CU(s, launch_compact(as<uint32_t>(s->flag), as<uint32_t>(s->offset), n, as<uint32_t>(s->list),
+                               as<uint32_t>(s->list_n), s->scan_tmp, s->stream));
+    const uint32_t* walk_list = learned ? as<uint32_t>(s->list) : nullptr;
+    const uint32_t* walk_n = learned ? as<uint32_t>(s->list_n) : nullptr;
     const float quad_half = (s->P.flags & CPM_SIM_QUADRUPOLE) ? quad_half_bound(s->P.split) : 0.0f;
     SIM_CU(s, tree_build(s->tree, as<uint64_t>(s->keys), as<float>(s->x), n, s->box, as<DevStatus>(s->status),
-                         s->stream, quad_half, s->levels, batch_box(s)));
+                         s->stream, quad_half, s->levels, batch_box(s), as<uint64_t>(s->okeys_sorted)));
     mark(s, 6);
     SIM_CU(s, cudaMemsetAsync(s->counters.p, 0, sizeof(TreeCounters), s->stream));
     const float k = tree_coupling(s->P.cosmo.omega_m, s->box, a, per_box(s));
@@ -354,10 +350,10 @@ static int sim_autotune(cpm_sim* s) {
     int rc = ensure(s->host_tmp, 3 * s->n * sizeof(float)) == cudaSuccess ? CPM_OK : CPM_E_NOMEM;
     if (rc) return set_error(&s->err, rc, "autotune: scratch allocation failed");
     const float kk = tree_coupling(s->P.cosmo.omega_m, s->box, s->a, per_box(s));
-    // the walk as the step runs it: in walk order (the first force evaluation left the list)
+    // the walk as the step runs it (a learned simulation's list from the first force evaluation)
     const bool learned = s->net != nullptr;
-    const uint32_t* wl = learned ? as<uint32_t>(s->list) : as<uint32_t>(s->worder);
-    const uint32_t* wn = as<uint32_t>(s->list_n);
+    const uint32_t* wl = learned ? as<uint32_t>(s->list) : nullptr;
+    const uint32_t* wn = learned ? as<uint32_t>(s->list_n) : nullptr;
     for (int k = 0; k < 3; ++k) {
       s->tree.walk_warps = TUNE_WARPS[k];
       c.ms[6 + k] = time_ms(s->stream, e0, e1, [&] {
@@ -424,6 +420,8 @@ static int sim_new(const cpm_sim_params* params, float a0, cpm_sim** out, int nb
   for (DevBuf* b : {&s->x, &s->p, &s->acc, &s->x2, &s->p2}) ok = ok && ensure(*b, 3 * n * sizeof(float)) == cudaSuccess;
   for (DevBuf* b : {&s->id, &s->id2, &s->vals}) ok = ok && ensure(*b, n * sizeof(uint32_t)) == cudaSuccess;
   ok = ok && ensure(s->keys, n * sizeof(uint64_t)) == cudaSuccess;
+  ok = ok && ensure(s->okeys, n * sizeof(uint64_t)) == cudaSuccess;
+  ok = ok && ensure(s->okeys_sorted, n * sizeof(uint64_t)) == cudaSuccess;
   ok = ok && ensure(s->fx, m * sizeof(unsigned long long)) == cudaSuccess;
   for (DevBuf* b : {&s->gx, &s->gy, &s->gz}) ok = ok && ensure(*b, m * sizeof(float)) == cudaSuccess;
   ok = ok && ensure(s->spec, 3 * half * (size_t)nb * sizeof(float2)) == cudaSuccess;
@@ -924,7 +922,7 @@ int cpm_sim_set_learned(cpm_sim* s, cpm_net* net, float delta_threshold, float i
   if (net && (!std::isfinite(delta_threshold) || !(in_scale > 0.0f) || !std::isfinite(in_scale)))
     return set_error(&s->err, CPM_E_INVALID, "cpm_sim_set_learned: threshold must be finite and in_scale > 0");
   if (net) {
-    for (DevBuf* b : {&s->flag, &s->offset, &s->list, &s->wflag}) SIM_CU(s, ensure(*b, s->n * sizeof(uint32_t)));
+    for (DevBuf* b : {&s->flag, &s->offset, &s->list}) SIM_CU(s, ensure(*b, s->n * sizeof(uint32_t)));
     SIM_CU(s, ensure(s->list_n, sizeof(uint32_t)));
     SIM_CU(s, cudaMemsetAsync(s->list_n.p, 0, sizeof(uint32_t), s->stream));
   }
@@ -1011,7 +1009,7 @@ int cpm_sim_destroy(cpm_sim* s) {
                     &s->tree.mass, &s->tree.link, &s->tree.counters, &s->tree.prefix, &s->tree.scan_tmp, &s->tree.x4, &s->tree.quad, &s->x, &s->p,
                     &s->acc, &s->id, &s->x2, &s->p2, &s->id2, &s->keys, &s->vals, &s->fx, &s->gx, &s->gy, &s->gz,
                     &s->spec, &s->status, &s->counters, &s->pk, &s->q, &s->q2, &s->snap, &s->flag, &s->offset,
-                    &s->list, &s->list_n, &s->scan_tmp, &s->wkeys, &s->worder, &s->wflag})
+                    &s->list, &s->list_n, &s->scan_tmp, &s->okeys, &s->okeys_sorted})
     release(*b);
   tree_walk_free(s->tree);
   release(s->host_tmp);

@@ -40,36 +40,91 @@ void release(DevBuf& b) {
 // With a batch of boxes (n_box > 0: particle i belongs to box i / n_box, boxes one after another),
 // the box index goes above the octant digits (bit `box_shift` up), so sorting keeps every box's
 // particles together and in box order.
+//
+// With hkeys, also the particle's Hilbert key over the same cubes: the octant digits are the bits of
+// integer coordinates (digit d holds bit levels-1-d of each axis), which J. Skilling's transform
+// of axes to the transposed Hilbert index ("Programming the Hilbert curve", AIP Conf. Proc. 707,
+// 381, 2004) maps to a key whose first 3d bits name the same level-d cube as the octant key's:
+// sorting by it keeps every octree node's particles contiguous and orders the nodes, and the
+// particles, along a Hilbert curve.
+__device__ __forceinline__ uint64_t hilbert_from_axes(uint32_t X0, uint32_t X1, uint32_t X2, int bits) {
+  uint32_t X[3] = {X0, X1, X2};
+  const uint32_t M = 1u << (bits - 1);
+  for (uint32_t Q = M; Q > 1; Q >>= 1) {  // undo excess work
+    const uint32_t P = Q - 1;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      if (X[i] & Q) {
+        X[0] ^= P;
+      } else {
+        const uint32_t t = (X[0] ^ X[i]) & P;
+        X[0] ^= t;
+        X[i] ^= t;
+      }
+    }
+  }
+  X[1] ^= X[0];  // Gray encode
+  X[2] ^= X[1];
+  uint32_t t = 0;
+  for (uint32_t Q = M; Q > 1; Q >>= 1)
+    if (X[2] & Q) t ^= Q - 1;
+  X[0] ^= t;
+  X[1] ^= t;
+  X[2] ^= t;
+  uint64_t key = 0;
+  for (int j = bits - 1; j >= 0; --j)
+    key = (key << 3) | (uint64_t)((((X[0] >> j) & 1u) << 2) | (((X[1] >> j) & 1u) << 1) | ((X[2] >> j) & 1u));
+  return key;
+}
+
 __global__ void k_octant_keys(const float* __restrict__ x3, size_t n, float half0, int levels,
                               uint64_t* __restrict__ keys, uint32_t* __restrict__ vals, DevStatus* st,
-                              size_t n_box, int box_shift) {
+                              size_t n_box, int box_shift, uint64_t* __restrict__ hkeys) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float p0 = x3[3 * i], p1 = x3[3 * i + 1], p2 = x3[3 * i + 2];
   if (!(isfinite(p0) && isfinite(p1) && isfinite(p2))) dev_fail(st, DEV_NONFINITE, (int)i);
   float half = half0, c0 = half0, c1 = half0, c2 = half0;
   uint64_t key = 0;
+  uint32_t a0 = 0, a1 = 0, a2 = 0;  // the digits' bits per axis
   for (int d = 0; d < levels; ++d) {
     const uint32_t o = (uint32_t)(p0 >= c0) | ((uint32_t)(p1 >= c1) << 1) | ((uint32_t)(p2 >= c2) << 2);
     key = (key << 3) | o;
+    a0 = (a0 << 1) | (o & 1u);
+    a1 = (a1 << 1) | ((o >> 1) & 1u);
+    a2 = (a2 << 1) | ((o >> 2) & 1u);
     const float q = half * 0.5f;  // == half / 2.0 exactly
     c0 = __fadd_rn(c0, (o & 1u) ? q : -q);
     c1 = __fadd_rn(c1, (o & 2u) ? q : -q);
     c2 = __fadd_rn(c2, (o & 4u) ? q : -q);
     half = q;
   }
-  if (n_box) key |= (uint64_t)(i / n_box) << box_shift;
-  keys[i] = key;
+  const uint64_t boxbits = n_box ? (uint64_t)(i / n_box) << box_shift : 0ull;
+  keys[i] = key | boxbits;
+  if (hkeys) hkeys[i] = hilbert_from_axes(a0, a1, a2, levels) | boxbits;
   if (vals) vals[i] = (uint32_t)i;
 }
 
 void launch_octant_keys(const float* x3, size_t n, float box, int levels, uint64_t* keys, uint32_t* vals,
-                        DevStatus* st, cudaStream_t s, size_t n_box) {
+                        DevStatus* st, cudaStream_t s, size_t n_box, uint64_t* hkeys) {
   if (n == 0) return;
   const int T = 256;
   count_launch();
   k_octant_keys<<<(unsigned)((n + T - 1) / T), T, 0, s>>>(x3, n, box / 2.0f, levels, keys, vals, st, n_box,
-                                                          3 * levels);
+                                                          3 * levels, hkeys);
+}
+
+__global__ void k_permute_u64(const uint64_t* __restrict__ in, const uint32_t* __restrict__ perm, size_t n,
+                              uint64_t* __restrict__ out) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = in[perm[i]];
+}
+
+void launch_permute_u64(const uint64_t* in, const uint32_t* perm, size_t n, uint64_t* out, cudaStream_t s) {
+  if (n == 0) return;
+  count_launch();
+  const unsigned blocks = (unsigned)std::min<size_t>((n + 255) / 256, 148 * 16);
+  k_permute_u64<<<blocks, 256, 0, s>>>(in, perm, n, out);
 }
 
 // ---------------------------------------------------------------------------------------------

@@ -1,12 +1,14 @@
 // tree.cu — octree build from sorted octant keys (tree.rs:171-250). The walk is in walk.cu.
 //
 // Build. Particles are sorted by their 63-bit octant key (21 digits of the reference's descent,
-// tree.rs:186-250), so every node of the reference's tree is a contiguous range of the sorted
-// array: the particles whose first d digits equal the node's prefix. One kernel per level splits
-// each node of that level that holds more than LEAF_SIZE particles: the 8 octant sub-ranges are
-// found on digit d+1 (sorted within the node: a thread per node on wide levels,
-// a warp per node on levels with few nodes), and the non-empty ones become
-// children, allocated contiguously in octant order. Node centres are built with the reference's
+// tree.rs:186-250), or by the Hilbert key of the same cubes (the simulation's order), so every
+// node of the reference's tree is a contiguous range of the sorted array: the particles whose
+// first d digits equal the node's prefix. One kernel per level splits each node of that level
+// that holds more than LEAF_SIZE particles: the 8 sub-ranges are found on digit d+1 (sorted
+// within the node: a thread per node on wide levels, a warp per node on levels with few nodes),
+// and the non-empty ones become children, allocated contiguously in digit order; a child's octant
+// (its centre, and the node's octant mask that the walk's children[0] rule reads) is the octant
+// digit of its first particle. Node centres are built with the reference's
 // f32 arithmetic (centre +- half/2), so they are bit-identical. A node deeper than the 21 key
 // digits that still holds more than LEAF_SIZE particles stays a leaf (the reference would keep
 // splitting to depth 40); such nodes are counted.
@@ -89,9 +91,12 @@ __device__ __forceinline__ uint32_t lower_bound_digit(const uint64_t* __restrict
 constexpr uint32_t SMALL_NODE = 256;
 constexpr uint32_t SCAN_NODE = 64;  // thread path: nodes up to this size count their digits
 
+// keys: the sort keys (octant or Hilbert digits split the node); okeys: the particles' octant keys
+// (a child's octant is the digit of its first particle; the same array as keys for octant order).
 __global__ void __launch_bounds__(BUILD_THREADS) k_tree_level(int d, int levels, const uint64_t* __restrict__ keys,
-                                                              uint4* link, float4* geo, uint32_t* counters,
-                                                              uint32_t capacity, DevStatus* st) {
+                                                              const uint64_t* __restrict__ okeys, uint4* link,
+                                                              float4* geo, uint32_t* counters, uint32_t capacity,
+                                                              DevStatus* st) {
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   uint32_t lb = 0;
@@ -146,6 +151,17 @@ __global__ void __launch_bounds__(BUILD_THREADS) k_tree_level(int d, int levels,
         for (int o = 0; o < 8; ++o)
           if (b[o + 1] > b[o]) mask |= 1u << o;
       }
+      // octant of each non-empty sub-range (its first particle's octant digit)
+      uint32_t octmask = 0, octs = 0;
+      if (split) {
+#pragma unroll
+        for (int o = 0; o < 8; ++o)
+          if (mask & (1u << o)) {
+            const uint32_t oc = okeys == keys ? (uint32_t)o : digit_at(__ldg(okeys + b[o]), shift);
+            octmask |= 1u << oc;
+            octs |= oc << (3 * o);
+          }
+      }
       // Children of the warp's nodes: an inclusive scan of their counts, one atomic by lane 31.
       const uint32_t nch = (uint32_t)__popc(mask);
       uint32_t incl = nch;
@@ -173,11 +189,12 @@ __global__ void __launch_bounds__(BUILD_THREADS) k_tree_level(int d, int levels,
       for (int o = 0; o < 8; ++o) {
         if (!(mask & (1u << o))) continue;
         const uint32_t child = first + r++;
+        const uint32_t oc = (octs >> (3 * o)) & 7u;
         link[child] = make_uint4(b[o], b[o + 1], 0u, 0u);
-        geo[child] = make_float4(__fadd_rn(G.x, (o & 1) ? q : -q), __fadd_rn(G.y, (o & 2) ? q : -q),
-                                 __fadd_rn(G.z, (o & 4) ? q : -q), q);
+        geo[child] = make_float4(__fadd_rn(G.x, (oc & 1) ? q : -q), __fadd_rn(G.y, (oc & 2) ? q : -q),
+                                 __fadd_rn(G.z, (oc & 4) ? q : -q), q);
       }
-      link[node] = make_uint4(s, e, first, mask | ((uint32_t)d << 8));
+      link[node] = make_uint4(s, e, first, octmask | ((uint32_t)d << 8));
     }
     return;
   }
@@ -231,17 +248,20 @@ __global__ void __launch_bounds__(BUILD_THREADS) k_tree_level(int d, int levels,
       }
       continue;
     }
-    if (lane < 8 && ((mask >> lane) & 1u)) {
+    // lane o: the octant of sub-range o (its first particle's octant digit)
+    const bool live = lane < 8 && ((mask >> lane) & 1u);
+    const uint32_t oc = !live ? 0u : (okeys == keys ? (uint32_t)lane : digit_at(__ldg(okeys + olo), shift));
+    const uint32_t octmask = __reduce_or_sync(FULL, live ? 1u << oc : 0u);
+    if (live) {
       const float4 G = geo[node];
       const float q = G.w * 0.5f;  // half / 2.0
-      const int o = lane;
-      const uint32_t child = first + (uint32_t)__popc(mask & ((1u << o) - 1u));
+      const uint32_t child = first + (uint32_t)__popc(mask & ((1u << lane) - 1u));
       link[child] = make_uint4(olo, ohi, 0u, 0u);
-      geo[child] = make_float4(__fadd_rn(G.x, (o & 1) ? q : -q), __fadd_rn(G.y, (o & 2) ? q : -q),
-                               __fadd_rn(G.z, (o & 4) ? q : -q), q);
+      geo[child] = make_float4(__fadd_rn(G.x, (oc & 1) ? q : -q), __fadd_rn(G.y, (oc & 2) ? q : -q),
+                               __fadd_rn(G.z, (oc & 4) ? q : -q), q);
     }
     if (lane == 0) {
-      link[node] = make_uint4(s, e, first, mask | ((uint32_t)d << 8));
+      link[node] = make_uint4(s, e, first, octmask | ((uint32_t)d << 8));
       atomicMax(&counters[CNT_MAX_DEPTH], (uint32_t)(d + 1));
     }
   }
@@ -400,7 +420,8 @@ __global__ void k_tree_quad(const uint4* __restrict__ link, const float4* __rest
 }
 
 cudaError_t tree_build(TreeNodes& t, const uint64_t* sorted_keys, const float* sorted_x3, size_t n, float box,
-                       DevStatus* st, cudaStream_t s, float quad_half_max, int levels, size_t n_box) {
+                       DevStatus* st, cudaStream_t s, float quad_half_max, int levels, size_t n_box,
+                       const uint64_t* octant_keys) {
   if (n == 0) return cudaSuccess;
   const size_t cap = 2 * n + 64;
   cudaError_t e;
@@ -423,8 +444,9 @@ cudaError_t tree_build(TreeNodes& t, const uint64_t* sorted_keys, const float* s
   k_tree_root<<<1, 256, 0, s>>>(link, geo, counters, (uint32_t)n, box / 2.0f, roots, (uint32_t)n_box);
   for (int d = 0; d <= levels; ++d) {
     count_launch();
-    k_tree_level<<<BUILD_BLOCKS, BUILD_THREADS, 0, s>>>(d, levels, sorted_keys, link, geo, counters,
-                                                        (uint32_t)t.capacity, st);
+    k_tree_level<<<BUILD_BLOCKS, BUILD_THREADS, 0, s>>>(d, levels, sorted_keys,
+                                                        octant_keys ? octant_keys : sorted_keys, link, geo,
+                                                        counters, (uint32_t)t.capacity, st);
   }
 
   D3* partial = as<D3>(t.scan_tmp);

@@ -679,115 +679,6 @@ __global__ void __launch_bounds__(WARPS * 32) k_tree_walk(const uint4* __restric
   }
 }
 
-// ------------------------------------------------------------------ walk order
-// The order in which warps take the particles: groups of 32 consecutive particles along a Hilbert
-// curve are more compact than along the octant (Morton) order of the tree, so fewer sources lie
-// within a group's reach but outside its particles' own. A particle's interactions do not depend on
-// its group (each lane applies the reference's tests for itself), only the order of its sums does.
-// Key: 8 bits per axis (cells of L/256) through J. Skilling's transform of axes to the transposed
-// Hilbert index ("Programming the Hilbert curve", AIP Conf. Proc. 707, 381, 2004), interleaved
-// into 24 bits; particles in one cell keep their octant order (the radix sort is stable).
-constexpr int WALK_ORDER_BITS = 8;
-
-__device__ __forceinline__ uint32_t hilbert_key24(uint32_t a0, uint32_t a1, uint32_t a2) {
-  uint32_t X[3] = {a0, a1, a2};
-  constexpr uint32_t M = 1u << (WALK_ORDER_BITS - 1);
-  for (uint32_t Q = M; Q > 1; Q >>= 1) {  // undo excess work
-    const uint32_t P = Q - 1;
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-      if (X[i] & Q) {
-        X[0] ^= P;
-      } else {
-        const uint32_t t = (X[0] ^ X[i]) & P;
-        X[0] ^= t;
-        X[i] ^= t;
-      }
-    }
-  }
-  X[1] ^= X[0];  // Gray encode
-  X[2] ^= X[1];
-  uint32_t t = 0;
-  for (uint32_t Q = M; Q > 1; Q >>= 1)
-    if (X[2] & Q) t ^= Q - 1;
-  X[0] ^= t;
-  X[1] ^= t;
-  X[2] ^= t;
-  uint32_t key = 0;
-#pragma unroll
-  for (int j = WALK_ORDER_BITS - 1; j >= 0; --j)
-    key = (key << 3) | (((X[0] >> j) & 1u) << 2) | (((X[1] >> j) & 1u) << 1) | ((X[2] >> j) & 1u);
-  return key;
-}
-
-// In a batch of boxes (n_box particles each, box by box) the box index sits above the 24 key bits, so
-// the order keeps every box's particles together (whole warps: n_box is a multiple of 32).
-__global__ void k_walk_order_keys(const float* __restrict__ x3, size_t n, float cells_per_box, size_t n_box,
-                                  uint64_t* __restrict__ keys, uint32_t* __restrict__ idx) {
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    uint32_t q[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      const float f = x3[3 * i + k] * cells_per_box;  // positions lie in [0, L]
-      constexpr float top = (float)((1u << WALK_ORDER_BITS) - 1);
-      q[k] = f > 0.0f ? (f < top ? (uint32_t)f : (uint32_t)top) : 0u;
-    }
-    const uint64_t boxi = n_box ? (uint64_t)(i / n_box) : 0ull;
-    keys[i] = (boxi << (3 * WALK_ORDER_BITS)) | hilbert_key24(q[0], q[1], q[2]);
-    idx[i] = (uint32_t)i;
-  }
-}
-
-void launch_walk_order_keys(const float* sorted_x3, size_t n, float box, uint64_t* keys, uint32_t* idx,
-                            cudaStream_t s, size_t n_box) {
-  if (n == 0) return;
-  count_launch();
-  const unsigned blocks = (unsigned)std::min<size_t>((n + 255) / 256, 148 * 16);
-  k_walk_order_keys<<<blocks, 256, 0, s>>>(sorted_x3, n, (float)(1u << WALK_ORDER_BITS) / box, n_box, keys, idx);
-}
-int walk_order_key_bits(size_t boxes) {
-  int b = 3 * WALK_ORDER_BITS;
-  while (boxes > 1) {
-    ++b;
-    boxes = (boxes + 1) / 2;
-  }
-  return b;
-}
-
-// list[t] = order[t] for the flagged particles, in walk order (the compaction of a flag over the
-// walk order); count = their number. offset = exclusive scan of flag[order[t]].
-__global__ void k_gather_flags(const uint32_t* __restrict__ order, const uint32_t* __restrict__ flag, size_t n,
-                               uint32_t* __restrict__ out) {
-  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x)
-    out[t] = flag[order[t]];
-}
-__global__ void k_compact_ordered(const uint32_t* __restrict__ order, const uint32_t* __restrict__ fo,
-                                  const uint32_t* __restrict__ offset, size_t n, uint32_t* __restrict__ list,
-                                  uint32_t* __restrict__ count) {
-  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x) {
-    if (fo[t]) list[offset[t]] = order[t];
-    if (t == n - 1) *count = offset[t] + fo[t];
-  }
-}
-__global__ void k_set_count(uint32_t* count, uint32_t v) { *count = v; }
-
-cudaError_t launch_ordered_list(const uint32_t* order, const uint32_t* flag, size_t n, uint32_t* fo, uint32_t* offset,
-                                uint32_t* list, uint32_t* count, DevBuf& scan_tmp, cudaStream_t s) {
-  const unsigned blocks = (unsigned)std::min<size_t>((n + 255) / 256, 148 * 16);
-  if (!flag) {  // every particle: the walk takes `order` itself as its list
-    count_launch();
-    k_set_count<<<1, 1, 0, s>>>(count, (uint32_t)n);
-    return cudaGetLastError();
-  }
-  count_launch();
-  k_gather_flags<<<blocks, 256, 0, s>>>(order, flag, n, fo);
-  cudaError_t e = exclusive_scan_u32(fo, offset, n, scan_tmp, s);
-  if (e != cudaSuccess) return e;
-  count_launch();
-  k_compact_ordered<<<blocks, 256, 0, s>>>(order, fo, offset, n, list, count);
-  return cudaGetLastError();
-}
-
 // Packs AoS positions into float4 (x, y, z, 0) for 16-byte loads.
 __global__ void k_pack4(const float* __restrict__ x3, size_t n, float4* __restrict__ x4) {
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
