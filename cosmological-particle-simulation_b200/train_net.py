@@ -18,7 +18,7 @@ tcgen05 tensor cores, Adam).
 
 The shipped weights (weights/short_range_net.npz) are the threshold-1 net: on held-out seed 2000 it
 keeps the final matter P(k) within 1 % of the plain run's for k <= k_Nyq/2 (0.4 % at 256^3, 0.7 % at
-128^3); nets for larger thresholds serve more particles and miss that bar (threshold 3: 5.3 %).
+128^3); nets for larger thresholds serve more particles and miss that bar (threshold 3: 5.1 %).
 """
 from __future__ import annotations
 

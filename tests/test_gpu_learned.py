@@ -11,8 +11,8 @@
   k <= k_Nyq/2, equal mode counts; median relative force error of the particles the net serves
   below 1e-2) and reports particle-steps/s of both. At this threshold the net serves the underdense
   particles only (half of them at z = 49, 7 % at z = 0), whose walks are cheap, so over a whole run
-  the learned step is slower than the plain one (0.89x at 256^3); thresholds that serve more particles
-  are faster and miss the bar (δ < 3: 1.18x at 256^3 with 5.3 % P(k) error).
+  the learned step is slower than the plain one (0.87x at 256^3); thresholds that serve more particles
+  are faster and miss the bar (δ < 3: 1.16x at 256^3 with 5.1 % P(k) error).
 """
 import math
 from pathlib import Path
