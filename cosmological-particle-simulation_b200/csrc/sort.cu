@@ -47,32 +47,32 @@ void release(DevBuf& b) {
 // 381, 2004) maps to a key whose first 3d bits name the same level-d cube as the octant key's:
 // sorting by it keeps every octree node's particles contiguous and orders the nodes, and the
 // particles, along a Hilbert curve.
-__device__ __forceinline__ uint64_t hilbert_from_axes(uint32_t X0, uint32_t X1, uint32_t X2, int bits) {
+template <int BITS>
+__device__ __forceinline__ uint64_t hilbert_from_axes(uint32_t X0, uint32_t X1, uint32_t X2) {
   uint32_t X[3] = {X0, X1, X2};
-  const uint32_t M = 1u << (bits - 1);
-  for (uint32_t Q = M; Q > 1; Q >>= 1) {  // undo excess work
-    const uint32_t P = Q - 1;
+#pragma unroll
+  for (int b = BITS - 1; b >= 1; --b) {  // undo excess work, Q = 2^b
+    const uint32_t Q = 1u << b, P = Q - 1;
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
-      if (X[i] & Q) {
-        X[0] ^= P;
-      } else {
-        const uint32_t t = (X[0] ^ X[i]) & P;
-        X[0] ^= t;
-        X[i] ^= t;
-      }
+      const uint32_t t = (X[0] ^ X[i]) & P;
+      const bool inv = (X[i] & Q) != 0u;
+      X[0] ^= inv ? P : t;  // invert the low bits of X[0], or exchange them with X[i]'s
+      if (i) X[i] ^= inv ? 0u : t;
     }
   }
   X[1] ^= X[0];  // Gray encode
   X[2] ^= X[1];
   uint32_t t = 0;
-  for (uint32_t Q = M; Q > 1; Q >>= 1)
-    if (X[2] & Q) t ^= Q - 1;
+#pragma unroll
+  for (int b = BITS - 1; b >= 1; --b)
+    if (X[2] & (1u << b)) t ^= (1u << b) - 1u;
   X[0] ^= t;
   X[1] ^= t;
   X[2] ^= t;
   uint64_t key = 0;
-  for (int j = bits - 1; j >= 0; --j)
+#pragma unroll
+  for (int j = BITS - 1; j >= 0; --j)
     key = (key << 3) | (uint64_t)((((X[0] >> j) & 1u) << 2) | (((X[1] >> j) & 1u) << 1) | ((X[2] >> j) & 1u));
   return key;
 }
@@ -101,7 +101,11 @@ __global__ void k_octant_keys(const float* __restrict__ x3, size_t n, float half
   }
   const uint64_t boxbits = n_box ? (uint64_t)(i / n_box) << box_shift : 0ull;
   keys[i] = key | boxbits;
-  if (hkeys) hkeys[i] = hilbert_from_axes(a0, a1, a2, levels) | boxbits;
+  if (hkeys) {
+    const uint64_t h = levels == KEY_LEVELS ? hilbert_from_axes<KEY_LEVELS>(a0, a1, a2)
+                                            : hilbert_from_axes<KEY_LEVELS - 2>(a0, a1, a2);
+    hkeys[i] = h | boxbits;
+  }
   if (vals) vals[i] = (uint32_t)i;
 }
 
