@@ -1,25 +1,28 @@
 // walk.cu — the short-range tree walk (tree.rs:264-323) and its pair kernel (tree.rs:54-66).
 //
-// Traversal. One warp walks for 32 consecutive sorted particles (one per lane). The unit of work
-// is a batch: the children of one opened node (contiguous in the node arrays), with the mask of
-// the lanes that opened it. Lanes c < count copy node c's three 16-byte records (centre and half,
-// centre of mass and mass, link) into shared memory with cp.async, double-buffered: the next
-// batch's copies are in flight while the current batch is summed. Lane c also derives the node's
-// constants once for the warp (prune radius squared, (2 half)^2), and a test against the bounding
-// box of the warp's particles drops nodes that every lane would prune. Every lane in the mask then
-// applies the reference's tests (tree.rs:264-310) to each remaining node for itself: prune when
+// Traversal. One warp walks for 32 consecutive sorted particles (one per lane). The stack holds
+// batches: the children of one opened node (contiguous in the node arrays), with the mask of the
+// lanes that opened it. The unit of work is a step of up to 32 nodes, one per lane: the top batch
+// and, while the stack is shallow (which bounds its depth), the batches below it as long as they
+// fit. Lane c copies node c's three 16-byte records (centre and half, centre of mass and mass,
+// link) into shared memory with cp.async, double-buffered: the next step's copies are in flight
+// while the current step is summed. Lane c also derives the node's constants once for the warp
+// (prune radius squared, (2 half)^2), and a test against the bounding box of the warp's particles
+// drops nodes that every lane would prune. Every lane then applies the reference's tests
+// (tree.rs:264-310), for itself, to each remaining node of the batches it opened: prune when
 // |min_image(centre - x)| > r_cut + sqrt(3) half; direct sum over the node's particles when its
 // octant-0 child is missing (`children[0] == NO_CHILD`, which includes leaves); else accept the
 // centre of mass when 2 half < theta |min_image(com - x)|, or open the node, which becomes a new
-// batch on a per-warp stack tagged with the lanes that opened it. A lane's set of interactions is
+// batch on the stack tagged with the lanes that opened it. A lane's set of interactions is
 // exactly the one its own reference walk visits: every decision uses separately rounded f32
-// operations and an exact minimum image (skipped for batches whose nodes are all far from the
+// operations and an exact minimum image (skipped for steps whose nodes are all far from the
 // box faces, where it is the identity), and the opening test, evaluated on squares, falls back to
 // the reference's square-root form whenever the two sides are within 1e-5; only the order in
 // which a lane adds its interactions differs.
 //
-// Direct sums concatenate the sources of all direct nodes of a batch into chunks of 32 (negated
-// positions, one array per axis, in shared memory). Per chunk a lane first marks the sources
+// Direct sums concatenate the sources of all direct nodes of a step into chunks of 32 (negated
+// positions, one array per axis, in shared memory); lane q finds the node of source base + q by a
+// binary search over the nodes' prefix sums. Per chunk a lane first marks the sources
 // within r_cut of it (bit mask; differences and squares two sources per f32x2 instruction, the
 // sums scalar so that r^2 rounds like the reference's), then evaluates the pair force only for
 // the marked ones, two per iteration in f32x2, so lanes do not idle on sources outside the cutoff
@@ -48,7 +51,13 @@
 namespace cpm {
 
 constexpr int WALK_WARPS = 4;
-constexpr int STACK_CAP = 8 * (KEY_LEVELS + 2);
+constexpr int SLOTS = 32;     // nodes per step of a warp's walk (one per lane)
+constexpr int MERGE_SP = 96;  // stack entries are merged into one step only while the stack is this shallow
+// Stack bound: a merging step starts at depth <= MERGE_SP and pushes at most SLOTS entries; from
+// there single-entry steps (depth first) keep at most 7 unvisited sibling entries per tree level
+// below, plus the 8 just pushed.
+constexpr int STACK_CAP = MERGE_SP + SLOTS + 7 * KEY_LEVELS + 8;
+constexpr uint32_t FIRST_BITS = 29;  // a stack entry: first node (29 bits) | (count - 1) << 29
 constexpr int FIT_DEG = 12;
 constexpr int FAR_PIECES_MAX = 8;
 constexpr double U_NEGLIGIBLE = 9.0;  // S(9) ~ 1e-34: contributions beyond are below f32 resolution
@@ -270,13 +279,15 @@ __device__ __forceinline__ bool accept_node_sq(float r2, const float4& pre, cons
 
 // Per-warp shared state of the walk.
 struct WalkShared {
-  uint2 stack[STACK_CAP];          // (first node, lane mask): a batch of sibling nodes ...
-  unsigned char count[STACK_CAP];  // ... and its node count
-  float4 geo[2][8];                // the current and the next batch: centre, half
-  float4 mass[2][8];               //                                 centre of mass, count
-  uint4 link[2][8];                //                                 start, end, first child, child mask
-  float4 pre[8];                   // per node of the current batch: prune radius^2, (2 half)^2,
+  uint2 stack[STACK_CAP];          // (first node | (count - 1) << 29, lane mask): a batch of siblings
+  float4 geo[2][SLOTS];            // the current and the next step's nodes: centre, half
+  float4 mass[2][SLOTS];           //                                        centre of mass, count
+  uint4 link[2][SLOTS];            //                                        start, end, first child, child mask
+  float4 pre[SLOTS];               // per node of the current step: prune radius^2, (2 half)^2,
                                    // 1e-5 (2 half)^2, 2 half
+  uint32_t dbeg[SLOTS], dend[SLOTS], dsrc[SLOTS];  // direct sums: node c's sources are positions
+                                                   // dbeg .. dend - 1 of the concatenation,
+                                                   // particles dsrc + (position - dbeg)
   float nx[32], ny[32], nz[32];    // a chunk of direct-sum sources, negated: -x, -y, -z
   float4 box_c, box_h;             // the warp's bounding box: centre, half extent (+ tolerance)
 };
@@ -397,7 +408,10 @@ __global__ void __launch_bounds__(WARPS * 32) k_tree_walk(const uint4* __restric
                                                             const uint32_t* __restrict__ list,
                                                             const uint32_t* __restrict__ list_n,
                                                             const float4* __restrict__ quad) {
-  __shared__ WalkShared shared[WARPS];
+  // Dynamic shared memory: WARPS WalkShared records, then (quadrupoles) the node index of each slot.
+  extern __shared__ __align__(16) unsigned char walk_smem[];
+  WalkShared* shared = reinterpret_cast<WalkShared*>(walk_smem);
+  uint32_t(*node_ids)[2][SLOTS] = reinterpret_cast<uint32_t(*)[2][SLOTS]>(walk_smem + WARPS * sizeof(WalkShared));
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   // Lane t of the grid walks for sorted particle t, or, with a list, for particle list[t] (t below
@@ -435,19 +449,21 @@ __global__ void __launch_bounds__(WARPS * 32) k_tree_walk(const uint4* __restric
   float2 A0 = make_float2(0.0f, 0.0f), A1 = A0, A2 = A0;
   uint32_t n_pairs = 0, n_accepts = 0, n_cand = 0;
 
-  // The current batch: sibling nodes first .. first + count - 1, walked by the lanes in mask.
-  // Lane c < count copies node first + c into shared buffer `cur` asynchronously; the next batch
-  // is copied into the other buffer while the current one is summed.
-  // The walk starts at the root: node 0, or in a batch of boxes the root of the warp's box (nodes
-  // 0 .. boxes - 1; a box's particles fill whole warps).
-  // (a list keeps each box's particles in whole warps: the first valid lane's box is the warp's)
+  // A step of the walk handles up to SLOTS nodes, one per lane: one or more stack entries (each the
+  // children of an opened node, with the mask of the lanes that opened it) placed in consecutive
+  // slots. `mine` holds the slots this lane walks. Lane c copies slot c's three records into shared
+  // buffer `cur` asynchronously; the next step's copies are in flight while the current step is
+  // summed. The walk starts at the root: node 0, or in a batch of boxes the root of the warp's box
+  // (nodes 0 .. boxes - 1; a box's particles fill whole warps, and a list keeps each box's
+  // particles in whole warps, so the first valid lane's box is the warp's).
   const uint32_t root = w.n_box ? __shfl_sync(FULL, (uint32_t)(i / w.n_box), __ffs(group) - 1) : 0u;
-  uint32_t b_count = 1, b_mask = group, b_first = root;
+  uint32_t b_count = 1, mine = (group >> lane) & 1u;
   int cur = 0;
   if (lane == 0) {
     cp_async16(&sh.geo[0][0], geo + root);
     cp_async16(&sh.mass[0][0], mass + root);
     cp_async16(&sh.link[0][0], link + root);
+    if constexpr (QUAD) node_ids[warp][0][0] = root;
   }
   int sp = 0;
   for (;;) {
@@ -485,56 +501,57 @@ __global__ void __launch_bounds__(WARPS * 32) k_tree_walk(const uint4* __restric
     const uint32_t dbits = __ballot_sync(FULL, direct);
     __syncwarp();
 
-    // Classify every remaining node of the batch for this lane: prune, direct sum, accept or open.
+    // Classify every remaining node of this lane for its particle: prune, direct sum, accept or open.
     uint32_t dmask = 0, nwmask = 0, amask = 0, omask = 0;
-    if ((b_mask >> lane) & 1u) {
-      if ((cand & ~nwall) == 0u) {
-        // No node of the batch involves a periodic image: raw differences.
-        for (uint32_t rem = cand; rem; rem &= rem - 1) {
-          const uint32_t c = __ffs(rem) - 1;
-          const float4 G = bgeo[c], P = sh.pre[c];
-          const float t0 = __fsub_rn(G.x, x0), t1 = __fsub_rn(G.y, x1), t2 = __fsub_rn(G.z, x2);
-          if (norm2(t0, t1, t2) > P.x) continue;
-          if ((dbits >> c) & 1u) {
-            dmask |= 1u << c;
-            continue;
-          }
-          const float4 M = bmass[c];
-          const float s0 = __fsub_rn(M.x, x0), s1 = __fsub_rn(M.y, x1), s2 = __fsub_rn(M.z, x2);
-          if (accept_node_sq(norm2(s0, s1, s2), P, w))
-            amask |= 1u << c;
-          else
-            omask |= 1u << c;
+    const uint32_t todo = cand & mine;
+    if ((todo & ~nwall) == 0u) {
+      // No node of the step involves a periodic image: raw differences.
+      for (uint32_t rem = todo; rem; rem &= rem - 1) {
+        const uint32_t c = __ffs(rem) - 1;
+        const float4 G = bgeo[c], P = sh.pre[c];
+        const float t0 = __fsub_rn(G.x, x0), t1 = __fsub_rn(G.y, x1), t2 = __fsub_rn(G.z, x2);
+        if (norm2(t0, t1, t2) > P.x) continue;
+        if ((dbits >> c) & 1u) {
+          dmask |= 1u << c;
+          continue;
         }
-        nwmask = dmask;
-      } else {
-        for (uint32_t rem = cand; rem; rem &= rem - 1) {
-          const uint32_t c = __ffs(rem) - 1;
-          const float4 G = bgeo[c], P = sh.pre[c];
-          float t0 = __fsub_rn(G.x, x0), t1 = __fsub_rn(G.y, x1), t2 = __fsub_rn(G.z, x2);
-          // every source y of the node lies in [centre - half, centre + half]
-          const bool nowrap = fmaxf(fabsf(t0), fmaxf(fabsf(t1), fabsf(t2))) + G.w < w.guard;
-          min_image3(t0, t1, t2, w);
-          if (norm2(t0, t1, t2) > P.x) continue;
-          if ((dbits >> c) & 1u) {
-            // children[0] == NO_CHILD: direct sum over the node's particles (tree.rs:286-298)
-            dmask |= 1u << c;
-            nwmask |= (uint32_t)nowrap << c;
-            continue;
-          }
-          const float4 M = bmass[c];
-          float s0 = __fsub_rn(M.x, x0), s1 = __fsub_rn(M.y, x1), s2 = __fsub_rn(M.z, x2);
-          min_image3(s0, s1, s2, w);
-          if (accept_node_sq(norm2(s0, s1, s2), P, w))
-            amask |= 1u << c;
-          else
-            omask |= 1u << c;
+        const float4 M = bmass[c];
+        const float s0 = __fsub_rn(M.x, x0), s1 = __fsub_rn(M.y, x1), s2 = __fsub_rn(M.z, x2);
+        if (accept_node_sq(norm2(s0, s1, s2), P, w))
+          amask |= 1u << c;
+        else
+          omask |= 1u << c;
+      }
+      nwmask = dmask;
+    } else {
+      for (uint32_t rem = todo; rem; rem &= rem - 1) {
+        const uint32_t c = __ffs(rem) - 1;
+        const float4 G = bgeo[c], P = sh.pre[c];
+        float t0 = __fsub_rn(G.x, x0), t1 = __fsub_rn(G.y, x1), t2 = __fsub_rn(G.z, x2);
+        // every source y of the node lies in [centre - half, centre + half]
+        const bool nowrap = fmaxf(fabsf(t0), fmaxf(fabsf(t1), fabsf(t2))) + G.w < w.guard;
+        min_image3(t0, t1, t2, w);
+        if (norm2(t0, t1, t2) > P.x) continue;
+        if ((dbits >> c) & 1u) {
+          // children[0] == NO_CHILD: direct sum over the node's particles (tree.rs:286-298)
+          dmask |= 1u << c;
+          nwmask |= (uint32_t)nowrap << c;
+          continue;
         }
+        const float4 M = bmass[c];
+        float s0 = __fsub_rn(M.x, x0), s1 = __fsub_rn(M.y, x1), s2 = __fsub_rn(M.z, x2);
+        min_image3(s0, s1, s2, w);
+        if (accept_node_sq(norm2(s0, s1, s2), P, w))
+          amask |= 1u << c;
+        else
+          omask |= 1u << c;
       }
     }
 
-    // Push the opened nodes' children as new batches (any order: contributions are summed per
-    // lane, and the set of interactions of each lane does not depend on the traversal order).
+    // Push the opened nodes' children as new stack entries (any order gives each lane the same
+    // set of interactions; only the order of its sums differs). Higher slots go deeper into the
+    // stack, so that the entries popped first, which fill the lowest slots, have their children
+    // popped first again.
     const uint32_t ouni = __reduce_or_sync(FULL, omask);
     if (ouni) {
       uint32_t opened_by = 0;
@@ -544,33 +561,39 @@ __global__ void __launch_bounds__(WARPS * 32) k_tree_walk(const uint4* __restric
         if (lane == c) opened_by = b;
       }
       const int npush = __popc(ouni);
-      if (sp + npush > STACK_CAP) {
+      // (node indices above 29 bits, trees of more than 2^28 particles, do not fit an entry)
+      const bool wide = __any_sync(FULL, ((ouni >> lane) & 1u) && (blink[lane].z >> FIRST_BITS) != 0u);
+      if (sp + npush > STACK_CAP || wide) {
         if (lane == 0) dev_fail(st, DEV_STACK_OVERFLOW, sp);
         break;
       }
       if ((ouni >> lane) & 1u) {
         const uint4 L = blink[lane];
-        const int slot = sp + __popc(ouni & ((1u << lane) - 1u));
-        sh.stack[slot] = make_uint2(L.z, opened_by);
-        sh.count[slot] = (unsigned char)__popc(L.w & 0xFFu);
+        const int slot = sp + __popc(ouni >> lane) - 1;
+        sh.stack[slot] = make_uint2(L.z | ((uint32_t)(__popc(L.w & 0xFFu) - 1) << FIRST_BITS), opened_by);
       }
       sp += npush;
       __syncwarp();
     }
 
-    // Start copying the next batch; the copies complete during the work below.
-    const bool more = sp > 0;
-    uint32_t nx_count = 0, nx_mask = 0, nx_first = 0;
-    if (more) {
-      const uint2 top = sh.stack[--sp];
-      const uint32_t first = top.x;
-      nx_first = first;
-      nx_count = sh.count[sp];
-      nx_mask = top.y;
-      if ((uint32_t)lane < nx_count) {
-        cp_async16(&sh.geo[cur ^ 1][lane], geo + first + lane);
-        cp_async16(&sh.mass[cur ^ 1][lane], mass + first + lane);
-        cp_async16(&sh.link[cur ^ 1][lane], link + first + lane);
+    // Pop the next step: the top entry, and while the stack is shallow, further entries as long as
+    // they fit in the slots. Its copies complete during the work below.
+    uint32_t nx_count = 0, nx_mine = 0;
+    if (sp > 0) {
+      const bool merge = sp <= MERGE_SP;
+      for (;;) {
+        const uint2 e = sh.stack[--sp];
+        const uint32_t first = e.x & ((1u << FIRST_BITS) - 1u), cnt = (e.x >> FIRST_BITS) + 1u;
+        if ((uint32_t)lane >= nx_count && (uint32_t)lane < nx_count + cnt) {
+          const uint32_t node = first + ((uint32_t)lane - nx_count);
+          cp_async16(&sh.geo[cur ^ 1][lane], geo + node);
+          cp_async16(&sh.mass[cur ^ 1][lane], mass + node);
+          cp_async16(&sh.link[cur ^ 1][lane], link + node);
+          if constexpr (QUAD) node_ids[warp][cur ^ 1][lane] = node;
+        }
+        if ((e.y >> lane) & 1u) nx_mine |= bit_span(nx_count, cnt);
+        nx_count += cnt;
+        if (!merge || sp == 0 || nx_count + (sh.stack[sp - 1].x >> FIRST_BITS) + 1u > (uint32_t)SLOTS) break;
       }
     }
 
@@ -585,56 +608,78 @@ __global__ void __launch_bounds__(WARPS * 32) k_tree_walk(const uint4* __restric
       A1.x = fmaf(-s1, f, A1.x);
       A2.x = fmaf(-s2, f, A2.x);
       if constexpr (QUAD) {
-        const size_t node = (size_t)b_first + (size_t)c;
+        const size_t node = node_ids[warp][cur][c];
         quad_term(s0, s1, s2, __ldg(quad + 2 * node), __ldg(quad + 2 * node + 1), w, A0, A1, A2);
       }
       ++n_accepts;
     }
 
-    // Direct sums: the sources of all direct nodes of the batch, concatenated in chunks of 32.
+    // Direct sums: the sources of all direct nodes of the step, concatenated in slot order, in
+    // chunks of 32.
     const uint32_t dset = __reduce_or_sync(FULL, dmask);
     if (dset) {
-      uint32_t total = 0;
-      for (uint32_t rem = dset; rem; rem &= rem - 1) {
-        const uint4 L = blink[__ffs(rem) - 1];
-        const uint32_t cnt = L.y - L.x;
-        total += cnt;
-        if ((dmask >> (__ffs(rem) - 1)) & 1u) n_cand += cnt;
+      uint32_t cnt = 0, first = 0;
+      if ((dset >> lane) & 1u) {
+        const uint4 L = blink[lane];
+        cnt = L.y - L.x;
+        first = L.x;
+      }
+      uint32_t end = cnt;  // inclusive prefix sum over the slots
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(FULL, end, o);
+        if (lane >= o) end += v;
+      }
+      sh.dbeg[lane] = end - cnt;
+      sh.dend[lane] = end;
+      sh.dsrc[lane] = first;
+      const uint32_t total = __shfl_sync(FULL, end, 31);
+      __syncwarp();
+      // This lane's candidates, and its own particle's position in the concatenation (j != i).
+      uint32_t selfpos = 0xffffffffu;
+      for (uint32_t rem = dmask; rem; rem &= rem - 1) {
+        const int c = __ffs(rem) - 1;
+        const uint32_t b0 = sh.dbeg[c], e0 = sh.dend[c], f0 = sh.dsrc[c];
+        n_cand += e0 - b0;
+        if (self - f0 < e0 - b0) selfpos = b0 + (self - f0);
       }
       const bool wrap = (dmask & ~nwmask) != 0u;
+      uint32_t open_d = dmask;  // this lane's direct nodes not yet wholly behind the current chunk
       for (uint32_t base = 0; base < total; base += 32) {
-        // Lane q loads source base + q of the concatenation; `live` gets the chunk positions of
-        // the nodes this lane sums directly, without the lane's own particle (j != i).
+        // Lane q loads source base + q: node c, the last with dbeg <= base + q (binary search).
         const uint32_t g = base + (uint32_t)lane;
-        uint32_t live = 0, selfbit = 0, off = 0;
-        for (uint32_t rem = dset; rem && off < base + 32u; rem &= rem - 1) {
-          const int c = __ffs(rem) - 1;
-          const uint4 L = blink[c];
-          const uint32_t cnt = L.y - L.x;
-          if (g >= off && g < off + cnt) {
-            const float4 y = __ldg(x4 + L.x + (g - off));
-            sh.nx[lane] = -y.x;
-            sh.ny[lane] = -y.y;
-            sh.nz[lane] = -y.z;
-          }
-          const uint32_t lo = max(off, base), hi = min(off + cnt, base + 32u);
-          if (((dmask >> c) & 1u) && lo < hi) live |= bit_span(lo - base, hi - lo);
-          if (self >= L.x && self < L.y) {
-            const uint32_t gs = off + (self - L.x);
-            if (gs >= base && gs < base + 32u) selfbit = 1u << (gs - base);
-          }
-          off += cnt;
+        if (g < total) {
+          int c = 0;
+#pragma unroll
+          for (int step = 16; step > 0; step >>= 1)
+            if (sh.dend[c + step - 1] <= g) c += step;
+          const float4 y = __ldg(x4 + sh.dsrc[c] + (g - sh.dbeg[c]));
+          sh.nx[lane] = -y.x;
+          sh.ny[lane] = -y.y;
+          sh.nz[lane] = -y.z;
         }
-        live &= ~selfbit;
+        // `live`: the chunk positions of this lane's direct nodes, without its own particle.
+        const uint32_t top = base + 32u;
+        uint32_t live = 0;
+        while (open_d) {
+          const int c = __ffs(open_d) - 1;
+          const uint32_t b0 = sh.dbeg[c], e0 = sh.dend[c];
+          if (b0 >= top) break;
+          const uint32_t lo = max(b0, base), hi = min(e0, top);
+          live |= bit_span(lo - base, hi - lo);
+          if (e0 > top) break;
+          open_d &= open_d - 1;
+        }
+        if (selfpos - base < 32u) live &= ~(1u << (selfpos - base));
         __syncwarp();
         if (live) {
-          const int cnt = (int)min(32u, total - base);
+          const int cnt_chunk = (int)min(32u, total - base);
           if (wrap) {
-            const uint32_t pairs = chunk_candidates<true>(sh, cnt, x0, x1, x2, w) & live;
+            const uint32_t pairs = chunk_candidates<true>(sh, cnt_chunk, x0, x1, x2, w) & live;
             n_pairs += __popc(pairs);
             chunk_forces<true>(sh, pairs, x0, x1, x2, w, far, A0, A1, A2);
           } else {
-            const uint32_t pairs = chunk_candidates<false>(sh, cnt, x0, x1, x2, w) & live;
+            const uint32_t pairs = chunk_candidates<false>(sh, cnt_chunk, x0, x1, x2, w) & live;
             n_pairs += __popc(pairs);
             chunk_forces<false>(sh, pairs, x0, x1, x2, w, far, A0, A1, A2);
           }
@@ -642,10 +687,9 @@ __global__ void __launch_bounds__(WARPS * 32) k_tree_walk(const uint4* __restric
         __syncwarp();
       }
     }
-    if (!more) break;
+    if (nx_count == 0) break;
     b_count = nx_count;
-    b_mask = nx_mask;
-    b_first = nx_first;
+    mine = nx_mine;
     cur ^= 1;
   }
   asm volatile("cp.async.wait_all;\n" ::: "memory");
@@ -755,7 +799,9 @@ void launch_tree_walk(const TreeNodes& t, const float* sorted_x3, size_t n, floa
               : warps == 2 ? (list ? k_tree_walk<false, true, 2> : k_tree_walk<false, false, 2>)
               : warps == 8 ? (list ? k_tree_walk<false, true, 8> : k_tree_walk<false, false, 8>)
                            : (list ? k_tree_walk<false, true, 4> : k_tree_walk<false, false, 4>);
-  kernel<<<blocks, warps * 32, 0, s>>>(static_cast<const uint4*>(t.link.p), static_cast<const float4*>(t.geo.p),
+  const size_t smem = (size_t)warps * (sizeof(WalkShared) + (t.has_quad ? 2 * SLOTS * sizeof(uint32_t) : 0));
+  if (smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  kernel<<<blocks, warps * 32, smem, s>>>(static_cast<const uint4*>(t.link.p), static_cast<const float4*>(t.geo.p),
                                          static_cast<const float4*>(t.mass.p), as<float4>(tm.x4), n, w,
                                          static_cast<const float*>(fc.far_dev.p), acc3, accumulate,
                                          reinterpret_cast<unsigned long long*>(counters), st, k_dev, list, list_n,
