@@ -115,6 +115,7 @@ def lib() -> C.CDLL:
         "cpm_sim_counters": (i, [vp, C.POINTER(u64), C.POINTER(u64), C.POINTER(u64), C.POINTER(u32)]),
         "cpm_sim_walk_candidates": (i, [vp, C.POINTER(u64)]),
         "cpm_walk_kernel_fit_error": (i, [fl, fl, i, C.POINTER(C.c_double)]),
+        "cpm_hilbert_fsm_check": (i, [i, u64, u64, C.POINTER(u64), C.POINTER(i)]),
         "cpm_sim_stream": (vp, [vp]),
         "cpm_sim_graphs": (i, [vp]),
         "cpm_sim_snapshot": (i, [vp, vp, vp, vp, vp, C.POINTER(i), C.POINTER(fl)]),

@@ -3,10 +3,15 @@
 // ballots, no tensor cores.
 #include <algorithm>
 #include <atomic>
+#include <mutex>
+#include <vector>
 
+#include "cpm_host.h"
 #include "cpm_internal.cuh"
 
 namespace cpm {
+
+constexpr int HFSM_STATES = 24;  // orientations of a cube: an upper bound on the Hilbert curve's states
 
 static std::atomic<unsigned long long> g_launches{0};
 unsigned long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
@@ -48,7 +53,7 @@ void release(DevBuf& b) {
 // sorting by it keeps every octree node's particles contiguous and orders the nodes, and the
 // particles, along a Hilbert curve.
 template <int BITS>
-__device__ __forceinline__ uint64_t hilbert_from_axes(uint32_t X0, uint32_t X1, uint32_t X2) {
+__host__ __device__ __forceinline__ uint64_t hilbert_from_axes(uint32_t X0, uint32_t X1, uint32_t X2) {
   uint32_t X[3] = {X0, X1, X2};
 #pragma unroll
   for (int b = BITS - 1; b >= 1; --b) {  // undo excess work, Q = 2^b
@@ -77,22 +82,149 @@ __device__ __forceinline__ uint64_t hilbert_from_axes(uint32_t X0, uint32_t X1, 
   return key;
 }
 
+// The same keys digit by digit: because a key's first 3d bits depend only on the first d octant
+// digits, digit d is a function of the octant at depth d and of a state (the orientation of the
+// curve in the depth-d cube) that the previous digits determine. The state machine is derived on
+// the host from hilbert_from_axes itself (states told apart by the order in which they visit the
+// eight octants; each transition read off from a representative prefix) and used only after it
+// reproduces the transform on every prefix of up to four digits and on 2^16 random coordinates.
+// Entry [state * 8 + octant] = digit | next state << 3.
+struct HilbertFsm {
+  unsigned char t[HFSM_STATES * 8];
+  int start = 0;
+  int states = 0;
+  int ok = 0;
+};
+
+static uint64_t hilbert_host(int bits, uint32_t a0, uint32_t a1, uint32_t a2) {
+  return bits == KEY_LEVELS ? hilbert_from_axes<KEY_LEVELS>(a0, a1, a2)
+                            : hilbert_from_axes<KEY_LEVELS - 2>(a0, a1, a2);
+}
+
+static uint64_t hilbert_fsm_host(const HilbertFsm& f, int bits, uint32_t a0, uint32_t a1, uint32_t a2) {
+  uint32_t st = (uint32_t)f.start;
+  uint64_t key = 0;
+  for (int d = 0; d < bits; ++d) {
+    const int j = bits - 1 - d;
+    const uint32_t o = ((a0 >> j) & 1u) | (((a1 >> j) & 1u) << 1) | (((a2 >> j) & 1u) << 2);
+    const uint32_t e = f.t[st * 8 + o];
+    key = (key << 3) | (e & 7u);
+    st = e >> 3;
+  }
+  return key;
+}
+
+static HilbertFsm derive_hilbert_fsm(int bits) {
+  HilbertFsm f;
+  // key of the point whose first digits are `pre` (octants, most significant first), zeros after
+  auto key_of = [&](const std::vector<uint32_t>& pre) {
+    uint32_t a0 = 0, a1 = 0, a2 = 0;
+    for (int d = 0; d < bits; ++d) {
+      const uint32_t o = d < (int)pre.size() ? pre[d] : 0u;
+      a0 = (a0 << 1) | (o & 1u);
+      a1 = (a1 << 1) | ((o >> 1) & 1u);
+      a2 = (a2 << 1) | ((o >> 2) & 1u);
+    }
+    return hilbert_host(bits, a0, a1, a2);
+  };
+  // the digits of the eight octants below prefix `pre`: the state's signature
+  auto order_of = [&](std::vector<uint32_t> pre) {
+    const int d = (int)pre.size();
+    uint32_t sig = 0;
+    pre.push_back(0);
+    for (uint32_t o = 0; o < 8; ++o) {
+      pre.back() = o;
+      sig |= (uint32_t)((key_of(pre) >> (3 * (bits - 1 - d))) & 7u) << (3 * o);
+    }
+    return sig;
+  };
+  std::vector<uint32_t> sigs;
+  std::vector<std::vector<uint32_t>> reps;
+  sigs.push_back(order_of({}));
+  reps.push_back({});
+  for (size_t q = 0; q < sigs.size(); ++q) {
+    if ((int)reps[q].size() + 2 > bits || sigs.size() > (size_t)HFSM_STATES) return f;
+    for (uint32_t o = 0; o < 8; ++o) {
+      std::vector<uint32_t> child = reps[q];
+      child.push_back(o);
+      const uint32_t sig = order_of(child);
+      size_t id = std::find(sigs.begin(), sigs.end(), sig) - sigs.begin();
+      if (id == sigs.size()) {
+        if (sigs.size() == (size_t)HFSM_STATES) return f;
+        sigs.push_back(sig);
+        reps.push_back(child);
+      }
+      f.t[q * 8 + o] = (unsigned char)(((sigs[q] >> (3 * o)) & 7u) | (id << 3));
+    }
+  }
+  f.states = (int)sigs.size();
+  // every prefix of up to four digits (the rest zero), then random coordinates
+  for (uint32_t p = 0; p < 4096u; ++p)
+    for (int len = 1; len <= 4; ++len) {
+      std::vector<uint32_t> pre;
+      for (int d = 0; d < len; ++d) pre.push_back((p >> (3 * d)) & 7u);
+      uint32_t a0 = 0, a1 = 0, a2 = 0;
+      for (int d = 0; d < bits; ++d) {
+        const uint32_t o = d < len ? pre[d] : 0u;
+        a0 = (a0 << 1) | (o & 1u);
+        a1 = (a1 << 1) | ((o >> 1) & 1u);
+        a2 = (a2 << 1) | ((o >> 2) & 1u);
+      }
+      if (hilbert_fsm_host(f, bits, a0, a1, a2) != hilbert_host(bits, a0, a1, a2)) return f;
+    }
+  uint64_t r = 0x9E3779B97F4A7C15ull;
+  const uint32_t mask = (1u << bits) - 1u;
+  for (int k = 0; k < (1 << 16); ++k) {
+    r ^= r << 13;
+    r ^= r >> 7;
+    r ^= r << 17;
+    const uint32_t a0 = (uint32_t)r & mask, a1 = (uint32_t)(r >> 21) & mask, a2 = (uint32_t)(r >> 42) & mask;
+    if (hilbert_fsm_host(f, bits, a0, a1, a2) != hilbert_host(bits, a0, a1, a2)) return f;
+  }
+  f.ok = 1;
+  return f;
+}
+
+// The state machines of the two key depths in use (21 digits; 19 under a batch of boxes), derived once.
+static const HilbertFsm& hilbert_fsm(int bits) {
+  static std::once_flag once;
+  static HilbertFsm f21, f19;
+  std::call_once(once, [] {
+    f21 = derive_hilbert_fsm(KEY_LEVELS);
+    f19 = derive_hilbert_fsm(KEY_LEVELS - 2);
+  });
+  return bits == KEY_LEVELS ? f21 : f19;
+}
+
 __global__ void k_octant_keys(const float* __restrict__ x3, size_t n, float half0, int levels,
                               uint64_t* __restrict__ keys, uint32_t* __restrict__ vals, DevStatus* st,
-                              size_t n_box, int box_shift, uint64_t* __restrict__ hkeys) {
+                              size_t n_box, int box_shift, uint64_t* __restrict__ hkeys, HilbertFsm fsm) {
+  __shared__ unsigned char table[HFSM_STATES * 8];
+  const bool use_fsm = hkeys && fsm.ok;
+  if (use_fsm) {
+    for (int j = threadIdx.x; j < HFSM_STATES * 8; j += blockDim.x) table[j] = fsm.t[j];
+    __syncthreads();
+  }
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float p0 = x3[3 * i], p1 = x3[3 * i + 1], p2 = x3[3 * i + 2];
   if (!(isfinite(p0) && isfinite(p1) && isfinite(p2))) dev_fail(st, DEV_NONFINITE, (int)i);
   float half = half0, c0 = half0, c1 = half0, c2 = half0;
-  uint64_t key = 0;
+  uint64_t key = 0, hkey = 0;
   uint32_t a0 = 0, a1 = 0, a2 = 0;  // the digits' bits per axis
+  uint32_t state = (uint32_t)fsm.start;
   for (int d = 0; d < levels; ++d) {
     const uint32_t o = (uint32_t)(p0 >= c0) | ((uint32_t)(p1 >= c1) << 1) | ((uint32_t)(p2 >= c2) << 2);
     key = (key << 3) | o;
-    a0 = (a0 << 1) | (o & 1u);
-    a1 = (a1 << 1) | ((o >> 1) & 1u);
-    a2 = (a2 << 1) | ((o >> 2) & 1u);
+    if (use_fsm) {
+      const uint32_t e = table[state * 8 + o];
+      hkey = (hkey << 3) | (e & 7u);
+      state = e >> 3;
+    } else {
+      a0 = (a0 << 1) | (o & 1u);
+      a1 = (a1 << 1) | ((o >> 1) & 1u);
+      a2 = (a2 << 1) | ((o >> 2) & 1u);
+    }
     const float q = half * 0.5f;  // == half / 2.0 exactly
     c0 = __fadd_rn(c0, (o & 1u) ? q : -q);
     c1 = __fadd_rn(c1, (o & 2u) ? q : -q);
@@ -102,8 +234,9 @@ __global__ void k_octant_keys(const float* __restrict__ x3, size_t n, float half
   const uint64_t boxbits = n_box ? (uint64_t)(i / n_box) << box_shift : 0ull;
   keys[i] = key | boxbits;
   if (hkeys) {
-    const uint64_t h = levels == KEY_LEVELS ? hilbert_from_axes<KEY_LEVELS>(a0, a1, a2)
-                                            : hilbert_from_axes<KEY_LEVELS - 2>(a0, a1, a2);
+    const uint64_t h = use_fsm ? hkey
+                               : (levels == KEY_LEVELS ? hilbert_from_axes<KEY_LEVELS>(a0, a1, a2)
+                                                       : hilbert_from_axes<KEY_LEVELS - 2>(a0, a1, a2));
     hkeys[i] = h | boxbits;
   }
   if (vals) vals[i] = (uint32_t)i;
@@ -114,8 +247,10 @@ void launch_octant_keys(const float* x3, size_t n, float box, int levels, uint64
   if (n == 0) return;
   const int T = 256;
   count_launch();
+  HilbertFsm fsm;  // ok = 0: the direct transform
+  if (hkeys && (levels == KEY_LEVELS || levels == KEY_LEVELS - 2)) fsm = hilbert_fsm(levels);
   k_octant_keys<<<(unsigned)((n + T - 1) / T), T, 0, s>>>(x3, n, box / 2.0f, levels, keys, vals, st, n_box,
-                                                          3 * levels, hkeys);
+                                                          3 * levels, hkeys, fsm);
 }
 
 __global__ void k_permute_u64(const uint64_t* __restrict__ in, const uint32_t* __restrict__ perm, size_t n,
@@ -406,3 +541,24 @@ cudaError_t radix_sort_pairs(uint64_t* keys, uint32_t* vals, size_t n, int bits,
 }
 
 }  // namespace cpm
+
+// Self-check of the table-driven Hilbert keys (host only): `samples` random integer coordinates
+// (xorshift from `seed`) keyed by the state machine and by the transform; mismatches counted.
+extern "C" int cpm_hilbert_fsm_check(int levels, uint64_t samples, uint64_t seed, uint64_t* mismatches, int* states) {
+  using namespace cpm;
+  if ((levels != KEY_LEVELS && levels != KEY_LEVELS - 2) || !mismatches || !states)
+    return set_error(nullptr, CPM_E_INVALID, "cpm_hilbert_fsm_check: levels must be 21 or 19, outputs non-null");
+  const HilbertFsm& f = hilbert_fsm(levels);
+  *states = f.ok ? f.states : 0;
+  uint64_t bad = 0, r = seed | 1ull;
+  const uint32_t mask = (1u << levels) - 1u;
+  for (uint64_t k = 0; k < samples; ++k) {
+    r ^= r << 13;
+    r ^= r >> 7;
+    r ^= r << 17;
+    const uint32_t a0 = (uint32_t)r & mask, a1 = (uint32_t)(r >> 21) & mask, a2 = (uint32_t)(r >> 42) & mask;
+    if (!f.ok || hilbert_fsm_host(f, levels, a0, a1, a2) != hilbert_host(levels, a0, a1, a2)) ++bad;
+  }
+  *mismatches = bad;
+  return CPM_OK;
+}

@@ -305,6 +305,12 @@ int cpm_sim_walk_candidates(cpm_sim* sim, uint64_t* candidates);
  * S(r) = erfc(u) + (2/sqrt(pi)) u e^{-u^2}, u = r / (2 r_split) (tree.rs:54-57), against a
  * double-precision evaluation on `samples` points of [0, r_cut]. */
 int cpm_walk_kernel_fit_error(float r_split, float r_cut, int samples, double* max_rel_err);
+/* Self-check of the simulation's Hilbert sort keys (host only): the keys are computed digit by
+ * digit by a state machine derived from the Hilbert transform; this compares the two on `samples`
+ * random integer coordinates of `levels` (21, or 19 under a batch of boxes) bits per axis and
+ * reports the mismatches and the machine's number of states (0 when it could not be derived, in
+ * which case the device computes the transform directly). */
+int cpm_hilbert_fsm_check(int levels, uint64_t samples, uint64_t seed, uint64_t* mismatches, int* states);
 /* Device-side counters of the last step: nodes, leaf pairs, accepted nodes, kernels launched per step. */
 int cpm_sim_counters(cpm_sim* sim, uint64_t* nodes, uint64_t* leaf_pairs, uint64_t* node_accepts,
                      uint32_t* launches_per_step);
