@@ -50,7 +50,6 @@
 
 namespace cpm {
 
-constexpr int WALK_WARPS = 4;
 constexpr int SLOTS = 32;     // nodes per step of a warp's walk (one per lane)
 constexpr int MERGE_SP = 96;  // stack entries are merged into one step only while the stack is this shallow
 // Stack bound: a merging step starts at depth <= MERGE_SP and pushes at most SLOTS entries; from
