@@ -68,3 +68,12 @@ def test_state_machine_keys_match_the_transform():
         assert native.lib().cpm_hilbert_fsm_check(levels, 200000, 12345, C.byref(bad), C.byref(states)) == 0
         assert states.value in (12, 24), (levels, states.value)
         assert bad.value == 0, (levels, bad.value)
+
+
+def test_state_machine_check_rejects_other_depths():
+    import ctypes as C
+    import importlib
+    native = importlib.import_module("cosmological-particle-simulation_b200._native")
+    bad, states = C.c_uint64(), C.c_int()
+    for levels in (0, 20, 22):
+        assert native.lib().cpm_hilbert_fsm_check(levels, 10, 1, C.byref(bad), C.byref(states)) != 0
